@@ -1,0 +1,331 @@
+"""Benchmark of the curvelet path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one pass of the whole path (spatial hash -> neighbour CSR -> pairwise
+curve bundles -> chain growth, dedup, record -> compacted chains + info) over
+one batch of seeded synthetic edges. Workloads:
+
+  plain_hd    one 1920x1080 map, ~242k edges, one map per launch (default)
+  plain_small one 480x320 map (~4.5k edges)
+  mixed64     64 maps of uneven size (640x480 .. 3840x2160) in one ragged batch
+
+value: edges/s with the edges already in HBM (CUDA events on the engine's
+stream around each step, L2 flushed between steps). e2e: the same metric
+through the C ABI call a user makes (cvl_run: pinned host edges in, chains and
+info out, copies inside the timed region). With N GPUs (torchrun) every rank
+processes its own instance of the workload (replicas, weak scaling) and the
+step time is the max over ranks; there is no data-path collective.
+
+--impl reference times the reference's own cpu_curvelet code (compiled from
+its sources into oracle/_ref/libcvlref.so) on this host's cores, on the same
+workload, metric and unit.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edges/s"
+# per computed (non-close) pair: 63 cells x 20 FP64 flops, divisions counted as 1
+FLOPS_PER_PAIR_CELL = 20
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="plain_hd", choices=["plain_hd", "plain_small", "mixed64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def _workload(name: str, rank: int):
+    from curvelet_construction_on_gpu_b200 import synth
+    if name == "plain_hd":
+        return [synth.plain_hd(1000 + rank)], {"image": "1920x1080", "curves": 1500, "clutter": 0.2}
+    if name == "plain_small":
+        return [synth.plain_small(0 + rank)], {"image": "480x320", "curves": 50, "clutter": 0.1}
+    maps = synth.mixed64(2000 + 64 * rank, 64)
+    return maps, {"maps": 64, "images": "640x480..3840x2160", "clutter": 0.2}
+
+
+class _Clocks:
+    """Samples SM clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.proc = None
+        self.index = index
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict:
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def _pinned(a: np.ndarray) -> np.ndarray:
+    """A page-locked copy of a (torch's pinned allocator), for the e2e copies."""
+    try:
+        import torch
+        t = torch.empty(a.size, dtype=torch.float64).pin_memory()
+        out = t.numpy().reshape(a.shape)
+        out[...] = a
+        out._keep = t  # type: ignore[attr-defined]
+        return out
+    except Exception:
+        return np.ascontiguousarray(a)
+
+
+def _dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def _max_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _sum_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def _barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
+    """The reference's own code (oracle/_ref) on this host's cores, on a bounded
+    sample of the workload: whole maps in order until ~budget_s of CPU work."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    kind = "reference" if O.ref_available() else "port"
+    edges = 0
+    secs = 0.0
+    used = 0
+    for m in maps:
+        t0 = time.perf_counter()
+        if kind == "reference":
+            r = O.ref_run(m, nthreads=threads, want_outputs=False)
+            dt = (r.ms["csr"] + r.ms["pairwise"] + r.ms["greedy"]) / 1e3
+        else:
+            O.run(m, nthreads=threads)
+            dt = time.perf_counter() - t0
+        edges += m.shape[0]
+        secs += dt
+        used += 1
+        if secs > budget_s:
+            break
+    return {"value": edges / secs, "unit": METRIC, "cores": threads, "kind": kind,
+            "sample": f"{used} of {len(maps)} map(s), {edges} edges, timed as the reference's own "
+                      f"CSR + form_pairwise_bundles + build_curvelets_greedy phases (file I/O excluded)"}
+
+
+def run_reference(args, maps, cfg, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcvlref.so was not built "
+                          "(the reference sources were absent at build time)"}))
+        return
+    threads = os.cpu_count() or 1
+    # each step: the whole workload when it is small enough, else a bounded sample of whole maps
+    sample, tot = [], 0
+    for m in maps:
+        sample.append(m)
+        tot += m.shape[0]
+        if tot >= 300_000:
+            break
+    for _ in range(args.warmup):
+        O.ref_run(sample[0], nthreads=threads, want_outputs=False)
+    step_s = []
+    for _ in range(args.steps):
+        s = 0.0
+        for m in sample:
+            r = O.ref_run(m, nthreads=threads, want_outputs=False)
+            s += (r.ms["csr"] + r.ms["pairwise"] + r.ms["greedy"]) / 1e3
+        step_s.append(s)
+    ms = 1e3 * float(np.mean(step_s))
+    value = tot / (ms / 1e3)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": dict(workload=args.workload, edges=tot, maps=len(sample), **cfg),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+                             "sample": f"{len(sample)} of {len(maps)} map(s), {tot} edges per step"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args, maps, cfg, world, rank, local, pg):
+    import curvelet_construction_on_gpu_b200 as cvl
+    eng = cvl.Engine(device=local)
+    n_edges = int(sum(m.shape[0] for m in maps))
+    batch = eng.upload_batch(maps)
+    # pairs that get a full bundle computation (not a close pair), from the neighbour graph
+    nonclose = 0
+    for m in maps:
+        g = eng.build_neighbor_graph(m, 3.5, 3, 128)
+        nonclose += int(np.count_nonzero(g.neighbor_dist2 >= 4 * 0.4 * 0.4))
+        del g
+    fp64_peak = eng.fp64_peak_tflops() if rank == 0 else None
+
+    for _ in range(max(args.warmup, 3) if args.warmup >= 3 else args.warmup):
+        r = eng.run_batch(batch)
+        r.close()
+    _barrier(pg)
+    step_ms, kern = [], []
+    with _Clocks(local) as clk:
+        for _ in range(args.steps):
+            eng.flush_l2()
+            r = eng.run_batch(batch)
+            st = r.stats()
+            step_ms.append(st["device_ms"])
+            kern.append(dict(eng.kernel_times()))
+            r.close()
+    _barrier(pg)
+    sum_ms = _max_over_ranks(pg, float(np.sum(step_ms)))
+    total_edges = _sum_over_ranks(pg, float(n_edges)) * args.steps
+    value = total_edges / (sum_ms / 1e3)
+    last = eng.run_batch(batch)
+    stats = last.stats()
+    n_curv = int(stats["num_curvelets"])
+    last.close()
+
+    # e2e through the public one-shot call (plain form: one map per call)
+    e2e = None
+    if not args.no_e2e:
+        pinned = [_pinned(m) for m in maps]
+        for m in pinned[: min(2, len(pinned))]:
+            eng.run(m)
+        _barrier(pg)
+        t0 = time.perf_counter()
+        bo = 0
+        for _ in range(args.steps):
+            for m in pinned:
+                res = eng.run(m)
+                bo += res.chains.nbytes + res.info.nbytes
+        wall = time.perf_counter() - t0
+        wall = _max_over_ranks(pg, wall)
+        e2e = {"value": _sum_over_ranks(pg, float(n_edges)) * args.steps / wall, "unit": METRIC,
+               "h2d_bytes_per_step": int(sum(m.nbytes for m in maps)), "d2h_bytes_per_step": int(bo // args.steps),
+               "path": "cvl_run (C ABI), one map per call, pinned host edges"}
+
+    if rank != 0:
+        return
+    curv_ms = float(np.mean([k.get("curvelets", 0.0) for k in kern]))
+    flops = FLOPS_PER_PAIR_CELL * 63 * nonclose
+    achieved = flops / (curv_ms / 1e3) / 1e12 if curv_ms > 0 else 0.0
+    clocks = clk.summary()
+    stage_ms = {k: float(np.mean([d.get(k, 0.0) for d in kern])) for k in kern[0]} if kern else {}
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sum_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators, curvelet_construction_on_gpu_b200/synth.py)",
+        "config": dict(workload=args.workload, edges_per_gpu=n_edges, l2="flushed between steps",
+                       curvelets_per_gpu=n_curv, pairs_per_gpu=int(stats["total_pairs"]),
+                       valid_pairs_per_gpu=int(stats["valid_pairs"]), parallelism=f"replicas x{world}", **cfg),
+        "curvelets_per_s": n_curv * world * args.steps / (sum_ms / 1e3),
+        "stage_ms": stage_ms,
+        "roofline": {"bound": "fp64", "kernel": "k_curvelets", "achieved": achieved, "peak": fp64_peak,
+                     "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if fp64_peak else None,
+                     "peak_source": "measured DFMA loop (cvl_measure_fp64_peak), 2 flops per FMA",
+                     "work": f"{FLOPS_PER_PAIR_CELL} flops x 63 cells x {nonclose} non-close pairs",
+                     "traffic": None},
+        "gpu_launches": None,
+        "clocks": clocks,
+        "e2e": e2e,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = _cpu_baseline(maps)
+    print(json.dumps(line))
+    eng.close()
+
+
+def main():
+    args = _args()
+    world, rank, local, pg = _dist_init(args)
+    maps, cfg = _workload(args.workload, rank)
+    try:
+        if args.impl == "reference":
+            run_reference(args, maps, cfg, world, rank)
+        else:
+            run_ours(args, maps, cfg, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

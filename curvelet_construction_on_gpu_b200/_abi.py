@@ -1,0 +1,114 @@
+"""ctypes binding of libcvl.so (include/cvl.h). No fallback: importing the
+package on a machine without the built library raises, and every call that
+needs a GPU fails with the engine's own error when none is present."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libcvl.so")
+
+CVL_OK = 0
+CVL_EINVAL = -1
+CVL_ENOMEM = -2
+CVL_ECUDA = -3
+CVL_EUNSUPPORTED = -4
+CVL_ETIMEDOUT = -5
+CVL_EOVERFLOW = -6
+CVL_EAGAIN = -7
+CVL_ENODEV = -8
+
+ERRNAMES = {0: "CVL_OK", -1: "CVL_EINVAL", -2: "CVL_ENOMEM", -3: "CVL_ECUDA", -4: "CVL_EUNSUPPORTED",
+            -5: "CVL_ETIMEDOUT", -6: "CVL_EOVERFLOW", -7: "CVL_EAGAIN", -8: "CVL_ENODEV"}
+
+
+class CvlParams(C.Structure):
+    _fields_ = [("nrad", C.c_double), ("gap", C.c_double), ("dx", C.c_double), ("dt_deg", C.c_double),
+                ("dt_rad", C.c_double), ("max_k", C.c_double), ("curvelet_style", C.c_uint),
+                ("group_max_sz", C.c_uint), ("out_type", C.c_uint), ("sx", C.c_double), ("st", C.c_double),
+                ("edge_data_sz", C.c_int), ("max_candidates", C.c_uint)]
+
+
+class CvlEngineCfg(C.Structure):
+    _fields_ = [("device", C.c_int), ("mem_budget_bytes", C.c_size_t), ("cell_size", C.c_int),
+                ("seeds_per_group", C.c_int), ("bundle_slots", C.c_int), ("warps_per_block", C.c_int)]
+
+
+class CvlResultView(C.Structure):
+    _fields_ = [("num_curvelets", C.c_uint32), ("chain_width", C.c_uint32),
+                ("chains", C.POINTER(C.c_uint32)), ("info", C.POINTER(C.c_double)),
+                ("valid_pairs", C.c_uint32), ("total_neighbor_pairs", C.c_int64),
+                ("max_num_of_neighbors", C.c_uint32), ("truncated_anchors", C.c_uint32),
+                ("num_edges", C.c_uint32), ("flags", C.c_uint32), ("device_ms", C.c_double)]
+
+
+class CvlGraphView(C.Structure):
+    _fields_ = [("num_edges", C.c_int32), ("total_neighbor_pairs", C.c_int64),
+                ("max_num_of_neighbors", C.c_uint32), ("truncated_anchors", C.c_uint32),
+                ("neighbor_offsets", C.POINTER(C.c_int32)), ("neighbor_ids", C.POINTER(C.c_int32)),
+                ("neighbor_dist2", C.POINTER(C.c_double))]
+
+
+# (name, restype, argtypes) of every entry point declared in include/cvl.h
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+SIGNATURES = [
+    ("cvl_params_default", None, [C.POINTER(CvlParams)]),
+    ("cvl_engine_cfg_default", None, [C.POINTER(CvlEngineCfg)]),
+    ("cvl_engine_create", C.c_int, [C.POINTER(CvlEngineCfg), C.POINTER(_vp)]),
+    ("cvl_engine_destroy", None, [_vp]),
+    ("cvl_last_error", C.c_char_p, []),
+    ("cvl_version", C.c_char_p, []),
+    ("cvl_run", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.POINTER(CvlParams), C.POINTER(_vp)]),
+    ("cvl_result_get", C.c_int, [_vp, C.POINTER(CvlResultView)]),
+    ("cvl_result_free", None, [_vp]),
+    ("cvl_build_neighbor_graph", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.c_double, C.c_uint, C.c_uint,
+                                           C.POINTER(_vp)]),
+    ("cvl_graph_get", C.c_int, [_vp, C.POINTER(CvlGraphView)]),
+    ("cvl_graph_free", None, [_vp]),
+    ("cvl_form_pairwise_bundles", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.POINTER(C.c_uint32)]),
+    ("cvl_build_curvelets", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.POINTER(_vp)]),
+    ("cvl_pair_bundles", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), _dp, _dp,
+                                   C.POINTER(C.c_uint8), C.POINTER(C.c_int32)]),
+    ("cvl_batch_upload", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    ("cvl_batch_free", None, [_vp]),
+    ("cvl_batch_run", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.POINTER(_vp)]),
+    ("cvl_batch_result_map", C.c_int, [_vp, C.c_int32, C.POINTER(CvlResultView)]),
+    ("cvl_batch_result_stats", C.c_int, [_vp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_uint64)]),
+    ("cvl_batch_result_free", None, [_vp]),
+    ("cvl_engine_flush_l2", C.c_int, [_vp]),
+    ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),
+    ("cvl_measure_fp64_peak", C.c_int, [_vp, _dp]),
+]
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads libcvl.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libcvl.so is not built ({LIB_PATH}); run "
+                              "`python -m curvelet_construction_on_gpu_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class CvlError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        msg = load().cvl_last_error().decode(errors="replace")
+        super().__init__(f"{what}: {ERRNAMES.get(code, code)}: {msg}")
+
+
+def check(code: int, what: str) -> None:
+    if code != CVL_OK:
+        raise CvlError(code, what)

@@ -1,0 +1,415 @@
+"""Host-side API over libcvl.so.
+
+Two layers, mirroring the reference:
+
+* the engine layer (``Engine``): one-shot ``run`` (run_curvelet<double> without
+  file I/O, cpu_curvelet/main.cpp:20-96), device-resident ragged batches,
+  per-kernel timings;
+* the reference's template API, same names and argument meaning:
+  ``build_neighbor_csr_graph`` (cpu_curvelet/preprocess.hpp:186-274) filling a
+  ``GPUNeighborGraph`` (the CPUNeighborGraph fields, preprocess.hpp:18-31), and
+  ``CurveletGPU`` (CurveletCPU, cpu_curvelet/cpu_curvelet.hpp:22-123) with
+  ``form_pairwise_bundles`` / ``build_curvelets_greedy`` / ``num_curvelets`` /
+  ``chain_width`` / ``_edge_chain_final`` / ``_curvelet_info``.
+
+Everything computes on the GPU through the C ABI; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import CvlEngineCfg, CvlGraphView, CvlParams, CvlResultView, check
+
+M_PI = 3.14159265358979323846  # curvelet_utils.hpp:10
+
+
+@dataclass
+class CurveletParams:
+    """CurveletParams (cpu_curvelet/param_settings.hpp:9-24): same fields and defaults."""
+    nrad: float = 3.5
+    gap: float = 1.5
+    dx: float = 0.4
+    dt_deg: float = 15.0
+    max_k: float = 0.3
+    curvelet_style: int = 2
+    group_max_sz: int = 4
+    out_type: int = 0
+    sx: float = 0.1
+    st: float = 0.08
+    edge_file: str = "eth3d_cables2.txt"
+    edge_data_sz: int = 4
+    max_candidates: int = 128
+
+    def to_c(self, dt_rad: float = 0.0) -> CvlParams:
+        p = CvlParams()
+        _abi.load().cvl_params_default(C.byref(p))
+        p.nrad, p.gap, p.dx, p.dt_deg, p.dt_rad, p.max_k = (self.nrad, self.gap, self.dx, self.dt_deg, dt_rad,
+                                                            self.max_k)
+        p.curvelet_style, p.group_max_sz, p.out_type = self.curvelet_style, self.group_max_sz, self.out_type
+        p.sx, p.st, p.edge_data_sz, p.max_candidates = self.sx, self.st, self.edge_data_sz, self.max_candidates
+        return p
+
+
+@dataclass
+class Result:
+    """Curvelets of one map: chains [C, group_max_sz + 1] uint32 (1-based ids,
+    zero padded) and info [C, 10] float64 (the info file's rows)."""
+    chains: np.ndarray
+    info: np.ndarray
+    valid_pairs: int
+    total_neighbor_pairs: int
+    max_num_of_neighbors: int
+    truncated_anchors: int
+    num_edges: int
+    device_ms: float = 0.0
+
+    @property
+    def num_curvelets(self) -> int:
+        return int(self.chains.shape[0])
+
+
+def _view_to_result(v: CvlResultView) -> Result:
+    nc, w = int(v.num_curvelets), int(v.chain_width)
+    if nc:
+        chains = np.ctypeslib.as_array(v.chains, shape=(nc * w,)).reshape(nc, w).copy()
+        info = np.ctypeslib.as_array(v.info, shape=(nc * 10,)).reshape(nc, 10).copy()
+    else:
+        chains = np.zeros((0, w), np.uint32)
+        info = np.zeros((0, 10), np.float64)
+    return Result(chains, info, int(v.valid_pairs), int(v.total_neighbor_pairs), int(v.max_num_of_neighbors),
+                  int(v.truncated_anchors), int(v.num_edges), float(v.device_ms))
+
+
+def _edges(edges) -> np.ndarray:
+    e = np.ascontiguousarray(edges, dtype=np.float64)
+    if e.ndim != 2:
+        raise ValueError("edges must be a 2-D array [num_edges, edge_data_sz]")
+    return e
+
+
+class Engine:
+    """One CUDA device, one stream, a grow-only device workspace."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, cell_size: int = 0, seeds_per_group: int = 0,
+                 bundle_slots: int = 0):
+        lib = _abi.load()
+        cfg = CvlEngineCfg()
+        lib.cvl_engine_cfg_default(C.byref(cfg))
+        cfg.device, cfg.mem_budget_bytes, cfg.cell_size = device, mem_budget_bytes, cell_size
+        cfg.seeds_per_group, cfg.bundle_slots = seeds_per_group, bundle_slots
+        h = C.c_void_p()
+        check(lib.cvl_engine_create(C.byref(cfg), C.byref(h)), "cvl_engine_create")
+        self._h = h
+        self._lib = lib
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.cvl_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- the plain form
+    def run(self, edges, params: CurveletParams | None = None, dt_rad: float = 0.0) -> Result:
+        params = params or CurveletParams()
+        e = _edges(edges)
+        p = params.to_c(dt_rad)
+        r = C.c_void_p()
+        check(self._lib.cvl_run(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1], C.byref(p),
+                                C.byref(r)), "cvl_run")
+        try:
+            v = CvlResultView()
+            check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
+            return _view_to_result(v)
+        finally:
+            self._lib.cvl_result_free(r)
+
+    # ---- staged API
+    def build_neighbor_graph(self, edges, rad: float = 3.5, neighbor_radius: int = 3,
+                             max_candidates: int = 128) -> "GPUNeighborGraph":
+        e = _edges(edges)
+        g = C.c_void_p()
+        check(self._lib.cvl_build_neighbor_graph(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1], rad,
+                                                 neighbor_radius, max_candidates, C.byref(g)),
+              "cvl_build_neighbor_graph")
+        return GPUNeighborGraph._from_handle(self, g, e)
+
+    def form_pairwise_bundles(self, graph: "GPUNeighborGraph", params: CurveletParams, dt_rad: float = 0.0) -> int:
+        p = params.to_c(dt_rad)
+        vp = C.c_uint32(0)
+        check(self._lib.cvl_form_pairwise_bundles(self._h, graph._h, C.byref(p), C.byref(vp)),
+              "cvl_form_pairwise_bundles")
+        return int(vp.value)
+
+    def build_curvelets(self, graph: "GPUNeighborGraph", params: CurveletParams, dt_rad: float = 0.0) -> Result:
+        p = params.to_c(dt_rad)
+        r = C.c_void_p()
+        check(self._lib.cvl_build_curvelets(self._h, graph._h, C.byref(p), C.byref(r)), "cvl_build_curvelets")
+        try:
+            v = CvlResultView()
+            check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
+            return _view_to_result(v)
+        finally:
+            self._lib.cvl_result_free(r)
+
+    def pair_bundles(self, pairs, params: CurveletParams | None = None, dt_rad: float = 0.0):
+        """Bundles of independent (anchor, neighbour) pairs, rows (te_x, te_y, te_theta, le_x, le_y, le_theta).
+        Returns (bmin [n, cells], bmax [n, cells], valid [n] bool)."""
+        params = params or CurveletParams()
+        q = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1, 6)
+        n = q.shape[0]
+        p = params.to_c(dt_rad)
+        cells = C.c_int32(0)
+        cap = 128
+        bmin = np.zeros((max(n, 1), cap))
+        bmax = np.zeros((max(n, 1), cap))
+        valid = np.zeros(max(n, 1), np.uint8)
+        # first call sizes the grid
+        check(self._lib.cvl_pair_bundles(self._h, q.ctypes.data_as(_abi._dp), 0, C.byref(p),
+                                         bmin.ctypes.data_as(_abi._dp), bmax.ctypes.data_as(_abi._dp),
+                                         valid.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(cells)),
+              "cvl_pair_bundles")
+        nc = cells.value
+        bmin = np.zeros((max(n, 1), nc))
+        bmax = np.zeros((max(n, 1), nc))
+        check(self._lib.cvl_pair_bundles(self._h, q.ctypes.data_as(_abi._dp), n, C.byref(p),
+                                         bmin.ctypes.data_as(_abi._dp), bmax.ctypes.data_as(_abi._dp),
+                                         valid.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(cells)),
+              "cvl_pair_bundles")
+        return bmin[:n], bmax[:n], valid[:n].astype(bool)
+
+    # ---- batches
+    def upload_batch(self, maps: list) -> "Batch":
+        arrs = [_edges(m) for m in maps]
+        sz = arrs[0].shape[1]
+        if any(a.shape[1] != sz for a in arrs):
+            raise ValueError("all maps of a batch need the same edge_data_sz")
+        cat = np.ascontiguousarray(np.concatenate(arrs, axis=0))
+        counts = np.asarray([a.shape[0] for a in arrs], dtype=np.int32)
+        b = C.c_void_p()
+        check(self._lib.cvl_batch_upload(self._h, cat.ctypes.data_as(_abi._dp),
+                                         counts.ctypes.data_as(C.POINTER(C.c_int32)), len(arrs), sz, C.byref(b)),
+              "cvl_batch_upload")
+        return Batch(self, b, counts)
+
+    def run_batch(self, batch: "Batch", params: CurveletParams | None = None) -> "BatchResult":
+        params = params or CurveletParams()
+        p = params.to_c()
+        r = C.c_void_p()
+        check(self._lib.cvl_batch_run(self._h, batch._h, C.byref(p), C.byref(r)), "cvl_batch_run")
+        return BatchResult(self, r, len(batch.counts))
+
+    # ---- measurement helpers
+    def flush_l2(self) -> None:
+        check(self._lib.cvl_engine_flush_l2(self._h), "cvl_engine_flush_l2")
+
+    def kernel_times(self) -> list[tuple[str, float]]:
+        names = (C.c_char_p * 64)()
+        ms = (C.c_double * 64)()
+        n = self._lib.cvl_engine_last_kernel_times(self._h, names, ms, 64)
+        if n < 0:
+            check(n, "cvl_engine_last_kernel_times")
+        return [(names[k].decode(), float(ms[k])) for k in range(min(n, 64))]
+
+    def fp64_peak_tflops(self) -> float:
+        t = C.c_double(0)
+        check(self._lib.cvl_measure_fp64_peak(self._h, C.byref(t)), "cvl_measure_fp64_peak")
+        return float(t.value)
+
+
+class Batch:
+    def __init__(self, eng: Engine, h, counts):
+        self._eng, self._h, self.counts = eng, h, counts
+
+    def close(self):
+        if self._h:
+            self._eng._lib.cvl_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchResult:
+    def __init__(self, eng: Engine, h, num_maps: int):
+        self._eng, self._h, self.num_maps = eng, h, num_maps
+
+    def stats(self) -> dict:
+        ms = C.c_double(0)
+        nc, vp, tp = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        check(self._eng._lib.cvl_batch_result_stats(self._h, C.byref(ms), C.byref(nc), C.byref(vp), C.byref(tp)),
+              "cvl_batch_result_stats")
+        return dict(device_ms=ms.value, num_curvelets=nc.value, valid_pairs=vp.value, total_pairs=tp.value)
+
+    def map(self, m: int) -> Result:
+        v = CvlResultView()
+        check(self._eng._lib.cvl_batch_result_map(self._h, m, C.byref(v)), "cvl_batch_result_map")
+        return _view_to_result(v)
+
+    def close(self):
+        if self._h:
+            self._eng._lib.cvl_batch_result_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# The reference's template API, same names and argument meaning
+# ---------------------------------------------------------------------------
+_default_engine: Engine | None = None
+
+
+def default_engine() -> Engine:
+    global _default_engine
+    if _default_engine is None:
+        _default_engine = Engine()
+    return _default_engine
+
+
+@dataclass
+class GPUNeighborGraph:
+    """CPUNeighborGraph<T> (preprocess.hpp:18-31): CSR over anchors in input order,
+    neighbour lists sorted by ascending squared distance."""
+    num_edges: int = 0
+    total_neighbor_pairs: int = 0
+    max_num_of_neighbors: int = 0
+    edges: np.ndarray = field(default_factory=lambda: np.zeros((0, 4)))
+    neighbor_offsets: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int32))
+    neighbor_ids: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    neighbor_dist2: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    truncated_anchors: int = 0
+    _h: object = None
+    _eng: object = None
+
+    @classmethod
+    def _from_handle(cls, eng: Engine, h, edges: np.ndarray) -> "GPUNeighborGraph":
+        v = CvlGraphView()
+        check(eng._lib.cvl_graph_get(h, C.byref(v)), "cvl_graph_get")
+        n, p = int(v.num_edges), int(v.total_neighbor_pairs)
+        g = cls()
+        g._fill(eng, h, edges, v, n, p)
+        return g
+
+    def _fill(self, eng, h, edges, v, n, p):
+        self.num_edges, self.total_neighbor_pairs = n, p
+        self.max_num_of_neighbors = int(v.max_num_of_neighbors)
+        self.truncated_anchors = int(v.truncated_anchors)
+        self.edges = edges
+        self.neighbor_offsets = np.ctypeslib.as_array(v.neighbor_offsets, shape=(n + 1,)).copy()
+        self.neighbor_ids = (np.ctypeslib.as_array(v.neighbor_ids, shape=(p,)).copy() if p
+                             else np.zeros(0, np.int32))
+        self.neighbor_dist2 = (np.ctypeslib.as_array(v.neighbor_dist2, shape=(p,)).copy() if p
+                               else np.zeros(0))
+        if self._h is not None and self._eng is not None:
+            self._eng._lib.cvl_graph_free(self._h)
+        self._h, self._eng = h, eng
+
+    def __del__(self):
+        try:
+            if self._h is not None and self._eng is not None and self._eng._h:
+                self._eng._lib.cvl_graph_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def build_neighbor_csr_graph(num_edges: int, sz_edge_data: int, edges, rad: float, neighbor_radius: int,
+                             max_candidates: int, nthreads: int, graph: GPUNeighborGraph,
+                             engine: Engine | None = None) -> bool:
+    """build_neighbor_csr_graph<T> (preprocess.hpp:186-274): returns False on
+    num_edges <= 0, sz_edge_data < 4 or no edges, as the reference does."""
+    del nthreads  # the GPU path has no host thread count
+    if num_edges <= 0 or sz_edge_data < 4 or edges is None:
+        return False
+    e = np.ascontiguousarray(edges, dtype=np.float64).reshape(-1)[: num_edges * sz_edge_data]
+    e = e.reshape(num_edges, sz_edge_data)
+    eng = engine or default_engine()
+    g = eng.build_neighbor_graph(e, rad, neighbor_radius, max_candidates)
+    # move the arrays and the handle over to the caller's graph object
+    if graph._h is not None and graph._eng is not None:
+        graph._eng._lib.cvl_graph_free(graph._h)
+    for k in ("num_edges", "total_neighbor_pairs", "max_num_of_neighbors", "edges", "neighbor_offsets",
+              "neighbor_ids", "neighbor_dist2", "truncated_anchors"):
+        setattr(graph, k, getattr(g, k))
+    graph._h, graph._eng = g._h, g._eng
+    g._h = None
+    return True
+
+
+@dataclass
+class CurveletFormationResult:
+    """CPUCurveletFormationResult (cpu_curvelet.hpp:18-20)."""
+    valid_pairs: int = 0
+
+
+class CurveletGPU:
+    """CurveletCPU<T> (cpu_curvelet.hpp:22-123) on the GPU. The constructor takes
+    the reference's arguments (dt in radians); the outputs are exposed under the
+    reference's member names:
+
+    * ``_edge_chain_final``: [num_curvelets, chain_width] uint32, 1-based ids;
+    * ``_curvelet_info``: column-major like the reference ([10, num_curvelets],
+      _curvelet_info[col, row]); ``curvelet_info_rows`` is the row-major file layout.
+    """
+
+    def __init__(self, num_edges: int, sz_edge_data: int, csr: GPUNeighborGraph, dx: float, dt: float, sx: float,
+                 st: float, max_k: float, group_max_sz: int, nthreads: int, to_edges, nrad: float,
+                 engine: Engine | None = None):
+        del nthreads, to_edges  # edges come from the graph, as the reference reads csr.edges
+        self._n, self._sz, self._csr = num_edges, sz_edge_data, csr
+        self._dt = dt
+        self._params = CurveletParams(nrad=nrad, dx=dx, dt_deg=dt * 180.0 / M_PI, max_k=max_k, sx=sx, st=st,
+                                      group_max_sz=group_max_sz, edge_data_sz=sz_edge_data)
+        self._eng = engine or csr._eng or default_engine()
+        self._group_max_sz = group_max_sz
+        self._num_curvelets = 0
+        self._edge_chain_final = np.zeros((0, group_max_sz + 1), np.uint32)
+        self._curvelet_info = np.zeros((10, 0))
+        self.curvelet_info_rows = np.zeros((0, 10))
+        self._max_curvelets = num_edges * (csr.max_num_of_neighbors + 1) * 2  # cpu_curvelet.hpp:64
+
+    def form_pairwise_bundles(self, result: CurveletFormationResult) -> bool:
+        result.valid_pairs = self._eng.form_pairwise_bundles(self._csr, self._params, dt_rad=self._dt)
+        return True
+
+    def build_curvelets_greedy(self) -> None:
+        r = self._eng.build_curvelets(self._csr, self._params, dt_rad=self._dt)
+        self._num_curvelets = r.num_curvelets
+        self._edge_chain_final = r.chains
+        self.curvelet_info_rows = r.info
+        self._curvelet_info = r.info.T
+        self.last_result = r
+
+    def num_curvelets(self) -> int:
+        return self._num_curvelets
+
+    def chain_width(self) -> int:
+        return self._group_max_sz + 1
+
+
+def run_curvelet(edges, params: CurveletParams | None = None, engine: Engine | None = None) -> Result:
+    """run_curvelet<double> (main.cpp:20-96) without the file I/O."""
+    return (engine or default_engine()).run(edges, params or CurveletParams())

@@ -1,0 +1,281 @@
+// cvl_cli.cpp -- drop-in replacement for the reference CURVELET program
+// (cpu_curvelet/main.cpp), running the path on the GPU through libcvl.
+//
+// Same flags and defaults (cpu_curvelet/param_settings.hpp:26-155), same input
+// location and format (../test_files/<edge-file>, data_io.hpp:11-79), same
+// outputs (../outputs/<output> and its info file, data_io.hpp:81-145, written
+// with the default ostream formatting), same summary lines on stdout.
+#include <cerrno>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/cvl.h"
+
+namespace {
+
+struct CliParams {
+    cvl_params p;
+    std::string edge_file = "eth3d_cables2.txt";  // param_settings.hpp:21
+};
+
+void print_usage(const char *prog) {
+    std::cerr << "Usage: " << prog << " [options]\n"
+              << "\n"
+              << "Options:\n"
+              << "  --float, --double          Scalar type (default: double; the GPU engine computes in double)\n"
+              << "  --output <file>            Output chain file (default: chain_cpu.txt)\n"
+              << "  --nthreads <N>             Host thread count (accepted; the path runs on the GPU)\n"
+              << "  --edge-file <file>         Input edge file in ../test_files/ (default: eth3d_cables2.txt)\n"
+              << "  --nrad <val>               Neighbor search radius (default: 3.5)\n"
+              << "  --dx <val>                 Edge position tolerance in pixels (default: 0.4)\n"
+              << "  --dt-deg <val>             Edge angle tolerance in degrees (default: 15)\n"
+              << "  --max-k <val>              Maximum curvature (default: 0.3)\n"
+              << "  --curvelet-style <N>       Curvelet style (default: 2)\n"
+              << "  --group-max-sz <N>         Maximum group size (default: 4)\n"
+              << "  --out-type <N>             Output type (default: 0)\n"
+              << "  --sx <val>                 Position sampling step (default: 0.1)\n"
+              << "  --st <val>                 Angle sampling step in radians (default: 0.08)\n"
+              << "  --edge-data-sz <N>         Values per edge in input file (default: 4)\n"
+              << "  --max-candidates <N>       Max neighbors per anchor in CSR build (default: 128)\n"
+              << "  --help                     Show this help message\n";
+}
+
+bool parse_num(const char *arg, const char *name, double &v) {
+    char *end = nullptr;
+    const double x = std::strtod(arg, &end);
+    if (end == arg || *end != '\0') {
+        std::cerr << "Error: invalid value for " << name << ": " << arg << std::endl;
+        return false;
+    }
+    v = x;
+    return true;
+}
+
+bool parse_uns(const char *arg, const char *name, unsigned &v) {
+    char *end = nullptr;
+    const unsigned long x = std::strtoul(arg, &end, 10);
+    if (end == arg || *end != '\0') {
+        std::cerr << "Error: invalid value for " << name << ": " << arg << std::endl;
+        return false;
+    }
+    v = (unsigned)x;
+    return true;
+}
+
+bool parse_int(const char *arg, const char *name, int &v) {
+    char *end = nullptr;
+    const long x = std::strtol(arg, &end, 10);
+    if (end == arg || *end != '\0') {
+        std::cerr << "Error: invalid value for " << name << ": " << arg << std::endl;
+        return false;
+    }
+    v = (int)x;
+    return true;
+}
+
+// Flag table of param_settings.hpp:86-155.
+bool parse_args(int argc, char **argv, CliParams &cp, bool &use_double, std::string &out_file, int &nthreads,
+                bool &show_help) {
+    show_help = false;
+    for (int i = 1; i < argc; i++) {
+        const char *a = argv[i];
+        auto next = [&](void) -> const char * { return argv[++i]; };
+        const bool has = (i + 1 < argc);
+        if (!std::strcmp(a, "--help") || !std::strcmp(a, "-h")) {
+            print_usage(argv[0]);
+            show_help = true;
+            return false;
+        }
+        if (!std::strcmp(a, "--float")) {
+            use_double = false;
+            out_file = "chain_cpu_float.txt";
+        } else if (!std::strcmp(a, "--double")) {
+            use_double = true;
+            out_file = "chain_cpu_double.txt";
+        } else if (!std::strcmp(a, "--output") && has) {
+            out_file = next();
+        } else if (!std::strcmp(a, "--nthreads") && has) {
+            nthreads = std::atoi(next());
+        } else if ((!std::strcmp(a, "--input") || !std::strcmp(a, "--edge-file")) && has) {
+            cp.edge_file = next();
+        } else if (!std::strcmp(a, "--nrad") && has) {
+            if (!parse_num(next(), "--nrad", cp.p.nrad)) return false;
+        } else if (!std::strcmp(a, "--dx") && has) {
+            if (!parse_num(next(), "--dx", cp.p.dx)) return false;
+        } else if (!std::strcmp(a, "--dt-deg") && has) {
+            if (!parse_num(next(), "--dt-deg", cp.p.dt_deg)) return false;
+        } else if (!std::strcmp(a, "--max-k") && has) {
+            if (!parse_num(next(), "--max-k", cp.p.max_k)) return false;
+        } else if (!std::strcmp(a, "--curvelet-style") && has) {
+            if (!parse_uns(next(), "--curvelet-style", cp.p.curvelet_style)) return false;
+        } else if (!std::strcmp(a, "--group-max-sz") && has) {
+            if (!parse_uns(next(), "--group-max-sz", cp.p.group_max_sz)) return false;
+        } else if (!std::strcmp(a, "--out-type") && has) {
+            if (!parse_uns(next(), "--out-type", cp.p.out_type)) return false;
+        } else if (!std::strcmp(a, "--sx") && has) {
+            if (!parse_num(next(), "--sx", cp.p.sx)) return false;
+        } else if (!std::strcmp(a, "--st") && has) {
+            if (!parse_num(next(), "--st", cp.p.st)) return false;
+        } else if (!std::strcmp(a, "--edge-data-sz") && has) {
+            if (!parse_int(next(), "--edge-data-sz", cp.p.edge_data_sz)) return false;
+        } else if (!std::strcmp(a, "--max-candidates") && has) {
+            if (!parse_uns(next(), "--max-candidates", cp.p.max_candidates)) return false;
+        } else {
+            std::cerr << "Unknown argument: " << a << std::endl;
+            print_usage(argv[0]);
+            return false;
+        }
+    }
+    return true;
+}
+
+bool blank(const std::string &s) { return s.find_first_not_of(" \t\r\n") == std::string::npos; }
+
+// Edge-file reader with the reference's acceptance rules (data_io.hpp:22-79).
+bool read_edges(const std::string &filename, int per_edge, std::vector<double> &out) {
+    const std::string path = "../test_files/" + filename;
+    std::ifstream in(path);
+    if (!in) {
+        std::cerr << "Error: input file does not exist: " << path << std::endl;
+        return false;
+    }
+    std::cout << "reading data from file " << filename << std::endl;
+    out.clear();
+    std::string line;
+    int ln = 0, count = 0;
+    while (std::getline(in, line)) {
+        ++ln;
+        if (blank(line)) {
+            std::cerr << "Error: blank line at line " << ln << " in " << path << " (each line must contain exactly "
+                      << per_edge << " numeric values)" << std::endl;
+            out.clear();
+            return false;
+        }
+        std::istringstream iss(line);
+        for (int j = 0; j < per_edge; j++) {
+            double v;
+            if (!(iss >> v)) {
+                std::cerr << "Error: invalid edge file format in " << path << " at line " << ln << ": expected "
+                          << per_edge << " numeric values per line, found " << j << "." << std::endl;
+                out.clear();
+                return false;
+            }
+            out.push_back(v);
+        }
+        std::string rest;
+        std::getline(iss, rest);
+        if (!blank(rest)) {
+            std::cerr << "Error: invalid edge file format in " << path << " at line " << ln << ": expected exactly "
+                      << per_edge << " numeric values per line, found extra data." << std::endl;
+            out.clear();
+            return false;
+        }
+        ++count;
+    }
+    if (count == 0) {
+        std::cerr << "Error: input file contains no valid edges: " << path << std::endl;
+        out.clear();
+        return false;
+    }
+    std::cout << "read " << count << " edges from " << filename << std::endl;
+    return true;
+}
+
+bool open_out(const std::string &name, std::ofstream &f) {
+    std::cout << "writing data to a file " << name << " ..." << std::endl;
+    const std::filesystem::path dir = "../outputs";
+    std::error_code ec;
+    std::filesystem::create_directories(dir, ec);
+    if (ec) {
+        std::cerr << "Failed to create output directory " << dir << ": " << ec.message() << std::endl;
+        return false;
+    }
+    f.open(dir.string() + "/" + name);
+    if (!f.is_open()) std::cout << "write data file cannot be opened!" << std::endl;
+    return true;
+}
+
+std::string info_name(const std::string &chain_file) {  // data_io.hpp:136-145
+    const std::size_t pos = chain_file.find("chain");
+    if (pos != std::string::npos) {
+        std::string s = chain_file;
+        s.replace(pos, 5, "info");
+        return s;
+    }
+    return "info_" + chain_file;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    int nthreads = 1;
+    bool use_double = true;
+    std::string out_file = "chain_cpu.txt";
+    CliParams cp;
+    cvl_params_default(&cp.p);
+    bool help = false;
+    if (!parse_args(argc, argv, cp, use_double, out_file, nthreads, help)) return help ? 0 : 1;
+    (void)nthreads;
+    if (!use_double) {
+        std::cerr << "Error: --float is not available: the B200 engine computes the path in double precision"
+                  << std::endl;
+        return 1;
+    }
+    std::cout << "Using scalar type: double" << std::endl;
+    std::vector<double> edges;
+    if (!read_edges(cp.edge_file, cp.p.edge_data_sz, edges)) return 1;
+    const int n = (int)(edges.size() / (size_t)cp.p.edge_data_sz);
+
+    cvl_engine *eng = nullptr;
+    if (cvl_engine_create(nullptr, &eng) != CVL_OK) {
+        std::cerr << "Error: " << cvl_last_error() << std::endl;
+        return 1;
+    }
+    cvl_result *res = nullptr;
+    if (cvl_run(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &res) != CVL_OK) {
+        std::cerr << "Error: " << cvl_last_error() << std::endl;
+        cvl_engine_destroy(eng);
+        return 1;
+    }
+    cvl_result_view v;
+    cvl_result_get(res, &v);
+    if (v.truncated_anchors)
+        std::cerr << "Warning: " << v.truncated_anchors << " anchors hit max_candidates=" << cp.p.max_candidates
+                  << "; neighbor lists may be truncated\n";
+    std::cout << "CSR neighbor graph: " << n << " anchors, " << v.total_neighbor_pairs
+              << " total pairs, max number of neighbors per anchor: " << v.max_num_of_neighbors << std::endl;
+    std::cout << "Pairwise curve bundles formed: " << v.valid_pairs << " valid pairs" << std::endl;
+    std::cout << "- Time of curvelet building (GPU, device): " << v.device_ms << " (ms)" << std::endl;
+    std::cout << "- Number of curvelets formed: " << v.num_curvelets << std::endl;
+    const unsigned out_h = v.num_curvelets, out_w = v.chain_width;
+    std::cout << "(out_h, out_w) = (" << out_h << ", " << out_w << ")" << std::endl;
+
+    {
+        std::ofstream f;
+        if (open_out(out_file, f)) {
+            for (unsigned i = 0; i < out_h; i++) {
+                for (unsigned j = 0; j < out_w; j++) f << (int)v.chains[(size_t)i * out_w + j] << "\t";
+                f << "\n";
+            }
+        }
+    }
+    {
+        std::ofstream f;
+        if (open_out(info_name(out_file), f)) {
+            for (unsigned i = 0; i < out_h; i++) {
+                for (unsigned j = 0; j < 10; j++) f << v.info[(size_t)i * 10 + j] << "\t";
+                f << "\n";
+            }
+        }
+    }
+    cvl_result_free(res);
+    cvl_engine_destroy(eng);
+    return 0;
+}

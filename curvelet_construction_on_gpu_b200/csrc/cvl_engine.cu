@@ -1,0 +1,1008 @@
+// cvl_engine.cu -- host engine and C ABI (include/cvl.h) of the curvelet path.
+//
+// One engine = one CUDA device + one stream + a grow-only device workspace.
+// A run over a ragged batch of maps (a single map for the plain form):
+//   H2D edges -> (a) binning -> (b) neighbour count, scan -> [sync: pair total]
+//   -> (b) neighbour fill -> (c+d) fused bundles/growth/dedup/record
+//   -> scan of per-anchor counts -> [sync: curvelet total] -> (e) finalize -> D2H
+// The two syncs size the CSR/record and output buffers exactly; everything
+// else stays on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cvl.h"
+#include "cvl_kernels.cuh"
+#include "cvl_scan.cuh"
+
+using namespace cvl;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CVL_CUDA(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) return fail(CVL_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CVL_TRY(call)              \
+    do {                           \
+        int rc_ = (call);          \
+        if (rc_ != CVL_OK) return rc_; \
+    } while (0)
+
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+inline unsigned next_pow2(unsigned long long v) {
+    unsigned long long p = 1;
+    while (p < v) p <<= 1;
+    return (unsigned)p;
+}
+
+}  // namespace
+
+struct cvl_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaDeviceProp prop{};
+    size_t budget = 0;
+    size_t held = 0;
+    int cell_size = 4;
+    int seeds_per_group = 4;
+    int slots = 10;
+    unsigned long long generation = 0;
+
+    // workspace
+    DBuf edges, map_off, ehash, bcount, bstart, bfill, pos_of, orig_of;
+    DBuf bx, by, bth, bsp, bcp, bsm, bcm, bcell, bmap;
+    DBuf ncand, deg, pair_off, csr_ids, csr_d2, rec_ids, rec_k, rec_meta, count, out_off;
+    DBuf chains, info, stats, err, work, scratch, scratch_chain, scan_tmp, flush, deg_orig, off_orig, gids, gd2;
+    DBuf pairs_in, pb_min, pb_max, pb_valid;
+
+    // per-kernel timing of the last run
+    std::vector<const char *> mark_names;
+    std::vector<cudaEvent_t> marks;
+    size_t nmarks = 0;
+    std::vector<std::pair<const char *, double>> last_times;
+    double last_device_ms = 0.0;
+
+    int alloc(DBuf &b, size_t bytes) {
+        if (bytes == 0) bytes = 16;
+        if (b.bytes >= bytes) return CVL_OK;
+        size_t want = std::max(bytes, b.bytes + b.bytes / 4);
+        want = (want + 255) & ~(size_t)255;
+        if (b.p) {
+            cudaFree(b.p);
+            held -= b.bytes;
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        if (budget && held + want > budget) {
+            want = bytes;
+            if (held + want > budget)
+                return fail(CVL_ENOMEM, "device memory budget exceeded (" + std::to_string(held + want) + " > " +
+                                            std::to_string(budget) + " bytes)");
+        }
+        cudaError_t e = cudaMalloc(&b.p, want);
+        if (e != cudaSuccess) {
+            b.p = nullptr;
+            cudaGetLastError();
+            return fail(CVL_ENOMEM, std::string("cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e));
+        }
+        b.bytes = want;
+        held += want;
+        return CVL_OK;
+    }
+
+    void mark(const char *name) {
+        if (nmarks == marks.size()) {
+            cudaEvent_t ev;
+            cudaEventCreate(&ev);
+            marks.push_back(ev);
+            mark_names.push_back(name);
+        }
+        mark_names[nmarks] = name;
+        cudaEventRecord(marks[nmarks], stream);
+        ++nmarks;
+    }
+
+    void collect_marks() {
+        last_times.clear();
+        last_device_ms = 0.0;
+        if (nmarks < 2) return;
+        cudaEventSynchronize(marks[nmarks - 1]);
+        for (size_t k = 1; k < nmarks; ++k) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, marks[k - 1], marks[k]);
+            last_times.emplace_back(mark_names[k], (double)ms);
+        }
+        float tot = 0.f;
+        cudaEventElapsedTime(&tot, marks[0], marks[nmarks - 1]);
+        last_device_ms = tot;
+    }
+
+    void release_all() {
+        DBuf *all[] = {&edges, &map_off, &ehash, &bcount, &bstart, &bfill, &pos_of, &orig_of, &bx, &by, &bth, &bsp,
+                       &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
+                       &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
+                       &scratch_chain, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
+                       &pb_max, &pb_valid};
+        for (DBuf *b : all) {
+            if (b->p) cudaFree(b->p);
+            b->p = nullptr;
+            b->bytes = 0;
+        }
+        held = 0;
+    }
+};
+
+struct cvl_result {
+    std::vector<uint32_t> chains;
+    std::vector<double> info;
+    cvl_result_view v{};
+};
+
+struct cvl_graph {
+    std::vector<double> edges;  // AoS copy, edge_data_sz per row
+    int sz = 4;
+    int n = 0;
+    double rad = 3.5;
+    unsigned neighbor_radius = 3;
+    unsigned max_candidates = 128;
+    std::vector<int32_t> offsets, ids;
+    std::vector<double> d2;
+    cvl_graph_view v{};
+};
+
+struct cvl_batch {
+    cvl_engine *eng = nullptr;
+    void *d_edges = nullptr;
+    void *d_map_off = nullptr;
+    int num_maps = 0;
+    int sz = 4;
+    int n = 0;
+    std::vector<int32_t> map_off;
+};
+
+struct cvl_batch_result {
+    cvl_engine *eng = nullptr;
+    unsigned long long generation = 0;
+    int num_maps = 0;
+    int n = 0;
+    int width = 0;
+    std::vector<int32_t> map_off;
+    std::vector<MapStats> stats;
+    std::vector<unsigned long long> cv_off;  // per-map curvelet offsets [M+1]
+    double device_ms = 0.0;
+    bool downloaded = false;
+    std::vector<uint32_t> chains;
+    std::vector<double> info;
+    bool truncated_any = false;
+};
+
+namespace {
+
+// ---- parameters -> model ---------------------------------------------------
+int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nbr_radius, unsigned max_cand, Model &md,
+               int &cpl) {
+    if (!p) return fail(CVL_EINVAL, "params is NULL");
+    if (!(p->sx > 0) || !(p->st > 0)) return fail(CVL_EINVAL, "sx and st must be > 0");
+    if (!std::isfinite(p->dx) || !std::isfinite(p->dt_deg) || !std::isfinite(p->dt_rad) || !std::isfinite(p->max_k) || !std::isfinite(p->nrad) ||
+        !std::isfinite(rad))
+        return fail(CVL_EINVAL, "non-finite parameter");
+    if (p->group_max_sz < 1 || p->group_max_sz > (unsigned)GMS_MAX)
+        return fail(CVL_EUNSUPPORTED, "group_max_sz must be in [1, 16]");
+    if (max_cand < 1 || max_cand > 1024) return fail(CVL_EUNSUPPORTED, "max_candidates must be in [1, 1024]");
+    if (nbr_radius > 64) return fail(CVL_EUNSUPPORTED, "neighbor_radius must be <= 64");
+    md.nrad = p->nrad;
+    md.rad_sqr = rad * rad;  // rad * rad (preprocess.hpp:221)
+    md.dx = p->dx;
+    md.dx2 = p->dx * p->dx;
+    md.four_dx_dx = 4 * p->dx * p->dx;
+    md.dt = (p->dt_rad > 0) ? p->dt_rad : (double)(p->dt_deg / 180.0) * (double)CVL_PI;  // main.cpp:24
+    md.sx = p->sx;
+    md.st = p->st;
+    md.max_k = p->max_k;
+    const double Pd = 2 * std::floor(md.dx / md.sx + 0.5) + 1;  // cpu_curvelet.hpp:73
+    const double Qd = 2 * std::floor(md.dt / md.st + 0.5) + 1;  // cpu_curvelet.hpp:74
+    if (!(Pd >= 1 && Pd <= 128 && Qd >= 1 && Qd <= QMAX))
+        return fail(CVL_EUNSUPPORTED, "bundle grid out of range (P <= 128, Q <= 32 required)");
+    md.P = (int)Pd;
+    md.Q = (int)Qd;
+    md.cells = md.P * md.Q;
+    if (md.cells > 128) return fail(CVL_EUNSUPPORTED, "bundle grid larger than 128 cells");
+    cpl = (md.cells + 31) / 32;
+    md.gms = (int)p->group_max_sz;
+    md.max_cand = (int)max_cand;
+    md.w = (int)nbr_radius;
+    md.S = e->cell_size > 0 ? e->cell_size : 4;
+    md.hash_mask = 0;
+    return CVL_OK;
+}
+
+int check_launch(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(CVL_ECUDA, std::string("launch ") + what + ": " + cudaGetErrorString(e));
+    return CVL_OK;
+}
+
+inline int grid_for(const cvl_engine *e, long long n, int threads, int per_sm = 16) {
+    long long g = (n + threads - 1) / threads;
+    const long long cap = (long long)e->prop.multiProcessorCount * per_sm;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+// ---- scans -------------------------------------------------------------------
+template <typename TIn, typename TOut>
+int scan_rec(cvl_engine *e, const TIn *in, size_t n, TOut *out, char *&tmp, size_t &left) {
+    if (n == 0) {
+        CVL_CUDA(cudaMemsetAsync(out, 0, sizeof(TOut), e->stream));
+        return CVL_OK;
+    }
+    const size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb == 1) {
+        k_scan_tiles<TIn, TOut><<<1, SCAN_THREADS, 0, e->stream>>>(in, n, nullptr, out);
+        return check_launch("k_scan_tiles");
+    }
+    const size_t need = (2 * nb + 1) * sizeof(TOut);
+    if (need > left) return fail(CVL_EOVERFLOW, "scan temp too small");
+    TOut *sums = (TOut *)tmp;
+    TOut *offs = sums + nb;
+    tmp += need;
+    left -= need;
+    k_scan_reduce<TIn, TOut><<<(unsigned)nb, SCAN_THREADS, 0, e->stream>>>(in, n, sums);
+    CVL_TRY(check_launch("k_scan_reduce"));
+    CVL_TRY((scan_rec<TOut, TOut>(e, sums, nb, offs, tmp, left)));
+    k_scan_tiles<TIn, TOut><<<(unsigned)nb, SCAN_THREADS, 0, e->stream>>>(in, n, offs, out);
+    return check_launch("k_scan_tiles");
+}
+
+template <typename TIn, typename TOut>
+int scan(cvl_engine *e, const TIn *in, size_t n, TOut *out) {
+    const size_t tmp_bytes = (n / SCAN_TILE + 64) * 4 * sizeof(unsigned long long) + 4096;
+    CVL_TRY(e->alloc(e->scan_tmp, tmp_bytes));
+    char *tmp = (char *)e->scan_tmp.p;
+    size_t left = e->scan_tmp.bytes;
+    return scan_rec<TIn, TOut>(e, in, n, out, tmp, left);
+}
+
+// ---- the pipeline -------------------------------------------------------------
+struct RunOut {
+    std::vector<MapStats> stats;
+    std::vector<unsigned long long> cv_off;  // per map
+    unsigned long long total_pairs = 0;
+    unsigned long long total_curvelets = 0;
+    unsigned max_deg = 0;
+};
+
+template <int CPL, int K>
+int launch_curvelets(cvl_engine *e, CurveletArgs &a, size_t per_warp, int blocks) {
+    const int threads = 128;
+    const size_t smem = per_warp * (threads / 32);
+    CVL_CUDA(cudaFuncSetAttribute(k_curvelets<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_curvelets<CPL, K><<<blocks, threads, smem, e->stream>>>(a);
+    return check_launch("k_curvelets");
+}
+
+template <int CPL, int K>
+int occupancy_curvelets(size_t smem, int &blocks_per_sm) {
+    CVL_CUDA(cudaFuncSetAttribute(k_curvelets<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CVL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_curvelets<CPL, K>, 128, smem));
+    return CVL_OK;
+}
+
+typedef int (*launch_fn)(cvl_engine *, CurveletArgs &, size_t, int);
+typedef int (*occ_fn)(size_t, int &);
+
+void pick_curvelet_kernel(int cpl, int K, launch_fn &lf, occ_fn &of) {
+#define CVL_PICK(C, KK)                        \
+    if (cpl == C && K == KK) {                 \
+        lf = launch_curvelets<C, KK>;          \
+        of = occupancy_curvelets<C, KK>;       \
+        return;                                \
+    }
+    CVL_PICK(1, 4) CVL_PICK(1, 8) CVL_PICK(2, 4) CVL_PICK(2, 8) CVL_PICK(3, 4) CVL_PICK(3, 8) CVL_PICK(4, 4)
+    CVL_PICK(4, 8)
+#undef CVL_PICK
+    lf = launch_curvelets<2, 4>;
+    of = occupancy_curvelets<2, 4>;
+}
+
+// mode: 0 = full run, 1 = count valid pairs only, 2 = neighbour graph only
+int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int *d_map_off,
+                 const std::vector<int32_t> &map_off_host, Model md, int cpl, int mode, bool want_d2, RunOut &ro) {
+    const int M = (int)map_off_host.size() - 1;
+    cudaStream_t s = e->stream;
+    e->nmarks = 0;
+    ++e->generation;
+    e->mark("start");
+
+    const unsigned T = next_pow2(std::max<unsigned long long>((unsigned long long)n, 1024ull));
+    md.hash_mask = T - 1;
+
+    // ---- workspace for N-sized arrays
+    CVL_TRY(e->alloc(e->ehash, sizeof(unsigned) * n));
+    CVL_TRY(e->alloc(e->bcount, sizeof(unsigned) * (T + 1)));
+    CVL_TRY(e->alloc(e->bstart, sizeof(unsigned) * (T + 1)));
+    CVL_TRY(e->alloc(e->bfill, sizeof(unsigned) * (T + 1)));
+    CVL_TRY(e->alloc(e->pos_of, sizeof(int) * n));
+    CVL_TRY(e->alloc(e->bx, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->by, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->bth, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->bsp, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->bcp, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->bsm, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->bcm, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->bcell, sizeof(int2) * n));
+    CVL_TRY(e->alloc(e->orig_of, sizeof(int) * n));
+    CVL_TRY(e->alloc(e->bmap, sizeof(int) * n));
+    CVL_TRY(e->alloc(e->ncand, sizeof(unsigned) * n));
+    CVL_TRY(e->alloc(e->deg, sizeof(unsigned) * n));
+    CVL_TRY(e->alloc(e->pair_off, sizeof(unsigned long long) * (n + 1)));
+    CVL_TRY(e->alloc(e->count, sizeof(unsigned) * n));
+    CVL_TRY(e->alloc(e->out_off, sizeof(unsigned long long) * (n + 1)));
+    CVL_TRY(e->alloc(e->stats, sizeof(MapStats) * M));
+    CVL_TRY(e->alloc(e->err, sizeof(unsigned) * 4));
+    CVL_TRY(e->alloc(e->work, sizeof(unsigned) * 4));
+
+    Binned B;
+    B.x = (double *)e->bx.p;
+    B.y = (double *)e->by.p;
+    B.th = (double *)e->bth.p;
+    B.sp = (double *)e->bsp.p;
+    B.cp = (double *)e->bcp.p;
+    B.sm = (double *)e->bsm.p;
+    B.cm = (double *)e->bcm.p;
+    B.cell = (int2 *)e->bcell.p;
+    B.orig = (int *)e->orig_of.p;
+    B.map = (int *)e->bmap.p;
+    unsigned *err = (unsigned *)e->err.p;
+    MapStats *stats = (MapStats *)e->stats.p;
+
+    CVL_CUDA(cudaMemsetAsync(e->bcount.p, 0, sizeof(unsigned) * (T + 1), s));
+    CVL_CUDA(cudaMemsetAsync(e->bfill.p, 0, sizeof(unsigned) * (T + 1), s));
+    CVL_CUDA(cudaMemsetAsync(e->stats.p, 0, sizeof(MapStats) * M, s));
+    CVL_CUDA(cudaMemsetAsync(e->err.p, 0, sizeof(unsigned) * 4, s));
+    CVL_CUDA(cudaMemsetAsync(e->work.p, 0, sizeof(unsigned) * 4, s));
+    CVL_CUDA(cudaMemsetAsync(e->count.p, 0, sizeof(unsigned) * n, s));
+
+    // ---- (a) binning
+    const int gb = grid_for(e, n, 256);
+    k_bin_keys<<<gb, 256, 0, s>>>(d_edges, sz, n, d_map_off, M, md, (unsigned *)e->ehash.p, (unsigned *)e->bcount.p,
+                                  err);
+    CVL_TRY(check_launch("k_bin_keys"));
+    CVL_TRY((scan<unsigned, unsigned>(e, (const unsigned *)e->bcount.p, T, (unsigned *)e->bstart.p)));
+    k_bin_scatter<<<gb, 256, 0, s>>>(d_edges, sz, n, d_map_off, M, md, (const unsigned *)e->ehash.p,
+                                     (const unsigned *)e->bstart.p, (unsigned *)e->bfill.p, B, (int *)e->pos_of.p);
+    CVL_TRY(check_launch("k_bin_scatter"));
+    e->mark("bin");
+
+    // ---- (b) neighbour count + CSR offsets
+    const int nb_wpb = 8;
+    const size_t nb_smem = (size_t)nb_wpb * md.max_cand * 20;
+    if (nb_smem > 48 * 1024) {
+        CVL_CUDA(cudaFuncSetAttribute(k_neighbors<NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
+        CVL_CUDA(cudaFuncSetAttribute(k_neighbors<NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
+    }
+    const int gn = grid_for(e, n, nb_wpb, 16);
+    k_neighbors<NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(md, B, (const unsigned *)e->bstart.p, n,
+                                                           (unsigned *)e->ncand.p, stats, nullptr, nullptr, nullptr,
+                                                           err);
+    CVL_TRY(check_launch("k_neighbors<COUNT>"));
+    k_deg_from_ncand<<<gb, 256, 0, s>>>(n, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p);
+    CVL_TRY(check_launch("k_deg_from_ncand"));
+    CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->deg.p, n,
+                                                (unsigned long long *)e->pair_off.p)));
+    e->mark("neighbors_count");
+
+    // sync 1: totals
+    ro.stats.assign(M, MapStats{});
+    unsigned h_err = 0;
+    CVL_CUDA(cudaMemcpyAsync(&ro.total_pairs, (unsigned long long *)e->pair_off.p + n, sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaStreamSynchronize(s));
+    if (h_err & ERR_NONFINITE) return fail(CVL_EINVAL, "non-finite or out-of-range (|v| >= 1e9) edge coordinate");
+    ro.max_deg = 0;
+    for (const MapStats &st : ro.stats) ro.max_deg = std::max(ro.max_deg, st.max_deg);
+    const unsigned long long P = ro.total_pairs;
+
+    // ---- (b) neighbour fill
+    CVL_TRY(e->alloc(e->csr_ids, sizeof(int) * P));
+    if (want_d2) CVL_TRY(e->alloc(e->csr_d2, sizeof(double) * P));
+    k_neighbors<NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(md, B, (const unsigned *)e->bstart.p, n,
+                                                          (unsigned *)e->ncand.p, stats,
+                                                          (const unsigned long long *)e->pair_off.p,
+                                                          (int *)e->csr_ids.p, want_d2 ? (double *)e->csr_d2.p : nullptr,
+                                                          err);
+    CVL_TRY(check_launch("k_neighbors<FILL>"));
+    e->mark("neighbors_fill");
+    if (mode == 2) {
+        e->mark("end");
+        return CVL_OK;
+    }
+
+    // ---- (c+d) fused bundles + growth
+    launch_fn lf;
+    occ_fn of;
+    const int K = (e->seeds_per_group == 8) ? 8 : 4;
+    pick_curvelet_kernel(cpl, K, lf, of);
+    int slots = e->slots > 0 ? e->slots : 10;
+    size_t per_warp = curvelet_smem_per_warp(md.max_cand, slots, md.gms, cpl);
+    while (per_warp * 4 > (size_t)e->prop.sharedMemPerBlockOptin && slots > 1) {
+        --slots;
+        per_warp = curvelet_smem_per_warp(md.max_cand, slots, md.gms, cpl);
+    }
+    int bps = 0;
+    CVL_TRY(of(per_warp * 4, bps));
+    if (bps < 1) return fail(CVL_EUNSUPPORTED, "k_curvelets does not fit on an SM with these parameters");
+    const int blocks = bps * e->prop.multiProcessorCount;
+    const int warps = blocks * 4;
+    const int scratch_deg = (int)ro.max_deg > slots ? (int)ro.max_deg - slots : 0;
+    CVL_TRY(e->alloc(e->scratch, sizeof(double) * (size_t)warps * (size_t)std::max(scratch_deg, 1) * 64 * cpl));
+    CVL_TRY(e->alloc(e->scratch_chain, sizeof(unsigned short) * (size_t)warps * (size_t)std::max(scratch_deg, 1) *
+                                           (size_t)md.gms));
+    if (mode == 0) {
+        CVL_TRY(e->alloc(e->rec_ids, sizeof(unsigned) * P * md.gms));
+        CVL_TRY(e->alloc(e->rec_k, sizeof(double) * P * 2));
+        CVL_TRY(e->alloc(e->rec_meta, sizeof(unsigned) * P));
+    }
+    CurveletArgs a;
+    a.md = md;
+    a.B = B;
+    a.N = n;
+    a.pair_off = (const unsigned long long *)e->pair_off.p;
+    a.csr_ids = (const int *)e->csr_ids.p;
+    a.rec.ids = (unsigned *)e->rec_ids.p;
+    a.rec.k = (double *)e->rec_k.p;
+    a.rec.meta = (unsigned *)e->rec_meta.p;
+    a.count = (unsigned *)e->count.p;
+    a.stats = stats;
+    a.work = (unsigned *)e->work.p;
+    a.scratch = (double *)e->scratch.p;
+    a.scratch_chain = (unsigned short *)e->scratch_chain.p;
+    a.scratch_deg = scratch_deg;
+    a.slots = slots;
+    a.count_only = (mode == 1) ? 1 : 0;
+    a.err = err;
+    CVL_TRY(lf(e, a, per_warp, blocks));
+    e->mark("curvelets");
+
+    if (mode == 1) {
+        CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        e->mark("end");
+        CVL_CUDA(cudaStreamSynchronize(s));
+        if (h_err) return fail(CVL_EOVERFLOW, "kernel reported error bits " + std::to_string(h_err));
+        return CVL_OK;
+    }
+
+    // ---- output positions (anchor-major, compact_curvelet_output)
+    CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->count.p, n,
+                                                (unsigned long long *)e->out_off.p)));
+    ro.cv_off.assign(M + 1, 0);
+    {
+        // per-map curvelet offsets are out_off at the map boundaries
+        std::vector<unsigned long long> tmp(M + 1);
+        for (int m = 0; m <= M; ++m) {
+            CVL_CUDA(cudaMemcpyAsync(&tmp[m], (unsigned long long *)e->out_off.p + map_off_host[m],
+                                     sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        }
+        CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaStreamSynchronize(s));
+        ro.cv_off = tmp;
+    }
+    if (h_err) return fail(CVL_EOVERFLOW, "kernel reported error bits " + std::to_string(h_err));
+    const unsigned long long C = ro.cv_off[M];
+    ro.total_curvelets = C;
+    const int W = md.gms + 1;
+    CVL_TRY(e->alloc(e->chains, sizeof(unsigned) * C * W));
+    CVL_TRY(e->alloc(e->info, sizeof(double) * C * 10));
+    k_finalize<<<gb, 256, 0, s>>>(md, d_edges, sz, n, d_map_off, M, (const int *)e->orig_of.p,
+                                  (const unsigned long long *)e->pair_off.p, a.rec, (const unsigned *)e->count.p,
+                                  (const unsigned long long *)e->out_off.p, (unsigned *)e->chains.p,
+                                  (double *)e->info.p);
+    CVL_TRY(check_launch("k_finalize"));
+    e->mark("finalize");
+    return CVL_OK;
+}
+
+int upload(cvl_engine *e, const double *edges, int n, int sz, const std::vector<int32_t> &map_off) {
+    CVL_TRY(e->alloc(e->edges, sizeof(double) * (size_t)n * sz));
+    CVL_TRY(e->alloc(e->map_off, sizeof(int) * map_off.size()));
+    CVL_CUDA(cudaMemcpyAsync(e->edges.p, edges, sizeof(double) * (size_t)n * sz, cudaMemcpyHostToDevice, e->stream));
+    CVL_CUDA(cudaMemcpyAsync(e->map_off.p, map_off.data(), sizeof(int) * map_off.size(), cudaMemcpyHostToDevice,
+                             e->stream));
+    return CVL_OK;
+}
+
+int check_edges_args(const double *edges, int32_t n, int32_t sz) {
+    if (n <= 0 || sz < 4 || edges == nullptr)  // preprocess.hpp:197-199
+        return fail(CVL_EINVAL, "num_edges must be > 0, edge_data_sz >= 4 and edges non-NULL");
+    return CVL_OK;
+}
+
+int fill_view_from_run(cvl_engine *e, const RunOut &ro, int n, int width, cvl_result *r) {
+    const unsigned long long C = ro.total_curvelets;
+    r->chains.resize(C * width);
+    r->info.resize(C * 10);
+    if (C) {
+        CVL_CUDA(cudaMemcpyAsync(r->chains.data(), e->chains.p, sizeof(unsigned) * C * width, cudaMemcpyDeviceToHost,
+                                 e->stream));
+        CVL_CUDA(cudaMemcpyAsync(r->info.data(), e->info.p, sizeof(double) * C * 10, cudaMemcpyDeviceToHost,
+                                 e->stream));
+    }
+    CVL_CUDA(cudaStreamSynchronize(e->stream));
+    cvl_result_view &v = r->v;
+    v.num_curvelets = (uint32_t)C;
+    v.chain_width = (uint32_t)width;
+    v.chains = r->chains.data();
+    v.info = r->info.data();
+    v.valid_pairs = ro.stats.empty() ? 0 : ro.stats[0].valid_pairs;
+    v.total_neighbor_pairs = (int64_t)ro.total_pairs;
+    v.max_num_of_neighbors = ro.max_deg;
+    v.truncated_anchors = ro.stats.empty() ? 0 : ro.stats[0].truncated;
+    v.num_edges = (uint32_t)n;
+    v.flags = v.truncated_anchors ? CVL_FLAG_TRUNCATED : 0u;
+    v.device_ms = e->last_device_ms;
+    return CVL_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+// C ABI
+// =============================================================================
+extern "C" {
+
+void cvl_params_default(cvl_params *p) {
+    if (!p) return;
+    p->nrad = 3.5;
+    p->gap = 1.5;
+    p->dx = 0.4;
+    p->dt_deg = 15.0;
+    p->dt_rad = 0.0;
+    p->max_k = 0.3;
+    p->curvelet_style = 2;
+    p->group_max_sz = 4;
+    p->out_type = 0;
+    p->sx = 0.1;
+    p->st = 0.08;
+    p->edge_data_sz = 4;
+    p->max_candidates = 128;
+}
+
+void cvl_engine_cfg_default(cvl_engine_cfg *c) {
+    if (!c) return;
+    c->device = 0;
+    c->mem_budget_bytes = 0;
+    c->cell_size = 0;
+    c->seeds_per_group = 0;
+    c->bundle_slots = 0;
+    c->warps_per_block = 0;
+}
+
+const char *cvl_last_error(void) { return g_err.c_str(); }
+
+const char *cvl_version(void) { return "cvl 0.1.0 (sm_100a, FP64)"; }
+
+int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out) {
+    if (!out) return fail(CVL_EINVAL, "out is NULL");
+    *out = nullptr;
+    cvl_engine_cfg c;
+    cvl_engine_cfg_default(&c);
+    if (cfg) c = *cfg;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(CVL_ENODEV, "no CUDA device");
+    }
+    if (c.device < 0 || c.device >= ndev) return fail(CVL_EINVAL, "device ordinal out of range");
+    cvl_engine *e = new cvl_engine();
+    e->device = c.device;
+    e->budget = c.mem_budget_bytes;
+    e->cell_size = c.cell_size > 0 ? c.cell_size : 4;
+    e->seeds_per_group = (c.seeds_per_group == 8) ? 8 : 4;
+    e->slots = c.bundle_slots > 0 ? c.bundle_slots : 10;
+    cudaError_t ce = cudaSetDevice(e->device);
+    if (ce == cudaSuccess) ce = cudaGetDeviceProperties(&e->prop, e->device);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+        delete e;
+        return fail(CVL_ECUDA, std::string("engine init: ") + cudaGetErrorString(ce));
+    }
+    if (e->prop.major < 10) {
+        cudaStreamDestroy(e->stream);
+        delete e;
+        return fail(CVL_ENODEV, "device is not sm_100 class (the library is built for sm_100a only)");
+    }
+    *out = e;
+    return CVL_OK;
+}
+
+void cvl_engine_destroy(cvl_engine *e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    e->release_all();
+    for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
+    cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz, const cvl_params *p,
+            cvl_result **out) {
+    if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
+    *out = nullptr;
+    CVL_TRY(check_edges_args(edges, num_edges, edge_data_sz));
+    CVL_CUDA(cudaSetDevice(e->device));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
+    std::vector<int32_t> mo = {0, num_edges};
+    CVL_TRY(upload(e, edges, num_edges, edge_data_sz, mo));
+    RunOut ro;
+    CVL_TRY(run_pipeline(e, (const double *)e->edges.p, num_edges, edge_data_sz, (const int *)e->map_off.p, mo, md,
+                         cpl, 0, false, ro));
+    e->collect_marks();
+    cvl_result *r = new cvl_result();
+    int rc = fill_view_from_run(e, ro, num_edges, md.gms + 1, r);
+    if (rc != CVL_OK) {
+        delete r;
+        return rc;
+    }
+    *out = r;
+    return CVL_OK;
+}
+
+int cvl_result_get(const cvl_result *r, cvl_result_view *view) {
+    if (!r || !view) return fail(CVL_EINVAL, "result/view is NULL");
+    *view = r->v;
+    return CVL_OK;
+}
+
+void cvl_result_free(cvl_result *r) { delete r; }
+
+int cvl_build_neighbor_graph(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz, double rad,
+                             unsigned neighbor_radius, unsigned max_candidates, cvl_graph **out) {
+    if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
+    *out = nullptr;
+    CVL_TRY(check_edges_args(edges, num_edges, edge_data_sz));
+    CVL_CUDA(cudaSetDevice(e->device));
+    cvl_params p;
+    cvl_params_default(&p);
+    p.nrad = rad;
+    p.max_candidates = max_candidates;
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, &p, rad, neighbor_radius, max_candidates, md, cpl));
+    std::vector<int32_t> mo = {0, num_edges};
+    CVL_TRY(upload(e, edges, num_edges, edge_data_sz, mo));
+    RunOut ro;
+    CVL_TRY(run_pipeline(e, (const double *)e->edges.p, num_edges, edge_data_sz, (const int *)e->map_off.p, mo, md,
+                         cpl, 2, true, ro));
+    if (ro.total_pairs > 0x7fffffffull) return fail(CVL_EOVERFLOW, "more than 2^31 neighbour pairs");
+    const int n = num_edges;
+    const unsigned long long P = ro.total_pairs;
+    CVL_TRY(e->alloc(e->deg_orig, sizeof(unsigned) * n));
+    CVL_TRY(e->alloc(e->off_orig, sizeof(unsigned long long) * (n + 1)));
+    CVL_TRY(e->alloc(e->gids, sizeof(int) * P));
+    CVL_TRY(e->alloc(e->gd2, sizeof(double) * P));
+    const int gb = grid_for(e, n, 256);
+    k_graph_degrees<<<gb, 256, 0, e->stream>>>(n, (const int *)e->orig_of.p, (const unsigned long long *)e->pair_off.p,
+                                              (unsigned *)e->deg_orig.p);
+    CVL_TRY(check_launch("k_graph_degrees"));
+    CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->deg_orig.p, n,
+                                                (unsigned long long *)e->off_orig.p)));
+    k_graph_export<<<gb, 256, 0, e->stream>>>(n, (const int *)e->orig_of.p, (const int *)e->map_off.p, 1,
+                                             (const unsigned long long *)e->pair_off.p, (const int *)e->csr_ids.p,
+                                             (const double *)e->csr_d2.p, (const unsigned long long *)e->off_orig.p,
+                                             (int *)e->gids.p, (double *)e->gd2.p);
+    CVL_TRY(check_launch("k_graph_export"));
+    e->mark("export");
+    cvl_graph *g = new cvl_graph();
+    g->edges.assign(edges, edges + (size_t)n * edge_data_sz);
+    g->sz = edge_data_sz;
+    g->n = n;
+    g->rad = rad;
+    g->neighbor_radius = neighbor_radius;
+    g->max_candidates = max_candidates;
+    std::vector<unsigned long long> off(n + 1);
+    g->ids.resize(P);
+    g->d2.resize(P);
+    cudaMemcpyAsync(off.data(), e->off_orig.p, sizeof(unsigned long long) * (n + 1), cudaMemcpyDeviceToHost, e->stream);
+    if (P) {
+        cudaMemcpyAsync(g->ids.data(), e->gids.p, sizeof(int) * P, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(g->d2.data(), e->gd2.p, sizeof(double) * P, cudaMemcpyDeviceToHost, e->stream);
+    }
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) {
+        delete g;
+        return fail(CVL_ECUDA, std::string("graph download: ") + cudaGetErrorString(ce));
+    }
+    e->collect_marks();
+    g->offsets.resize(n + 1);
+    for (int i = 0; i <= n; ++i) g->offsets[i] = (int32_t)off[i];
+    g->v.num_edges = n;
+    g->v.total_neighbor_pairs = (int64_t)P;
+    g->v.max_num_of_neighbors = ro.max_deg;
+    g->v.truncated_anchors = ro.stats[0].truncated;
+    g->v.neighbor_offsets = g->offsets.data();
+    g->v.neighbor_ids = g->ids.data();
+    g->v.neighbor_dist2 = g->d2.data();
+    *out = g;
+    return CVL_OK;
+}
+
+int cvl_graph_get(const cvl_graph *g, cvl_graph_view *view) {
+    if (!g || !view) return fail(CVL_EINVAL, "graph/view is NULL");
+    *view = g->v;
+    return CVL_OK;
+}
+
+void cvl_graph_free(cvl_graph *g) { delete g; }
+
+static int graph_pipeline(cvl_engine *e, const cvl_graph *g, const cvl_params *p, int mode, RunOut &ro, int &width) {
+    if (!e || !g) return fail(CVL_EINVAL, "engine/graph is NULL");
+    CVL_CUDA(cudaSetDevice(e->device));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, g->rad, g->neighbor_radius, g->max_candidates, md, cpl));
+    std::vector<int32_t> mo = {0, g->n};
+    CVL_TRY(upload(e, g->edges.data(), g->n, g->sz, mo));
+    CVL_TRY(run_pipeline(e, (const double *)e->edges.p, g->n, g->sz, (const int *)e->map_off.p, mo, md, cpl, mode,
+                         false, ro));
+    width = md.gms + 1;
+    return CVL_OK;
+}
+
+int cvl_form_pairwise_bundles(cvl_engine *e, const cvl_graph *g, const cvl_params *p, uint32_t *valid_pairs) {
+    if (!valid_pairs) return fail(CVL_EINVAL, "valid_pairs is NULL");
+    RunOut ro;
+    int width = 0;
+    CVL_TRY(graph_pipeline(e, g, p, 1, ro, width));
+    e->collect_marks();
+    *valid_pairs = ro.stats[0].valid_pairs;
+    return CVL_OK;
+}
+
+int cvl_build_curvelets(cvl_engine *e, const cvl_graph *g, const cvl_params *p, cvl_result **out) {
+    if (!out) return fail(CVL_EINVAL, "out is NULL");
+    *out = nullptr;
+    RunOut ro;
+    int width = 0;
+    CVL_TRY(graph_pipeline(e, g, p, 0, ro, width));
+    e->collect_marks();
+    cvl_result *r = new cvl_result();
+    int rc = fill_view_from_run(e, ro, g->n, width, r);
+    if (rc != CVL_OK) {
+        delete r;
+        return rc;
+    }
+    *out = r;
+    return CVL_OK;
+}
+
+int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p, double *bmin, double *bmax,
+                     uint8_t *valid, int32_t *cells) {
+    if (!e || !pairs || !bmin || !bmax || !valid || !cells || n < 0) return fail(CVL_EINVAL, "invalid argument");
+    CVL_CUDA(cudaSetDevice(e->device));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? std::max(p->max_candidates, 1u) : 1u, md, cpl));
+    *cells = md.cells;
+    if (n == 0) return CVL_OK;
+    CVL_TRY(e->alloc(e->pairs_in, sizeof(double) * 6 * n));
+    CVL_TRY(e->alloc(e->pb_min, sizeof(double) * (size_t)n * md.cells));
+    CVL_TRY(e->alloc(e->pb_max, sizeof(double) * (size_t)n * md.cells));
+    CVL_TRY(e->alloc(e->pb_valid, (size_t)n));
+    cudaStream_t s = e->stream;
+    CVL_CUDA(cudaMemcpyAsync(e->pairs_in.p, pairs, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
+    const int blocks = grid_for(e, n, 4, 16);
+#define CVL_PB(C)                                                                                              \
+    case C:                                                                                                    \
+        k_pair_bundles<C><<<blocks, 128, 0, s>>>(md, (const double *)e->pairs_in.p, n, (double *)e->pb_min.p, \
+                                                 (double *)e->pb_max.p, (unsigned char *)e->pb_valid.p);      \
+        break;
+    switch (cpl) {
+        CVL_PB(1) CVL_PB(2) CVL_PB(3) CVL_PB(4)
+        default: return fail(CVL_EUNSUPPORTED, "grid");
+    }
+#undef CVL_PB
+    CVL_TRY(check_launch("k_pair_bundles"));
+    CVL_CUDA(cudaMemcpyAsync(bmin, e->pb_min.p, sizeof(double) * (size_t)n * md.cells, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(bmax, e->pb_max.p, sizeof(double) * (size_t)n * md.cells, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(valid, e->pb_valid.p, (size_t)n, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaStreamSynchronize(s));
+    return CVL_OK;
+}
+
+// ---- device-resident batches -----------------------------------------------------
+int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps, int32_t edge_data_sz,
+                     cvl_batch **out) {
+    if (!e || !edges || !counts || !out || num_maps <= 0 || edge_data_sz < 4)
+        return fail(CVL_EINVAL, "invalid batch arguments");
+    *out = nullptr;
+    std::vector<int32_t> mo(num_maps + 1, 0);
+    for (int m = 0; m < num_maps; ++m) {
+        if (counts[m] <= 0) return fail(CVL_EINVAL, "every map needs at least one edge");
+        if ((long long)mo[m] + counts[m] > 0x7fffffffLL) return fail(CVL_EOVERFLOW, "batch larger than 2^31 edges");
+        mo[m + 1] = mo[m] + counts[m];
+    }
+    CVL_CUDA(cudaSetDevice(e->device));
+    cvl_batch *b = new cvl_batch();
+    b->eng = e;
+    b->num_maps = num_maps;
+    b->sz = edge_data_sz;
+    b->n = mo[num_maps];
+    b->map_off = mo;
+    const size_t eb = sizeof(double) * (size_t)b->n * edge_data_sz;
+    if ((e->budget && e->held + eb > e->budget) || cudaMalloc(&b->d_edges, eb) != cudaSuccess ||
+        cudaMalloc(&b->d_map_off, sizeof(int) * mo.size()) != cudaSuccess) {
+        cudaGetLastError();
+        if (b->d_edges) cudaFree(b->d_edges);
+        delete b;
+        return fail(CVL_ENOMEM, "batch allocation failed");
+    }
+    e->held += eb;
+    cudaMemcpyAsync(b->d_edges, edges, eb, cudaMemcpyHostToDevice, e->stream);
+    cudaMemcpyAsync(b->d_map_off, mo.data(), sizeof(int) * mo.size(), cudaMemcpyHostToDevice, e->stream);
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) {
+        cvl_batch_free(b);
+        return fail(CVL_ECUDA, std::string("batch upload: ") + cudaGetErrorString(ce));
+    }
+    *out = b;
+    return CVL_OK;
+}
+
+void cvl_batch_free(cvl_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->eng->device);
+    if (b->d_edges) {
+        cudaFree(b->d_edges);
+        b->eng->held -= sizeof(double) * (size_t)b->n * b->sz;
+    }
+    if (b->d_map_off) cudaFree(b->d_map_off);
+    delete b;
+}
+
+int cvl_batch_run(cvl_engine *e, const cvl_batch *b, const cvl_params *p, cvl_batch_result **out) {
+    if (!e || !b || !out) return fail(CVL_EINVAL, "engine/batch/out is NULL");
+    if (b->eng != e) return fail(CVL_EINVAL, "batch belongs to another engine");
+    *out = nullptr;
+    CVL_CUDA(cudaSetDevice(e->device));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
+    RunOut ro;
+    CVL_TRY(run_pipeline(e, (const double *)b->d_edges, b->n, b->sz, (const int *)b->d_map_off, b->map_off, md, cpl, 0,
+                         false, ro));
+    CVL_CUDA(cudaStreamSynchronize(e->stream));
+    e->collect_marks();
+    cvl_batch_result *r = new cvl_batch_result();
+    r->eng = e;
+    r->generation = e->generation;
+    r->num_maps = b->num_maps;
+    r->n = b->n;
+    r->width = md.gms + 1;
+    r->map_off = b->map_off;
+    r->stats = ro.stats;
+    r->cv_off = ro.cv_off;
+    r->device_ms = e->last_device_ms;
+    *out = r;
+    return CVL_OK;
+}
+
+int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view) {
+    if (!r || !view || m < 0 || m >= r->num_maps) return fail(CVL_EINVAL, "invalid batch result arguments");
+    if (!r->downloaded) {
+        if (r->eng->generation != r->generation)
+            return fail(CVL_EINVAL, "batch result outputs were overwritten by a later run on the engine");
+        const unsigned long long C = r->cv_off[r->num_maps];
+        r->chains.resize(C * r->width);
+        r->info.resize(C * 10);
+        if (C) {
+            CVL_CUDA(cudaMemcpyAsync(r->chains.data(), r->eng->chains.p, sizeof(unsigned) * C * r->width,
+                                     cudaMemcpyDeviceToHost, r->eng->stream));
+            CVL_CUDA(cudaMemcpyAsync(r->info.data(), r->eng->info.p, sizeof(double) * C * 10, cudaMemcpyDeviceToHost,
+                                     r->eng->stream));
+        }
+        CVL_CUDA(cudaStreamSynchronize(r->eng->stream));
+        r->downloaded = true;
+    }
+    const unsigned long long c0 = r->cv_off[m], c1 = r->cv_off[m + 1];
+    cvl_result_view &v = *view;
+    v.num_curvelets = (uint32_t)(c1 - c0);
+    v.chain_width = (uint32_t)r->width;
+    v.chains = r->chains.data() + c0 * r->width;
+    v.info = r->info.data() + c0 * 10;
+    v.valid_pairs = r->stats[m].valid_pairs;
+    v.total_neighbor_pairs = (int64_t)r->stats[m].pairs;
+    v.max_num_of_neighbors = r->stats[m].max_deg;
+    v.truncated_anchors = r->stats[m].truncated;
+    v.num_edges = (uint32_t)(r->map_off[m + 1] - r->map_off[m]);
+    v.flags = v.truncated_anchors ? CVL_FLAG_TRUNCATED : 0u;
+    v.device_ms = r->device_ms;
+    return CVL_OK;
+}
+
+int cvl_batch_result_stats(const cvl_batch_result *r, double *device_ms, uint64_t *num_curvelets,
+                           uint64_t *valid_pairs, uint64_t *total_pairs) {
+    if (!r) return fail(CVL_EINVAL, "result is NULL");
+    uint64_t vp = 0, tp = 0;
+    for (const MapStats &s : r->stats) {
+        vp += s.valid_pairs;
+        tp += s.pairs;
+    }
+    if (device_ms) *device_ms = r->device_ms;
+    if (num_curvelets) *num_curvelets = r->cv_off[r->num_maps];
+    if (valid_pairs) *valid_pairs = vp;
+    if (total_pairs) *total_pairs = tp;
+    return CVL_OK;
+}
+
+void cvl_batch_result_free(cvl_batch_result *r) { delete r; }
+
+int cvl_engine_flush_l2(cvl_engine *e) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    CVL_CUDA(cudaSetDevice(e->device));
+    const size_t bytes = std::max<size_t>((size_t)e->prop.l2CacheSize * 2, (size_t)256 << 20);
+    CVL_TRY(e->alloc(e->flush, bytes));
+    k_flush<<<e->prop.multiProcessorCount * 8, 256, 0, e->stream>>>((unsigned *)e->flush.p, bytes / 4, 7u);
+    CVL_TRY(check_launch("k_flush"));
+    CVL_CUDA(cudaStreamSynchronize(e->stream));
+    return CVL_OK;
+}
+
+int cvl_engine_last_kernel_times(cvl_engine *e, const char **names, double *ms, int cap) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    const int n = (int)e->last_times.size();
+    for (int k = 0; k < n && k < cap; ++k) {
+        if (names) names[k] = e->last_times[k].first;
+        if (ms) ms[k] = e->last_times[k].second;
+    }
+    return n;
+}
+
+int cvl_measure_fp64_peak(cvl_engine *e, double *tflops) {
+    if (!e || !tflops) return fail(CVL_EINVAL, "invalid argument");
+    CVL_CUDA(cudaSetDevice(e->device));
+    CVL_TRY(e->alloc(e->flush, 1024));
+    const int blocks = e->prop.multiProcessorCount * 8, threads = 256, iters = 4096;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    k_fp64_peak<<<blocks, threads, 0, e->stream>>>((double *)e->flush.p, 64, 1.0);  // warm-up
+    cudaEventRecord(a, e->stream);
+    k_fp64_peak<<<blocks, threads, 0, e->stream>>>((double *)e->flush.p, iters, 1.0);
+    cudaEventRecord(b, e->stream);
+    cudaError_t ce = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ce != cudaSuccess) return fail(CVL_ECUDA, std::string("fp64 probe: ") + cudaGetErrorString(ce));
+    const double fmas = (double)blocks * threads * iters * 16.0 * 8.0;
+    *tflops = 2.0 * fmas / (ms * 1e-3) / 1e12;
+    return CVL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,192 @@
+/*
+ * cvl.h -- C ABI of the B200 curvelet-construction engine (libcvl.so).
+ *
+ * The engine is a drop-in for the reference cpu_curvelet path
+ *   preprocess (spatial hash + neighbour CSR)
+ *   -> pairwise curve-bundle formation
+ *   -> greedy edge-chain growth, dedup and record,
+ * computed in FP64 by hand-written sm_100a CUDA kernels on one GPU.
+ *
+ * Conventions: plain C types; every entry point returns an int status
+ * (CVL_OK = 0, negative on error) unless stated; cvl_last_error() gives a
+ * one-line reason for the calling thread's last failure. An engine handle is
+ * used by one host thread at a time. Inputs are caller-owned and only read
+ * during the call; results are engine-owned until freed.
+ *
+ * Reference citations are path:line within the reference project
+ * (C-H-Chien/Curvelet_Construction_on_GPU).
+ */
+#ifndef CVL_H
+#define CVL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define CVL_OK 0
+#define CVL_EINVAL (-1)       /* invalid argument (reference: preprocess.hpp:197-199 returns false) */
+#define CVL_ENOMEM (-2)       /* device or host allocation failed, or over the memory budget */
+#define CVL_ECUDA (-3)        /* a CUDA runtime call failed */
+#define CVL_EUNSUPPORTED (-4) /* parameters outside what the kernels are built for */
+#define CVL_ETIMEDOUT (-5)    /* a bounded wait expired (serving) */
+#define CVL_EOVERFLOW (-6)    /* a capacity was exceeded (reported, never silently truncated) */
+#define CVL_EAGAIN (-7)       /* request not finished yet (serving poll) */
+#define CVL_ENODEV (-8)       /* no usable CUDA device */
+
+/* ---- parameters ------------------------------------------------------ */
+/* Mirrors CurveletParams, cpu_curvelet/param_settings.hpp:9-24 (same names,
+ * same defaults, same meaning). gap, curvelet_style and out_type are accepted
+ * and ignored exactly as the reference ignores them (main.cpp:29,32,94-95). */
+typedef struct cvl_params {
+    double nrad;             /* neighbour radius, px (3.5) */
+    double gap;              /* unused by the path (1.5) */
+    double dx;               /* edge position uncertainty, px (0.4) */
+    double dt_deg;           /* edge orientation uncertainty, degrees (15) */
+    double dt_rad;           /* the same in radians, as CurveletCPU's ctor takes it (cpu_curvelet.hpp:82-83);
+                                used as is when > 0, else dt = (dt_deg / 180) * pi (main.cpp:24) (0) */
+    double max_k;            /* curvature bound (0.3) */
+    unsigned curvelet_style; /* 2 = anchor-leading bidirectional (the only style the path runs) */
+    unsigned group_max_sz;   /* maximum edges per curvelet, anchor included (4); 1..16 supported */
+    unsigned out_type;       /* unused by the path (0) */
+    double sx;               /* bundle grid step in position, px (0.1) */
+    double st;               /* bundle grid step in orientation, rad (0.08) */
+    int edge_data_sz;        /* values per edge row, >= 4 (4) */
+    unsigned max_candidates; /* neighbour cap per anchor (128); 1..1024 supported */
+} cvl_params;
+
+/* Fills the reference defaults (param_settings.hpp:11-23). */
+void cvl_params_default(cvl_params *p);
+
+/* ---- engine ----------------------------------------------------------- */
+typedef struct cvl_engine cvl_engine;
+
+typedef struct cvl_engine_cfg {
+    int device;               /* CUDA device ordinal (0) */
+    size_t mem_budget_bytes;  /* device memory the engine may hold; 0 = no limit */
+    int cell_size;            /* spatial-hash cell edge in pixel cells; 0 = auto (4) */
+    int seeds_per_group;      /* chain-growth seeds walked together per warp: 4 or 8; 0 = auto */
+    int bundle_slots;         /* bundles kept in shared memory per warp; 0 = auto */
+    int warps_per_block;      /* 0 = auto */
+} cvl_engine_cfg;
+
+void cvl_engine_cfg_default(cvl_engine_cfg *cfg);
+int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out);
+void cvl_engine_destroy(cvl_engine *e);
+
+/* One-line description of the calling thread's last error ("" if none). */
+const char *cvl_last_error(void);
+/* Library version string. */
+const char *cvl_version(void);
+
+/* ---- results ---------------------------------------------------------- */
+typedef struct cvl_result cvl_result;
+
+/* Flags reported in cvl_result_view.flags. */
+#define CVL_FLAG_TRUNCATED 1u /* some anchor reached max_candidates (preprocess.hpp:224-229) */
+
+typedef struct cvl_result_view {
+    uint32_t num_curvelets;  /* rows, = CurveletCPU::num_curvelets() (cpu_curvelet.hpp:95) */
+    uint32_t chain_width;    /* group_max_sz + 1 (cpu_curvelet.hpp:96) */
+    const uint32_t *chains;  /* [num_curvelets][chain_width], row-major, 1-based edge ids,
+                                zero padded: _edge_chain_final[0:num_curvelets] (cpu_curvelet.hpp:258-280) */
+    const double *info;      /* [num_curvelets][10], row-major: the info file's rows
+                                (main.cpp:81-88; columns per cpu_curvelet.hpp:246-255) */
+    uint32_t valid_pairs;    /* form_pairwise_bundles' count (cpu_curvelet.hpp:305-361) */
+    int64_t total_neighbor_pairs;  /* CPUNeighborGraph::total_neighbor_pairs (preprocess.hpp:248) */
+    uint32_t max_num_of_neighbors; /* CPUNeighborGraph::max_num_of_neighbors (preprocess.hpp:243-245) */
+    uint32_t truncated_anchors;    /* anchors that reached max_candidates (preprocess.hpp:224-229) */
+    uint32_t num_edges;
+    uint32_t flags;                /* CVL_FLAG_* */
+    double device_ms;              /* device time of the compute (CUDA events), excluding copies */
+} cvl_result_view;
+
+/* The one-shot plain form: one edge map (AoS rows of edge_data_sz doubles,
+ * host memory) -> curvelets, i.e. run_curvelet<double> without the file I/O
+ * (main.cpp:20-96: build_neighbor_csr_graph + CurveletCPU::form_pairwise_bundles
+ * + CurveletCPU::build_curvelets_greedy). Copies in, computes, copies out. */
+int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
+            const cvl_params *p, cvl_result **out);
+
+/* Views a result (pointers stay valid until cvl_result_free). */
+int cvl_result_get(const cvl_result *r, cvl_result_view *view);
+void cvl_result_free(cvl_result *r);
+
+/* ---- the reference's staged template API ------------------------------ */
+/* Neighbour graph: build_neighbor_csr_graph<T> (preprocess.hpp:186-274) and
+ * CPUNeighborGraph<T> (preprocess.hpp:18-31). neighbor_radius is the pixel-cell
+ * window half width (the reference passes 3u, main.cpp:48). */
+typedef struct cvl_graph cvl_graph;
+typedef struct cvl_graph_view {
+    int32_t num_edges;
+    int64_t total_neighbor_pairs;
+    uint32_t max_num_of_neighbors;
+    uint32_t truncated_anchors;
+    const int32_t *neighbor_offsets; /* [num_edges + 1] (int64 totals above 2^31 are rejected) */
+    const int32_t *neighbor_ids;     /* [total_neighbor_pairs], ascending distance */
+    const double *neighbor_dist2;    /* [total_neighbor_pairs] */
+} cvl_graph_view;
+
+int cvl_build_neighbor_graph(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
+                             double rad, unsigned neighbor_radius, unsigned max_candidates, cvl_graph **out);
+int cvl_graph_get(const cvl_graph *g, cvl_graph_view *view);
+void cvl_graph_free(cvl_graph *g);
+
+/* CurveletCPU::form_pairwise_bundles (cpu_curvelet.hpp:305-361): the number of
+ * (anchor, neighbour) pairs with a valid curve bundle, over the graph's pairs. */
+int cvl_form_pairwise_bundles(cvl_engine *e, const cvl_graph *g, const cvl_params *p, uint32_t *valid_pairs);
+
+/* CurveletCPU::build_curvelets_greedy (cpu_curvelet.hpp:363-634) over a graph
+ * built by cvl_build_neighbor_graph. */
+int cvl_build_curvelets(cvl_engine *e, const cvl_graph *g, const cvl_params *p, cvl_result **out);
+
+/* CurveletCPU::compute_curve_bundle for n independent pairs (cpu_curvelet.hpp:637-819):
+ * pairs[i] = (te_x, te_y, te_theta, le_x, le_y, le_theta). Writes bmin/bmax
+ * [n][cells] and valid[n] (1 = the reference's hyp_LookEdge true). cells =
+ * P*Q of the grid (cpu_curvelet.hpp:73-74) is returned in *cells. */
+int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p,
+                     double *bmin, double *bmax, uint8_t *valid, int32_t *cells);
+
+/* ---- device-resident maps (benchmarks, batching) ---------------------- */
+/* A ragged batch of edge maps kept in device memory: maps[m] has counts[m]
+ * rows of edge_data_sz doubles, concatenated in edges. */
+typedef struct cvl_batch cvl_batch;
+
+int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps,
+                     int32_t edge_data_sz, cvl_batch **out);
+void cvl_batch_free(cvl_batch *b);
+
+/* Runs the whole path over every map of a device-resident batch in one pass
+ * (ragged: one spatial hash, one neighbour pass, one fused bundle/growth pass,
+ * one compaction for all maps). Results stay in device memory; device_ms is
+ * filled. Per-map results are read with cvl_batch_result_*. */
+typedef struct cvl_batch_result cvl_batch_result;
+int cvl_batch_run(cvl_engine *e, const cvl_batch *b, const cvl_params *p, cvl_batch_result **out);
+/* Downloads (once) and views map m of a batch result. */
+int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view);
+/* Device time (ms) of the batch compute, and the totals over all maps. */
+int cvl_batch_result_stats(const cvl_batch_result *r, double *device_ms, uint64_t *num_curvelets,
+                           uint64_t *valid_pairs, uint64_t *total_pairs);
+void cvl_batch_result_free(cvl_batch_result *r);
+
+/* Writes a buffer larger than the L2 cache on the engine's stream and waits
+ * (timing hygiene between benchmark iterations). */
+int cvl_engine_flush_l2(cvl_engine *e);
+
+/* Per-kernel device times (ms) of the engine's last run: fills up to cap
+ * entries of names/ms and returns the count (or a negative status). */
+int cvl_engine_last_kernel_times(cvl_engine *e, const char **names, double *ms, int cap);
+
+/* Measures the device's FP64 FMA throughput (TFLOP/s, 2 flops per FMA) with a
+ * register-resident dependent-chain loop; the roofline denominator for the
+ * FP64-bound bundle kernel. */
+int cvl_measure_fp64_peak(cvl_engine *e, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVL_H */

@@ -1,0 +1,233 @@
+"""ctypes front end of the CPU checker -- TEST INFRASTRUCTURE ONLY.
+
+Loads ``oracle/libcvl_oracle.so`` (the C restatement of the reference path,
+``oracle/cvl_oracle.c``) and, when it was built, ``oracle/_ref/libcvlref.so``
+(the reference's own cpu_curvelet templates behind ``oracle/ref_harness.cpp``).
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's cpu_baseline /
+reference legs import this module; the engine never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libcvl_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libcvlref.so")
+REF_CLI = os.path.join(HERE, "_ref", "CURVELET")
+
+# reference defaults, cpu_curvelet/param_settings.hpp:9-24
+DEFAULTS = dict(nrad=3.5, dx=0.4, dt_deg=15.0, max_k=0.3, sx=0.1, st=0.08,
+                group_max_sz=4, max_candidates=128)
+
+
+def build(quiet: bool = True) -> None:
+    """Builds the restatement (and the reference leg when its sources exist)."""
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+class _OrcCsr(C.Structure):
+    _fields_ = [("num_edges", C.c_int), ("total_neighbor_pairs", C.c_int),
+                ("max_num_of_neighbors", C.c_uint), ("truncated_anchors", C.c_uint),
+                ("tie_anchors", C.c_uint),
+                ("neighbor_offsets", C.POINTER(C.c_int)), ("neighbor_ids", C.POINTER(C.c_int)),
+                ("neighbor_dist2", C.POINTER(C.c_double))]
+
+
+class _OrcResult(C.Structure):
+    _fields_ = [("num_edges", C.c_int), ("total_neighbor_pairs", C.c_int),
+                ("max_num_of_neighbors", C.c_uint), ("truncated_anchors", C.c_uint),
+                ("tie_anchors", C.c_uint), ("valid_pairs", C.c_uint),
+                ("num_curvelets", C.c_uint), ("chain_width", C.c_uint),
+                ("chains", C.POINTER(C.c_uint)), ("info", C.POINTER(C.c_double)),
+                ("anchor_count", C.POINTER(C.c_uint))]
+
+
+class _RefOut(C.Structure):
+    _fields_ = [("num_edges", C.c_int), ("total_neighbor_pairs", C.c_int),
+                ("max_num_of_neighbors", C.c_uint), ("valid_pairs", C.c_uint),
+                ("num_curvelets", C.c_uint), ("chain_width", C.c_uint),
+                ("neighbor_offsets", C.POINTER(C.c_int)), ("neighbor_ids", C.POINTER(C.c_int)),
+                ("neighbor_dist2", C.POINTER(C.c_double)),
+                ("chains", C.POINTER(C.c_uint)), ("info", C.POINTER(C.c_double)),
+                ("ms_csr", C.c_double), ("ms_pairwise", C.c_double), ("ms_greedy", C.c_double)]
+
+
+@dataclass
+class Csr:
+    offsets: np.ndarray
+    ids: np.ndarray
+    dist2: np.ndarray
+    max_deg: int
+    truncated_anchors: int = 0
+    tie_anchors: int = 0
+
+
+@dataclass
+class Result:
+    """The observable outputs of one run: chains (uint32, 1-based ids, rows of
+    group_max_sz + 1) and info (float64, rows of 10), plus the path's counters."""
+    chains: np.ndarray
+    info: np.ndarray
+    valid_pairs: int
+    total_neighbor_pairs: int
+    max_num_of_neighbors: int
+    truncated_anchors: int = 0
+    tie_anchors: int = 0
+    anchor_count: np.ndarray | None = None
+    csr: Csr | None = None
+    ms: dict = field(default_factory=dict)
+
+    @property
+    def num_curvelets(self) -> int:
+        return int(self.chains.shape[0])
+
+
+def _arr(ptr, n, dtype):
+    if n == 0:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        dp = C.POINTER(C.c_double)
+        L.orc_build_csr.argtypes = [dp, C.c_int, C.c_int, C.c_double, C.c_uint, C.c_uint, C.c_int,
+                                    C.POINTER(_OrcCsr)]
+        L.orc_csr_free.argtypes = [C.POINTER(_OrcCsr)]
+        L.orc_run.argtypes = [dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                              C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_int, C.POINTER(_OrcResult)]
+        L.orc_result_free.argtypes = [C.POINTER(_OrcResult)]
+        L.orc_pair_bundle.argtypes = [C.c_double] * 12 + [dp, dp, C.POINTER(C.c_int)]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError("reference harness not built: " + REF_SO)
+        L = C.CDLL(REF_SO)
+        dp = C.POINTER(C.c_double)
+        L.cvlref_run.argtypes = [dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_int, C.c_int, C.c_int,
+                                 C.POINTER(_RefOut)]
+        L.cvlref_free.argtypes = [C.POINTER(_RefOut)]
+        L.cvlref_pair_bundle.argtypes = [C.c_double] * 12 + [dp, dp, C.POINTER(C.c_int)]
+        _ref = L
+    return _ref
+
+
+def _edges_arg(edges):
+    e = np.ascontiguousarray(edges, dtype=np.float64)
+    assert e.ndim == 2 and e.shape[1] >= 4
+    return e, e.ctypes.data_as(C.POINTER(C.c_double)), e.shape[0], e.shape[1]
+
+
+def build_csr(edges, nrad=3.5, neighbor_radius=3, max_candidates=128, nthreads=1) -> Csr:
+    e, p, n, sz = _edges_arg(edges)
+    g = _OrcCsr()
+    rc = lib().orc_build_csr(p, n, sz, nrad, neighbor_radius, max_candidates, nthreads, C.byref(g))
+    if rc != 0:
+        raise ValueError("orc_build_csr rejected the input")
+    try:
+        np_ = g.total_neighbor_pairs
+        return Csr(_arr(g.neighbor_offsets, n + 1, np.int32), _arr(g.neighbor_ids, np_, np.int32),
+                   _arr(g.neighbor_dist2, np_, np.float64), int(g.max_num_of_neighbors),
+                   int(g.truncated_anchors), int(g.tie_anchors))
+    finally:
+        lib().orc_csr_free(C.byref(g))
+
+
+def run(edges, nthreads=1, **params) -> Result:
+    """The restatement over one edge map (AoS rows of >= 4 values)."""
+    p = dict(DEFAULTS, **params)
+    e, ptr, n, sz = _edges_arg(edges)
+    r = _OrcResult()
+    rc = lib().orc_run(ptr, n, sz, p["nrad"], p["dx"], p["dt_deg"], p["max_k"], p["sx"], p["st"],
+                       p["group_max_sz"], p["max_candidates"], nthreads, C.byref(r))
+    if rc != 0:
+        raise ValueError(f"orc_run failed ({rc})")
+    try:
+        w = r.chain_width
+        nc = r.num_curvelets
+        return Result(_arr(r.chains, nc * w, np.uint32).reshape(nc, w),
+                      _arr(r.info, nc * 10, np.float64).reshape(nc, 10),
+                      int(r.valid_pairs), int(r.total_neighbor_pairs), int(r.max_num_of_neighbors),
+                      int(r.truncated_anchors), int(r.tie_anchors),
+                      _arr(r.anchor_count, n, np.uint32))
+    finally:
+        lib().orc_result_free(C.byref(r))
+
+
+def ref_run(edges, nthreads=1, want_outputs=True, **params) -> Result:
+    """The reference's own cpu_curvelet code over one edge map."""
+    p = dict(DEFAULTS, **params)
+    e, ptr, n, sz = _edges_arg(edges)
+    r = _RefOut()
+    rc = ref_lib().cvlref_run(ptr, n, sz, p["nrad"], p["dx"], p["dt_deg"], p["max_k"], p["sx"], p["st"],
+                              p["group_max_sz"], p["max_candidates"], nthreads, 1, int(want_outputs),
+                              C.byref(r))
+    if rc != 0:
+        raise ValueError(f"cvlref_run failed ({rc})")
+    try:
+        w, nc, np_ = r.chain_width, r.num_curvelets, r.total_neighbor_pairs
+        ms = dict(csr=r.ms_csr, pairwise=r.ms_pairwise, greedy=r.ms_greedy)
+        if not want_outputs:
+            return Result(np.zeros((0, w), np.uint32), np.zeros((0, 10)), int(r.valid_pairs), np_,
+                          int(r.max_num_of_neighbors), ms=ms)
+        csr = Csr(_arr(r.neighbor_offsets, n + 1, np.int32), _arr(r.neighbor_ids, np_, np.int32),
+                  _arr(r.neighbor_dist2, np_, np.float64), int(r.max_num_of_neighbors))
+        return Result(_arr(r.chains, nc * w, np.uint32).reshape(nc, w),
+                      _arr(r.info, nc * 10, np.float64).reshape(nc, 10),
+                      int(r.valid_pairs), np_, int(r.max_num_of_neighbors), csr=csr, ms=ms)
+    finally:
+        ref_lib().cvlref_free(C.byref(r))
+
+
+def pair_bundle(te, le, use_ref=False, **params):
+    """One pair's bundle grid: (valid, bmin[cells], bmax[cells]). te/le = (x, y, theta)."""
+    p = dict(DEFAULTS, **params)
+    bmin = np.zeros(1024)
+    bmax = np.zeros(1024)
+    nc = C.c_int(0)
+    f = ref_lib().cvlref_pair_bundle if use_ref else lib().orc_pair_bundle
+    dp = C.POINTER(C.c_double)
+    v = f(te[0], te[1], te[2], le[0], le[1], le[2], p["nrad"], p["dx"], p["dt_deg"], p["max_k"],
+          p["sx"], p["st"], bmin.ctypes.data_as(dp), bmax.ctypes.data_as(dp), C.byref(nc))
+    return bool(v), bmin[:nc.value].copy(), bmax[:nc.value].copy()
+
+
+def read_edge_file(path: str, values_per_edge: int = 4) -> np.ndarray:
+    """Parses the reference's edge-file format (data_io.hpp:22-79) into [N, values_per_edge]."""
+    rows = []
+    with open(path) as fh:
+        for ln, line in enumerate(fh, 1):
+            toks = line.split()
+            if len(toks) != values_per_edge:
+                raise ValueError(f"{path}:{ln}: expected {values_per_edge} values, found {len(toks)}")
+            rows.append([float(t) for t in toks])
+    if not rows:
+        raise ValueError(f"{path}: no edges")
+    return np.asarray(rows, dtype=np.float64)

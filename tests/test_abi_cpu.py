@@ -1,0 +1,92 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry point
+include/cvl.h declares, keeps the reference defaults, rejects bad arguments
+before touching a device, and fails loudly (no CPU fallback) without a GPU."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+import curvelet_construction_on_gpu_b200 as cvl
+from curvelet_construction_on_gpu_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
+
+
+def _declared():
+    names = set()
+    for h in HEADERS:
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(cvl_[a-z0-9_]+)\s*\(", src):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def test_every_declared_symbol_is_exported():
+    lib = C.CDLL(_abi.LIB_PATH)
+    names = _declared()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding covers all of them
+    bound = {n for n, _, _ in _abi.SIGNATURES}
+    assert set(names) <= bound, sorted(set(names) - bound)
+
+
+def test_param_defaults_match_reference():
+    p = _abi.CvlParams()
+    _abi.load().cvl_params_default(C.byref(p))
+    # cpu_curvelet/param_settings.hpp:11-23
+    assert (p.nrad, p.gap, p.dx, p.dt_deg, p.max_k) == (3.5, 1.5, 0.4, 15.0, 0.3)
+    assert (p.curvelet_style, p.group_max_sz, p.out_type) == (2, 4, 0)
+    assert (p.sx, p.st, p.edge_data_sz, p.max_candidates) == (0.1, 0.08, 4, 128)
+    assert p.dt_rad == 0.0
+    py = cvl.CurveletParams()
+    assert (py.nrad, py.dx, py.dt_deg, py.max_k, py.group_max_sz, py.sx, py.st, py.max_candidates) == \
+        (3.5, 0.4, 15.0, 0.3, 4, 0.1, 0.08, 128)
+
+
+def test_null_arguments_are_rejected():
+    lib = _abi.load()
+    r = C.c_void_p()
+    assert lib.cvl_run(None, None, 0, 4, None, C.byref(r)) == _abi.CVL_EINVAL
+    assert lib.cvl_result_get(None, None) == _abi.CVL_EINVAL
+    assert lib.cvl_engine_create(None, None) == _abi.CVL_EINVAL
+    assert "NULL" in lib.cvl_last_error().decode()
+    assert lib.cvl_version().decode().startswith("cvl ")
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU failure path")
+def test_no_gpu_fails_loudly():
+    with pytest.raises(cvl.CvlError) as ei:
+        cvl.Engine()
+    assert ei.value.code == _abi.CVL_ENODEV
+
+
+def test_cli_flags_without_gpu(tmp_path):
+    cli = os.path.join(ROOT, "curvelet_construction_on_gpu_b200", "bin", "CURVELET")
+    assert os.path.exists(cli), "CLI not built"
+    r = subprocess.run([cli, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "--max-candidates" in r.stderr
+    r = subprocess.run([cli, "--bogus"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Unknown argument: --bogus" in r.stderr
+    r = subprocess.run([cli, "--float"], capture_output=True, text=True)
+    assert r.returncode == 1
+    r = subprocess.run([cli, "--nrad", "abc"], capture_output=True, text=True)
+    assert r.returncode == 1 and "invalid value for --nrad" in r.stderr
+    # missing input file is reported before any device work (data_io.hpp:27-31)
+    run_dir = tmp_path / "run"
+    run_dir.mkdir()
+    r = subprocess.run([cli, "--edge-file", "nope.txt"], capture_output=True, text=True, cwd=run_dir)
+    assert r.returncode == 1 and "input file does not exist: ../test_files/nope.txt" in r.stderr
