@@ -80,6 +80,7 @@ SIGNATURES = [
     ("cvl_batch_result_free", None, [_vp]),
     ("cvl_engine_flush_l2", C.c_int, [_vp]),
     ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),
+    ("cvl_engine_last_launch_count", C.c_int, [_vp]),
     ("cvl_measure_fp64_peak", C.c_int, [_vp, _dp]),
 ]
 

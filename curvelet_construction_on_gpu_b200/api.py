@@ -226,6 +226,12 @@ class Engine:
             check(n, "cvl_engine_last_kernel_times")
         return [(names[k].decode(), float(ms[k])) for k in range(min(n, 64))]
 
+    def launch_count(self) -> int:
+        n = self._lib.cvl_engine_last_launch_count(self._h)
+        if n < 0:
+            check(n, "cvl_engine_last_launch_count")
+        return int(n)
+
     def fp64_peak_tflops(self) -> float:
         t = C.c_double(0)
         check(self._lib.cvl_measure_fp64_peak(self._h, C.byref(t)), "cvl_measure_fp64_peak")

@@ -10,12 +10,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/cvl.h"
-#include "cvl_kernels.cuh"
+#include "cvl_curvelets.cuh"
 #include "cvl_scan.cuh"
 
 using namespace cvl;
@@ -45,6 +46,8 @@ struct DBuf {
     void *p = nullptr;
     size_t bytes = 0;
 };
+
+int g_launches_snapshot();
 
 inline unsigned next_pow2(unsigned long long v) {
     unsigned long long p = 1;
@@ -119,7 +122,10 @@ struct cvl_engine {
         ++nmarks;
     }
 
+    int last_launches = 0;
+
     void collect_marks() {
+        last_launches = g_launches_snapshot();
         last_times.clear();
         last_device_ms = 0.0;
         if (nmarks < 2) return;
@@ -233,9 +239,23 @@ int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nb
     return CVL_OK;
 }
 
+// CVL_SYNC_CHECK=1 in the environment synchronizes after every launch so that a
+// device-side error is reported against the kernel that raised it.
+const bool g_sync_check = std::getenv("CVL_SYNC_CHECK") != nullptr;
+
+// kernels launched by this thread since the last run started (cvl_engine_last_launch_count)
+thread_local int g_launches = 0;
+
+int g_launches_snapshot() { return g_launches; }
+
 int check_launch(const char *what) {
+    ++g_launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(CVL_ECUDA, std::string("launch ") + what + ": " + cudaGetErrorString(e));
+    if (g_sync_check) {
+        e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return fail(CVL_ECUDA, std::string("kernel ") + what + " failed: " + cudaGetErrorString(e));
+    }
     return CVL_OK;
 }
 
@@ -291,9 +311,8 @@ struct RunOut {
 };
 
 template <int CPL, int K>
-int launch_curvelets(cvl_engine *e, CurveletArgs &a, size_t per_warp, int blocks) {
+int launch_curvelets(cvl_engine *e, CurveletArgs &a, size_t smem, int blocks) {
     const int threads = 128;
-    const size_t smem = per_warp * (threads / 32);
     CVL_CUDA(cudaFuncSetAttribute(k_curvelets<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_curvelets<CPL, K><<<blocks, threads, smem, e->stream>>>(a);
     return check_launch("k_curvelets");
@@ -330,6 +349,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     cudaStream_t s = e->stream;
     e->nmarks = 0;
     ++e->generation;
+    g_launches = 0;
     e->mark("start");
 
     const unsigned T = next_pow2(std::max<unsigned long long>((unsigned long long)n, 1024ull));
@@ -394,7 +414,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
 
     // ---- (b) neighbour count + CSR offsets
     const int nb_wpb = 8;
-    const size_t nb_smem = (size_t)nb_wpb * md.max_cand * 20;
+    const size_t nb_smem = (size_t)nb_wpb * nbr_smem_per_warp(md.max_cand);
     if (nb_smem > 48 * 1024) {
         CVL_CUDA(cudaFuncSetAttribute(k_neighbors<NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
         CVL_CUDA(cudaFuncSetAttribute(k_neighbors<NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
@@ -444,19 +464,20 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     const int K = (e->seeds_per_group == 8) ? 8 : 4;
     pick_curvelet_kernel(cpl, K, lf, of);
     int slots = e->slots > 0 ? e->slots : 10;
-    size_t per_warp = curvelet_smem_per_warp(md.max_cand, slots, md.gms, cpl);
-    while (per_warp * 4 > (size_t)e->prop.sharedMemPerBlockOptin && slots > 1) {
+    size_t smem = curvelet_smem_bytes(4, md.max_cand, slots, md.gms, cpl, md.Q);
+    while (smem > (size_t)e->prop.sharedMemPerBlockOptin && slots > 1) {
         --slots;
-        per_warp = curvelet_smem_per_warp(md.max_cand, slots, md.gms, cpl);
+        smem = curvelet_smem_bytes(4, md.max_cand, slots, md.gms, cpl, md.Q);
     }
     int bps = 0;
-    CVL_TRY(of(per_warp * 4, bps));
+    CVL_TRY(of(smem, bps));
     if (bps < 1) return fail(CVL_EUNSUPPORTED, "k_curvelets does not fit on an SM with these parameters");
     const int blocks = bps * e->prop.multiProcessorCount;
     const int warps = blocks * 4;
-    const int scratch_deg = (int)ro.max_deg > slots ? (int)ro.max_deg - slots : 0;
-    CVL_TRY(e->alloc(e->scratch, sizeof(double) * (size_t)warps * (size_t)std::max(scratch_deg, 1) * 64 * cpl));
-    CVL_TRY(e->alloc(e->scratch_chain, sizeof(unsigned short) * (size_t)warps * (size_t)std::max(scratch_deg, 1) *
+    // a run holds at most max_deg seeds plus one chunk of tentative slots
+    const int scratch_slots = std::max((int)ro.max_deg + PCH - slots, 0);
+    CVL_TRY(e->alloc(e->scratch, sizeof(double) * (size_t)warps * (size_t)std::max(scratch_slots, 1) * 64 * cpl));
+    CVL_TRY(e->alloc(e->scratch_chain, sizeof(unsigned short) * (size_t)warps * (size_t)std::max(scratch_slots, 1) *
                                            (size_t)md.gms));
     if (mode == 0) {
         CVL_TRY(e->alloc(e->rec_ids, sizeof(unsigned) * P * md.gms));
@@ -474,14 +495,13 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     a.rec.meta = (unsigned *)e->rec_meta.p;
     a.count = (unsigned *)e->count.p;
     a.stats = stats;
-    a.work = (unsigned *)e->work.p;
     a.scratch = (double *)e->scratch.p;
     a.scratch_chain = (unsigned short *)e->scratch_chain.p;
-    a.scratch_deg = scratch_deg;
+    a.scratch_slots = scratch_slots;
     a.slots = slots;
     a.count_only = (mode == 1) ? 1 : 0;
     a.err = err;
-    CVL_TRY(lf(e, a, per_warp, blocks));
+    CVL_TRY(lf(e, a, smem, blocks));
     e->mark("curvelets");
 
     if (mode == 1) {
@@ -816,16 +836,8 @@ int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_pa
     cudaStream_t s = e->stream;
     CVL_CUDA(cudaMemcpyAsync(e->pairs_in.p, pairs, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
     const int blocks = grid_for(e, n, 4, 16);
-#define CVL_PB(C)                                                                                              \
-    case C:                                                                                                    \
-        k_pair_bundles<C><<<blocks, 128, 0, s>>>(md, (const double *)e->pairs_in.p, n, (double *)e->pb_min.p, \
-                                                 (double *)e->pb_max.p, (unsigned char *)e->pb_valid.p);      \
-        break;
-    switch (cpl) {
-        CVL_PB(1) CVL_PB(2) CVL_PB(3) CVL_PB(4)
-        default: return fail(CVL_EUNSUPPORTED, "grid");
-    }
-#undef CVL_PB
+    k_pair_bundles<<<blocks, 128, 0, s>>>(md, (const double *)e->pairs_in.p, n, (double *)e->pb_min.p,
+                                          (double *)e->pb_max.p, (unsigned char *)e->pb_valid.p);
     CVL_TRY(check_launch("k_pair_bundles"));
     CVL_CUDA(cudaMemcpyAsync(bmin, e->pb_min.p, sizeof(double) * (size_t)n * md.cells, cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaMemcpyAsync(bmax, e->pb_max.p, sizeof(double) * (size_t)n * md.cells, cudaMemcpyDeviceToHost, s));
@@ -980,6 +992,11 @@ int cvl_engine_last_kernel_times(cvl_engine *e, const char **names, double *ms, 
         if (ms) ms[k] = e->last_times[k].second;
     }
     return n;
+}
+
+int cvl_engine_last_launch_count(cvl_engine *e) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    return e->last_launches;
 }
 
 int cvl_measure_fp64_peak(cvl_engine *e, double *tflops) {

@@ -180,6 +180,9 @@ int cvl_engine_flush_l2(cvl_engine *e);
  * entries of names/ms and returns the count (or a negative status). */
 int cvl_engine_last_kernel_times(cvl_engine *e, const char **names, double *ms, int cap);
 
+/* Kernels the engine launched in its last run (>= 0), or a negative status. */
+int cvl_engine_last_launch_count(cvl_engine *e);
+
 /* Measures the device's FP64 FMA throughput (TFLOP/s, 2 flops per FMA) with a
  * register-resident dependent-chain loop; the roofline denominator for the
  * FP64-bound bundle kernel. */

@@ -154,15 +154,21 @@ def test_batch_equals_plain(engine):
             synth.mixed_map(2001), synth.plain_small(13)]
     b = engine.upload_batch(maps)
     br = engine.run_batch(b)
+    mixed = [br.map(m) for m in range(len(maps))]  # results live in the engine's workspace until fetched
     for m, e in enumerate(maps):
         alone = engine.run(e)
-        inmix = br.map(m)
+        inmix = mixed[m]
         assert np.array_equal(alone.chains, inmix.chains), m
         assert np.array_equal(alone.info.view(np.uint64), inmix.info.view(np.uint64)), m
         assert (alone.valid_pairs, alone.total_neighbor_pairs, alone.max_num_of_neighbors) == \
             (inmix.valid_pairs, inmix.total_neighbor_pairs, inmix.max_num_of_neighbors), m
     st = br.stats()
-    assert st["num_curvelets"] == sum(br.map(m).num_curvelets for m in range(len(maps)))
+    assert st["num_curvelets"] == sum(r.num_curvelets for r in mixed)
+    # a result whose outputs were overwritten by a later run refuses to serve stale data
+    br2 = engine.run_batch(b)
+    engine.run(maps[0])
+    with pytest.raises(cvl.CvlError):
+        br2.map(0)
 
 
 # ---- edge cases -------------------------------------------------------------------------
