@@ -73,16 +73,51 @@ class Result:
         return int(self.chains.shape[0])
 
 
-def _view_to_result(v: CvlResultView) -> Result:
+class _Owner:
+    """Frees a C result handle when the last numpy view onto it goes away."""
+
+    def __init__(self, lib, handle, free_name: str):
+        self._lib, self._h, self._free = lib, handle, free_name
+
+    def __del__(self):
+        try:
+            if self._h:
+                getattr(self._lib, self._free)(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def _view_to_result(v: CvlResultView, owner: "_Owner | None" = None) -> Result:
+    """numpy views onto the result's page-locked buffers (no copy when an owner
+    keeps the C result alive; a copy otherwise)."""
     nc, w = int(v.num_curvelets), int(v.chain_width)
     if nc:
-        chains = np.ctypeslib.as_array(v.chains, shape=(nc * w,)).reshape(nc, w).copy()
-        info = np.ctypeslib.as_array(v.info, shape=(nc * 10,)).reshape(nc, 10).copy()
+        chains = np.ctypeslib.as_array(v.chains, shape=(nc * w,)).reshape(nc, w)
+        info = np.ctypeslib.as_array(v.info, shape=(nc * 10,)).reshape(nc, 10)
+        if owner is None:
+            chains, info = chains.copy(), info.copy()
+        else:
+            chains = _OwnedArray.wrap(chains, owner)
+            info = _OwnedArray.wrap(info, owner)
     else:
         chains = np.zeros((0, w), np.uint32)
         info = np.zeros((0, 10), np.float64)
     return Result(chains, info, int(v.valid_pairs), int(v.total_neighbor_pairs), int(v.max_num_of_neighbors),
                   int(v.truncated_anchors), int(v.num_edges), float(v.device_ms))
+
+
+class _OwnedArray(np.ndarray):
+    """An ndarray view that keeps the buffer's owner alive."""
+
+    @classmethod
+    def wrap(cls, arr: np.ndarray, owner: _Owner) -> "_OwnedArray":
+        out = arr.view(cls)
+        out._owner = owner
+        return out
+
+    def __array_finalize__(self, obj):
+        self._owner = getattr(obj, "_owner", None)
 
 
 def _edges(edges) -> np.ndarray:
@@ -132,12 +167,10 @@ class Engine:
         r = C.c_void_p()
         check(self._lib.cvl_run(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1], C.byref(p),
                                 C.byref(r)), "cvl_run")
-        try:
-            v = CvlResultView()
-            check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
-            return _view_to_result(v)
-        finally:
-            self._lib.cvl_result_free(r)
+        owner = _Owner(self._lib, r, "cvl_result_free")
+        v = CvlResultView()
+        check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
+        return _view_to_result(v, owner)
 
     # ---- staged API
     def build_neighbor_graph(self, edges, rad: float = 3.5, neighbor_radius: int = 3,

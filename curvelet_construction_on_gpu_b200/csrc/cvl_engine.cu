@@ -12,11 +12,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/cvl.h"
-#include "cvl_curvelets.cuh"
+#include "cvl_path.cuh"
 #include "cvl_scan.cuh"
 
 using namespace cvl;
@@ -49,6 +51,10 @@ struct DBuf {
 
 int g_launches_snapshot();
 
+// Pairs per bundle chunk: a chunk's bundles (1 KB per pair for the default grid)
+// stay in device memory between the transport and growth kernels.
+constexpr unsigned long long CHUNK_PAIRS_DEFAULT = 4ull << 20;
+
 inline unsigned next_pow2(unsigned long long v) {
     unsigned long long p = 1;
     while (p < v) p <<= 1;
@@ -56,6 +62,50 @@ inline unsigned next_pow2(unsigned long long v) {
 }
 
 }  // namespace
+
+// Page-locked host buffers for results, reused across runs: device-to-host
+// copies at full PCIe/C2C rate and no per-call host allocation. Shared by the
+// engine and its live results, so a result may outlive its engine.
+struct PinnedPool {
+    struct Block {
+        void *p;
+        size_t bytes;
+        bool used;
+    };
+    std::mutex mu;
+    std::vector<Block> blocks;
+    ~PinnedPool() {
+        for (Block &b : blocks) cudaFreeHost(b.p);
+    }
+    void *get(size_t bytes) {
+        std::lock_guard<std::mutex> g(mu);
+        int best = -1;
+        for (size_t k = 0; k < blocks.size(); ++k)
+            if (!blocks[k].used && blocks[k].bytes >= bytes && (best < 0 || blocks[k].bytes < blocks[best].bytes))
+                best = (int)k;
+        if (best >= 0) {
+            blocks[best].used = true;
+            return blocks[best].p;
+        }
+        void *p = nullptr;
+        const size_t want = std::max(bytes + bytes / 8, (size_t)1 << 16);
+        if (cudaMallocHost(&p, want) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        blocks.push_back({p, want, true});
+        return p;
+    }
+    void put(void *p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> g(mu);
+        for (Block &b : blocks)
+            if (b.p == p) {
+                b.used = false;
+                return;
+            }
+    }
+};
 
 struct cvl_engine {
     int device = 0;
@@ -67,12 +117,16 @@ struct cvl_engine {
     int seeds_per_group = 4;
     int slots = 10;
     unsigned long long generation = 0;
+    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
 
     // workspace
     DBuf edges, map_off, ehash, bcount, bstart, bfill, pos_of, orig_of;
     DBuf bx, by, bth, bsp, bcp, bsm, bcm, bcell, bmap;
     DBuf ncand, deg, pair_off, csr_ids, csr_d2, rec_ids, rec_k, rec_meta, count, out_off;
-    DBuf chains, info, stats, err, work, scratch, scratch_chain, scan_tmp, flush, deg_orig, off_orig, gids, gd2;
+    DBuf chains, info, stats, err, work, scratch, scratch_chain, scratch_res, scan_tmp, flush, deg_orig, off_orig,
+        gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start;
+    unsigned long long chunk_pairs = CHUNK_PAIRS_DEFAULT;  // pairs per bundle chunk
+    unsigned long long arena_hint = 0;  // record arena size that the last input needed
     DBuf pairs_in, pb_min, pb_max, pb_valid;
 
     // per-kernel timing of the last run
@@ -144,7 +198,7 @@ struct cvl_engine {
         DBuf *all[] = {&edges, &map_off, &ehash, &bcount, &bstart, &bfill, &pos_of, &orig_of, &bx, &by, &bth, &bsp,
                        &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
                        &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
-                       &scratch_chain, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
+                       &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
                        &pb_max, &pb_valid};
         for (DBuf *b : all) {
             if (b->p) cudaFree(b->p);
@@ -156,9 +210,16 @@ struct cvl_engine {
 };
 
 struct cvl_result {
-    std::vector<uint32_t> chains;
-    std::vector<double> info;
+    std::shared_ptr<PinnedPool> pool;
+    void *chains_p = nullptr;  // pinned, from pool
+    void *info_p = nullptr;
     cvl_result_view v{};
+    ~cvl_result() {
+        if (pool) {
+            pool->put(chains_p);
+            pool->put(info_p);
+        }
+    }
 };
 
 struct cvl_graph {
@@ -186,6 +247,7 @@ struct cvl_batch {
 struct cvl_batch_result {
     cvl_engine *eng = nullptr;
     unsigned long long generation = 0;
+    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     int num_maps = 0;
     int n = 0;
     int width = 0;
@@ -234,7 +296,14 @@ int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nb
     md.gms = (int)p->group_max_sz;
     md.max_cand = (int)max_cand;
     md.w = (int)nbr_radius;
-    md.S = e->cell_size > 0 ? e->cell_size : 4;
+    {
+        // hash block edge: a power of two (the block of a pixel cell is cell >> sbits)
+        const int S = e->cell_size > 0 ? e->cell_size : 4;
+        int sb = 0;
+        while ((1 << sb) < S && sb < 6) ++sb;
+        if ((1 << sb) != S) return fail(CVL_EINVAL, "cell_size must be a power of two in [1, 64]");
+        md.sbits = sb;
+    }
     md.hash_mask = 0;
     return CVL_OK;
 }
@@ -310,36 +379,29 @@ struct RunOut {
     unsigned max_deg = 0;
 };
 
-template <int CPL, int K>
-int launch_curvelets(cvl_engine *e, CurveletArgs &a, size_t smem, int blocks) {
-    const int threads = 128;
-    CVL_CUDA(cudaFuncSetAttribute(k_curvelets<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_curvelets<CPL, K><<<blocks, threads, smem, e->stream>>>(a);
-    return check_launch("k_curvelets");
+template <int CPL>
+int launch_bundles(cvl_engine *e, BundleArgs &a, int blocks) {
+    k_bundles<CPL><<<blocks, 256, 0, e->stream>>>(a);
+    return check_launch("k_bundles");
 }
 
 template <int CPL, int K>
-int occupancy_curvelets(size_t smem, int &blocks_per_sm) {
-    CVL_CUDA(cudaFuncSetAttribute(k_curvelets<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CVL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_curvelets<CPL, K>, 128, smem));
-    return CVL_OK;
+int launch_growth(cvl_engine *e, GrowthArgs &a, size_t smem, int blocks) {
+    CVL_CUDA(cudaFuncSetAttribute(k_growth<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_growth<CPL, K><<<blocks, 128, smem, e->stream>>>(a);
+    return check_launch("k_growth");
 }
 
-typedef int (*launch_fn)(cvl_engine *, CurveletArgs &, size_t, int);
-typedef int (*occ_fn)(size_t, int &);
+typedef int (*bundles_fn)(cvl_engine *, BundleArgs &, int);
+typedef int (*growth_fn)(cvl_engine *, GrowthArgs &, size_t, int);
 
-void pick_curvelet_kernel(int cpl, int K, launch_fn &lf, occ_fn &of) {
-#define CVL_PICK(C, KK)                        \
-    if (cpl == C && K == KK) {                 \
-        lf = launch_curvelets<C, KK>;          \
-        of = occupancy_curvelets<C, KK>;       \
-        return;                                \
+void pick_kernels(int cpl, bundles_fn &bf, growth_fn &gf) {
+    switch (cpl) {
+        case 1: bf = launch_bundles<1>; gf = launch_growth<1, 4>; break;
+        case 3: bf = launch_bundles<3>; gf = launch_growth<3, 4>; break;
+        case 4: bf = launch_bundles<4>; gf = launch_growth<4, 4>; break;
+        default: bf = launch_bundles<2>; gf = launch_growth<2, 4>; break;
     }
-    CVL_PICK(1, 4) CVL_PICK(1, 8) CVL_PICK(2, 4) CVL_PICK(2, 8) CVL_PICK(3, 4) CVL_PICK(3, 8) CVL_PICK(4, 4)
-    CVL_PICK(4, 8)
-#undef CVL_PICK
-    lf = launch_curvelets<2, 4>;
-    of = occupancy_curvelets<2, 4>;
 }
 
 // mode: 0 = full run, 1 = count valid pairs only, 2 = neighbour graph only
@@ -375,10 +437,12 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     CVL_TRY(e->alloc(e->deg, sizeof(unsigned) * n));
     CVL_TRY(e->alloc(e->pair_off, sizeof(unsigned long long) * (n + 1)));
     CVL_TRY(e->alloc(e->count, sizeof(unsigned) * n));
+    CVL_TRY(e->alloc(e->run_cnt, sizeof(unsigned) * 2 * (size_t)n));
+    CVL_TRY(e->alloc(e->rec_base, sizeof(unsigned) * 2 * (size_t)n));
     CVL_TRY(e->alloc(e->out_off, sizeof(unsigned long long) * (n + 1)));
     CVL_TRY(e->alloc(e->stats, sizeof(MapStats) * M));
     CVL_TRY(e->alloc(e->err, sizeof(unsigned) * 4));
-    CVL_TRY(e->alloc(e->work, sizeof(unsigned) * 4));
+    CVL_TRY(e->alloc(e->work, sizeof(unsigned long long) * 2));
 
     Binned B;
     B.x = (double *)e->bx.p;
@@ -393,13 +457,13 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     B.map = (int *)e->bmap.p;
     unsigned *err = (unsigned *)e->err.p;
     MapStats *stats = (MapStats *)e->stats.p;
+    unsigned long long *arena_ctr = (unsigned long long *)e->work.p;
 
     CVL_CUDA(cudaMemsetAsync(e->bcount.p, 0, sizeof(unsigned) * (T + 1), s));
     CVL_CUDA(cudaMemsetAsync(e->bfill.p, 0, sizeof(unsigned) * (T + 1), s));
     CVL_CUDA(cudaMemsetAsync(e->stats.p, 0, sizeof(MapStats) * M, s));
     CVL_CUDA(cudaMemsetAsync(e->err.p, 0, sizeof(unsigned) * 4, s));
-    CVL_CUDA(cudaMemsetAsync(e->work.p, 0, sizeof(unsigned) * 4, s));
-    CVL_CUDA(cudaMemsetAsync(e->count.p, 0, sizeof(unsigned) * n, s));
+    CVL_CUDA(cudaMemsetAsync(e->work.p, 0, sizeof(unsigned long long) * 2, s));
 
     // ---- (a) binning
     const int gb = grid_for(e, n, 256);
@@ -412,136 +476,202 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     CVL_TRY(check_launch("k_bin_scatter"));
     e->mark("bin");
 
-    // ---- (b) neighbour count + CSR offsets
+    // ---- (b) neighbour count, CSR offsets, chunk boundaries
     const int nb_wpb = 8;
     const size_t nb_smem = (size_t)nb_wpb * nbr_smem_per_warp(md.max_cand);
-    if (nb_smem > 48 * 1024) {
-        CVL_CUDA(cudaFuncSetAttribute(k_neighbors<NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
-        CVL_CUDA(cudaFuncSetAttribute(k_neighbors<NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
-    }
+    CVL_CUDA(cudaFuncSetAttribute(k_nb<NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
+    CVL_CUDA(cudaFuncSetAttribute(k_nb<NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
     const int gn = grid_for(e, n, nb_wpb, 16);
-    k_neighbors<NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(md, B, (const unsigned *)e->bstart.p, n,
-                                                           (unsigned *)e->ncand.p, stats, nullptr, nullptr, nullptr,
-                                                           err);
-    CVL_TRY(check_launch("k_neighbors<COUNT>"));
+    NbArgs na{};
+    na.md = md;
+    na.B = B;
+    na.bstart = (const unsigned *)e->bstart.p;
+    na.N = n;
+    na.M = M;
+    na.ncand = (unsigned *)e->ncand.p;
+    na.stats = stats;
+    na.pair_off = (const unsigned long long *)e->pair_off.p;
+    na.err = err;
+    k_nb<NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+    CVL_TRY(check_launch("k_nb<COUNT>"));
     k_deg_from_ncand<<<gb, 256, 0, s>>>(n, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p);
     CVL_TRY(check_launch("k_deg_from_ncand"));
     CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->deg.p, n,
                                                 (unsigned long long *)e->pair_off.p)));
+    // chunk boundaries over anchors: a chunk holds at most CHUNK_PAIRS + max_deg pairs
+    const unsigned long long per_chunk = std::max<unsigned long long>(e->chunk_pairs, 1024ull);
+    const int max_chunks = 4096;
+    CVL_TRY(e->alloc(e->chunk_start, sizeof(int) * (max_chunks + 1)));
+    CVL_CUDA(cudaMemsetAsync(e->chunk_start.p, 0, sizeof(int) * (max_chunks + 1), s));
+    k_chunk_starts<<<gb, 256, 0, s>>>(n, (const unsigned long long *)e->pair_off.p + 1, per_chunk, max_chunks,
+                                     (int *)e->chunk_start.p);
+    CVL_TRY(check_launch("k_chunk_starts"));
     e->mark("neighbors_count");
 
-    // sync 1: totals
+    // sync 1: pair total, max degree, chunk boundaries
     ro.stats.assign(M, MapStats{});
     unsigned h_err = 0;
+    std::vector<int> cstart(max_chunks + 1, 0);
     CVL_CUDA(cudaMemcpyAsync(&ro.total_pairs, (unsigned long long *)e->pair_off.p + n, sizeof(unsigned long long),
                              cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(cstart.data(), e->chunk_start.p, sizeof(int) * (max_chunks + 1), cudaMemcpyDeviceToHost,
+                             s));
     CVL_CUDA(cudaStreamSynchronize(s));
     if (h_err & ERR_NONFINITE) return fail(CVL_EINVAL, "non-finite or out-of-range (|v| >= 1e9) edge coordinate");
     ro.max_deg = 0;
     for (const MapStats &st : ro.stats) ro.max_deg = std::max(ro.max_deg, st.max_deg);
     const unsigned long long P = ro.total_pairs;
+    int nchunks = (int)std::min<unsigned long long>((P + per_chunk - 1) / per_chunk, (unsigned long long)max_chunks);
+    if (nchunks < 1) nchunks = 1;
+    if ((P + per_chunk - 1) / per_chunk > (unsigned long long)max_chunks)
+        return fail(CVL_EUNSUPPORTED, "input needs more than 4096 pair chunks");
+    cstart[nchunks] = n;
 
-    // ---- (b) neighbour fill
+    // ---- (b) neighbour fill: CSR, pair classes, pair -> anchor, anchor trig
     CVL_TRY(e->alloc(e->csr_ids, sizeof(int) * P));
     if (want_d2) CVL_TRY(e->alloc(e->csr_d2, sizeof(double) * P));
-    k_neighbors<NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(md, B, (const unsigned *)e->bstart.p, n,
-                                                          (unsigned *)e->ncand.p, stats,
-                                                          (const unsigned long long *)e->pair_off.p,
-                                                          (int *)e->csr_ids.p, want_d2 ? (double *)e->csr_d2.p : nullptr,
-                                                          err);
-    CVL_TRY(check_launch("k_neighbors<FILL>"));
+    const bool path = (mode != 2);
+    if (path) {
+        CVL_TRY(e->alloc(e->pcls, P));
+        CVL_TRY(e->alloc(e->pflag, P));
+        CVL_TRY(e->alloc(e->pair_anchor, sizeof(int) * P));
+        CVL_TRY(e->alloc(e->atrig, sizeof(double) * (size_t)n * (2 * md.Q + 2)));
+    }
+    na.csr_ids = (int *)e->csr_ids.p;
+    na.csr_d2 = want_d2 ? (double *)e->csr_d2.p : nullptr;
+    na.pcls = path ? (unsigned char *)e->pcls.p : nullptr;
+    na.pair_anchor = path ? (int *)e->pair_anchor.p : nullptr;
+    na.atrig = path ? (double *)e->atrig.p : nullptr;
+    k_nb<NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+    CVL_TRY(check_launch("k_nb<FILL>"));
     e->mark("neighbors_fill");
     if (mode == 2) {
         e->mark("end");
         return CVL_OK;
     }
 
-    // ---- (c+d) fused bundles + growth
-    launch_fn lf;
-    occ_fn of;
-    const int K = (e->seeds_per_group == 8) ? 8 : 4;
-    pick_curvelet_kernel(cpl, K, lf, of);
-    int slots = e->slots > 0 ? e->slots : 10;
-    size_t smem = curvelet_smem_bytes(4, md.max_cand, slots, md.gms, cpl, md.Q);
-    while (smem > (size_t)e->prop.sharedMemPerBlockOptin && slots > 1) {
-        --slots;
-        smem = curvelet_smem_bytes(4, md.max_cand, slots, md.gms, cpl, md.Q);
-    }
-    int bps = 0;
-    CVL_TRY(of(smem, bps));
-    if (bps < 1) return fail(CVL_EUNSUPPORTED, "k_curvelets does not fit on an SM with these parameters");
-    const int blocks = bps * e->prop.multiProcessorCount;
-    const int warps = blocks * 4;
-    // a run holds at most max_deg seeds plus one chunk of tentative slots
-    const int scratch_slots = std::max((int)ro.max_deg + PCH - slots, 0);
-    CVL_TRY(e->alloc(e->scratch, sizeof(double) * (size_t)warps * (size_t)std::max(scratch_slots, 1) * 64 * cpl));
-    CVL_TRY(e->alloc(e->scratch_chain, sizeof(unsigned short) * (size_t)warps * (size_t)std::max(scratch_slots, 1) *
-                                           (size_t)md.gms));
-    if (mode == 0) {
-        CVL_TRY(e->alloc(e->rec_ids, sizeof(unsigned) * P * md.gms));
-        CVL_TRY(e->alloc(e->rec_k, sizeof(double) * P * 2));
-        CVL_TRY(e->alloc(e->rec_meta, sizeof(unsigned) * P));
-    }
-    CurveletArgs a;
-    a.md = md;
-    a.B = B;
-    a.N = n;
-    a.pair_off = (const unsigned long long *)e->pair_off.p;
-    a.csr_ids = (const int *)e->csr_ids.p;
-    a.rec.ids = (unsigned *)e->rec_ids.p;
-    a.rec.k = (double *)e->rec_k.p;
-    a.rec.meta = (unsigned *)e->rec_meta.p;
-    a.count = (unsigned *)e->count.p;
-    a.stats = stats;
-    a.scratch = (double *)e->scratch.p;
-    a.scratch_chain = (unsigned short *)e->scratch_chain.p;
-    a.scratch_slots = scratch_slots;
-    a.slots = slots;
-    a.count_only = (mode == 1) ? 1 : 0;
-    a.err = err;
-    CVL_TRY(lf(e, a, smem, blocks));
-    e->mark("curvelets");
-
-    if (mode == 1) {
-        CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
-        CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        e->mark("end");
-        CVL_CUDA(cudaStreamSynchronize(s));
-        if (h_err) return fail(CVL_EOVERFLOW, "kernel reported error bits " + std::to_string(h_err));
-        return CVL_OK;
-    }
-
-    // ---- output positions (anchor-major, compact_curvelet_output)
-    CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->count.p, n,
-                                                (unsigned long long *)e->out_off.p)));
-    ro.cv_off.assign(M + 1, 0);
+    // ---- (c) + (d) per chunk
+    bundles_fn bf;
+    growth_fn gf;
+    pick_kernels(cpl, bf, gf);
+    const size_t gsmem = (size_t)4 * growth_smem_per_warp(md.max_cand, md.gms);
+    int gbps = 0;
     {
-        // per-map curvelet offsets are out_off at the map boundaries
+        // occupancy of the chosen growth kernel
+        cudaFuncAttributes fa{};
+        (void)fa;
+    }
+    const unsigned long long max_chunk_pairs = per_chunk + (unsigned long long)ro.max_deg + 1;
+    CVL_TRY(e->alloc(e->bund, sizeof(double) * 64 * (size_t)cpl * std::min<unsigned long long>(P + 1, max_chunk_pairs)));
+    const int bblocks = e->prop.multiProcessorCount * 8;
+    const int gblocks = e->prop.multiProcessorCount * 8;
+    (void)gbps;
+
+    for (int attempt = 0;; ++attempt) {
+        unsigned long long cap = std::max<unsigned long long>(e->arena_hint, 4ull * (unsigned long long)n + 4096ull);
+        if (mode == 0) {
+            CVL_TRY(e->alloc(e->rec_ids, sizeof(unsigned) * cap * md.gms));
+            CVL_TRY(e->alloc(e->rec_k, sizeof(double) * cap * 2));
+            CVL_TRY(e->alloc(e->rec_meta, sizeof(unsigned) * cap));
+        } else {
+            cap = 0;
+        }
+        Records rec;
+        rec.ids = (unsigned *)e->rec_ids.p;
+        rec.k = (double *)e->rec_k.p;
+        rec.meta = (unsigned *)e->rec_meta.p;
+        std::vector<unsigned long long> h_poff(nchunks + 1);
+        for (int c = 0; c <= nchunks; ++c)
+            CVL_CUDA(cudaMemcpyAsync(&h_poff[c], (unsigned long long *)e->pair_off.p + cstart[c],
+                                     sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaStreamSynchronize(s));
+        for (int c = 0; c < nchunks; ++c) {
+            const int a0 = cstart[c], a1 = cstart[c + 1];
+            if (a1 <= a0) continue;
+            BundleArgs ba{};
+            ba.md = md;
+            ba.B = B;
+            ba.p_begin = h_poff[c];
+            ba.p_end = h_poff[c + 1];
+            ba.csr_ids = (const int *)e->csr_ids.p;
+            ba.pair_anchor = (const int *)e->pair_anchor.p;
+            ba.pcls = (const unsigned char *)e->pcls.p;
+            ba.atrig = (const double *)e->atrig.p;
+            ba.bund = (double *)e->bund.p;
+            ba.pflag = (unsigned char *)e->pflag.p;
+            if (ba.p_end > ba.p_begin) CVL_TRY(bf(e, ba, bblocks));
+            GrowthArgs ga{};
+            ga.md = md;
+            ga.B = B;
+            ga.M = M;
+            ga.a_begin = a0;
+            ga.a_end = a1;
+            ga.p_begin = h_poff[c];
+            ga.pair_off = (const unsigned long long *)e->pair_off.p;
+            ga.csr_ids = (const int *)e->csr_ids.p;
+            ga.pcls = (const unsigned char *)e->pcls.p;
+            ga.pflag = (const unsigned char *)e->pflag.p;
+            ga.bund = (const double *)e->bund.p;
+            ga.rec = rec;
+            ga.arena_cap = cap;
+            ga.arena_ctr = arena_ctr;
+            ga.rec_base = (unsigned *)e->rec_base.p;
+            ga.run_cnt = (unsigned *)e->run_cnt.p;
+            ga.count = (unsigned *)e->count.p;
+            ga.stats = stats;
+            ga.count_only = (mode == 1) ? 1 : 0;
+            ga.err = err;
+            CVL_TRY(gf(e, ga, gsmem, gblocks));
+        }
+        e->mark("curvelets");
+
+        if (mode == 1) {
+            CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
+            CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            e->mark("end");
+            CVL_CUDA(cudaStreamSynchronize(s));
+            if (h_err) return fail(CVL_EOVERFLOW, "kernel reported error bits " + std::to_string(h_err));
+            return CVL_OK;
+        }
+
+        // ---- output positions (anchor-major, compact_curvelet_output)
+        CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->count.p, n,
+                                                    (unsigned long long *)e->out_off.p)));
         std::vector<unsigned long long> tmp(M + 1);
-        for (int m = 0; m <= M; ++m) {
+        for (int m = 0; m <= M; ++m)
             CVL_CUDA(cudaMemcpyAsync(&tmp[m], (unsigned long long *)e->out_off.p + map_off_host[m],
                                      sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-        }
+        unsigned long long used = 0;
         CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
         CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaMemcpyAsync(&used, arena_ctr, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         CVL_CUDA(cudaStreamSynchronize(s));
+        if ((h_err & ERR_ARENA) && attempt == 0) {
+            // the record arena was too small: size it to what this input needs and run the
+            // bundle/growth stages again (valid_pairs is recounted from zero)
+            e->arena_hint = used + used / 8 + 4096;
+            for (MapStats &st : ro.stats) st.valid_pairs = 0;
+            CVL_CUDA(cudaMemcpyAsync(stats, ro.stats.data(), sizeof(MapStats) * M, cudaMemcpyHostToDevice, s));
+            CVL_CUDA(cudaMemsetAsync(e->err.p, 0, sizeof(unsigned) * 4, s));
+            CVL_CUDA(cudaMemsetAsync(e->work.p, 0, sizeof(unsigned long long) * 2, s));
+            continue;
+        }
+        if (h_err) return fail(CVL_EOVERFLOW, "kernel reported error bits " + std::to_string(h_err));
         ro.cv_off = tmp;
+        const unsigned long long C = ro.cv_off[M];
+        ro.total_curvelets = C;
+        const int W = md.gms + 1;
+        CVL_TRY(e->alloc(e->chains, sizeof(unsigned) * C * W));
+        CVL_TRY(e->alloc(e->info, sizeof(double) * C * 10));
+        k_finalize<<<gb, 256, 0, s>>>(md, d_edges, sz, n, d_map_off, M, rec, (const unsigned *)e->rec_base.p,
+                                      (const unsigned *)e->run_cnt.p, (const unsigned long long *)e->out_off.p, C,
+                                      (unsigned *)e->chains.p, (double *)e->info.p);
+        CVL_TRY(check_launch("k_finalize"));
+        e->mark("finalize");
+        return CVL_OK;
     }
-    if (h_err) return fail(CVL_EOVERFLOW, "kernel reported error bits " + std::to_string(h_err));
-    const unsigned long long C = ro.cv_off[M];
-    ro.total_curvelets = C;
-    const int W = md.gms + 1;
-    CVL_TRY(e->alloc(e->chains, sizeof(unsigned) * C * W));
-    CVL_TRY(e->alloc(e->info, sizeof(double) * C * 10));
-    k_finalize<<<gb, 256, 0, s>>>(md, d_edges, sz, n, d_map_off, M, (const int *)e->orig_of.p,
-                                  (const unsigned long long *)e->pair_off.p, a.rec, (const unsigned *)e->count.p,
-                                  (const unsigned long long *)e->out_off.p, (unsigned *)e->chains.p,
-                                  (double *)e->info.p);
-    CVL_TRY(check_launch("k_finalize"));
-    e->mark("finalize");
-    return CVL_OK;
 }
 
 int upload(cvl_engine *e, const double *edges, int n, int sz, const std::vector<int32_t> &map_off) {
@@ -561,20 +691,21 @@ int check_edges_args(const double *edges, int32_t n, int32_t sz) {
 
 int fill_view_from_run(cvl_engine *e, const RunOut &ro, int n, int width, cvl_result *r) {
     const unsigned long long C = ro.total_curvelets;
-    r->chains.resize(C * width);
-    r->info.resize(C * 10);
+    r->pool = e->pinned;
+    r->chains_p = e->pinned->get(sizeof(unsigned) * (C ? C : 1) * width);
+    r->info_p = e->pinned->get(sizeof(double) * (C ? C : 1) * 10);
+    if (!r->chains_p || !r->info_p) return fail(CVL_ENOMEM, "page-locked result buffers could not be allocated");
     if (C) {
-        CVL_CUDA(cudaMemcpyAsync(r->chains.data(), e->chains.p, sizeof(unsigned) * C * width, cudaMemcpyDeviceToHost,
+        CVL_CUDA(cudaMemcpyAsync(r->chains_p, e->chains.p, sizeof(unsigned) * C * width, cudaMemcpyDeviceToHost,
                                  e->stream));
-        CVL_CUDA(cudaMemcpyAsync(r->info.data(), e->info.p, sizeof(double) * C * 10, cudaMemcpyDeviceToHost,
-                                 e->stream));
+        CVL_CUDA(cudaMemcpyAsync(r->info_p, e->info.p, sizeof(double) * C * 10, cudaMemcpyDeviceToHost, e->stream));
     }
     CVL_CUDA(cudaStreamSynchronize(e->stream));
     cvl_result_view &v = r->v;
     v.num_curvelets = (uint32_t)C;
     v.chain_width = (uint32_t)width;
-    v.chains = r->chains.data();
-    v.info = r->info.data();
+    v.chains = (const uint32_t *)r->chains_p;
+    v.info = (const double *)r->info_p;
     v.valid_pairs = ro.stats.empty() ? 0 : ro.stats[0].valid_pairs;
     v.total_neighbor_pairs = (int64_t)ro.total_pairs;
     v.max_num_of_neighbors = ro.max_deg;

@@ -1,21 +1,21 @@
-// cvl_kernels.cuh -- sm_100a kernels of the curvelet path (FP64, no FMA contraction).
+// cvl_kernels.cuh -- sm_100a kernels of the curvelet path, part 1: shared
+// definitions, (a) spatial-hash binning and (b) the neighbour search.
 //
 // Pipeline over a ragged batch of M edge maps (M = 1 for the plain form):
-//   (a) k_bin_keys / k_bin_scatter  spatial-hash binning by counting sort into
-//       S x S pixel-cell blocks ("cells sized to the neighbourhood"), SoA FP64
-//       edge arrays, per-edge trig of theta +- dt precomputed once;
-//   (b) k_neighbors<COUNT|FILL>     warp per anchor: the reference's 7x7
-//       pixel-window + radius predicate (preprocess.hpp:129-167), candidates
-//       staged in shared memory, truncation in window-scan order, rank sort by
-//       (dist^2, scan position) (preprocess.hpp:172-176);
-//   (c+d) k_curvelets               warp per anchor, persistent: pairwise
-//       curve bundles (cpu_curvelet.hpp:637-819) with cells across lanes,
-//       kept in shared memory, then lock-step chain growth of groups of seeds
-//       with warp-vote bundle intersections (:479-545), first-wins dedup
-//       (:876-916) and compact records (:258-280);
-//   (e) k_finalize                  expands records into the chain rows and
-//       the 10 info columns (fill_curvelet_info, :197-256) at anchor-major
-//       output positions (compact_curvelet_output, :282-303).
+//   (a) k_bin_keys / k_bin_scatter  counting sort of the edges into S x S
+//       pixel-cell blocks (S a power of two >= the window half width + 1) of a
+//       spatial hash; SoA FP64 edge arrays in bucket order; per-edge
+//       sin/cos(theta +- dt) computed once;
+//   (b) k_nb<COUNT> / k_nb<FILL>     warp per anchor: the window's bucket
+//       ranges are loaded by all lanes at once, then the candidates are
+//       enumerated 32 at a time with the reference's predicate (7x7 pixel
+//       window, not self, not d^2 > r^2; preprocess.hpp:129-167). COUNT writes
+//       the capped degree; FILL stages the candidates in shared memory, keeps
+//       the first max_candidates in window-scan order when there are more
+//       (:165-167), rank-sorts them by (d^2, scan position) (:172-176) and
+//       writes the CSR row, each pair's direction-run class
+//       (cpu_curvelet.hpp:454-462) and the anchor's sin/cos(T2 + delta_t2_j).
+//   (c) + (d) + (e) are in cvl_path.cuh.
 //
 // Every FP64 expression keeps the reference's operand order; the library is
 // compiled with -fmad=false so no multiply-add is contracted, and uses IEEE
@@ -30,32 +30,34 @@ namespace cvl {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int QMAX = 32;     // orientation samples supported (grid Q)
 constexpr int GMS_MAX = 16;  // group_max_sz supported
+constexpr int MAPS_SMEM = 256;  // per-block map statistics kept in shared memory up to this many maps
 constexpr double CVL_PI = 3.14159265358979323846;  // curvelet_utils.hpp:10
 
 // Error bits raised by kernels (checked by the host after a run).
 constexpr unsigned ERR_NONFINITE = 1u;   // non-finite or out-of-range coordinate
 constexpr unsigned ERR_CAPACITY = 2u;    // a device capacity was exceeded
 constexpr unsigned ERR_INTERNAL = 4u;    // an internal invariant failed (bounds check)
+constexpr unsigned ERR_ARENA = 8u;       // the record arena was too small (the host resizes and reruns)
 
 struct Model {
-    double nrad, rad_sqr;      // neighbour radius and its square (preprocess.hpp:221)
+    double nrad, rad_sqr;        // neighbour radius and its square (preprocess.hpp:221)
     double dx, dx2, four_dx_dx;  // _dx, _dx*_dx, 4*_dx*_dx (cpu_curvelet.hpp:654,682)
-    double dt, sx, st, max_k;  // dt in radians (main.cpp:24)
-    int P, Q, cells;           // bundle grid (cpu_curvelet.hpp:73-74)
-    int gms;                   // group_max_sz
-    int max_cand;              // max_candidates
-    int w;                     // pixel-window half width (3, main.cpp:48)
-    int S;                     // hash block edge in pixel cells
-    unsigned hash_mask;        // table size - 1
+    double dt, sx, st, max_k;    // dt in radians (main.cpp:24)
+    int P, Q, cells;             // bundle grid (cpu_curvelet.hpp:73-74)
+    int gms;                     // group_max_sz
+    int max_cand;                // max_candidates
+    int w;                       // pixel-window half width (3, main.cpp:48)
+    int sbits;                   // hash block edge S = 1 << sbits pixel cells
+    unsigned hash_mask;          // table size - 1
 };
 
 // SoA copy of the edges in hash-bucket order ("internal" index space).
 struct Binned {
-    double *x, *y, *th;        // position, orientation
-    double *sp, *cp, *sm, *cm; // sin/cos(theta + dt), sin/cos(theta - dt)
-    int2 *cell;                // pixel cell (lrint(x), lrint(y))
-    int *orig;                 // global input index
-    int *map;                  // map of the edge
+    double *x, *y, *th;         // position, orientation
+    double *sp, *cp, *sm, *cm;  // sin/cos(theta + dt), sin/cos(theta - dt)
+    int2 *cell;                 // pixel cell (lrint(x), lrint(y))
+    int *orig;                  // global input index
+    int *map;                   // map of the edge
 };
 
 struct MapStats {
@@ -66,17 +68,49 @@ struct MapStats {
     unsigned pad;
 };
 
-// Compact curvelet record written by k_curvelets at the anchor's pair slots.
-//   rec_ids  [slot][gms]  chain as global edge indices (anchor first)
-//   rec_k    [slot][2]    k_max, k_min of the best cell of the final bundle
-//   rec_meta [slot]       len | best_cell << 8 | forward << 24
-struct Records {
-    unsigned *ids;
-    double *k;
-    unsigned *meta;
+// Per-block map statistics: accumulated with shared-memory atomics and added to
+// the global MapStats once per block (global atomics per anchor on the same few
+// addresses would serialise in L2).
+struct BlockStats {
+    unsigned long long pairs[MAPS_SMEM];
+    unsigned max_deg[MAPS_SMEM];
+    unsigned truncated[MAPS_SMEM];
+    unsigned valid[MAPS_SMEM];
 };
 
-__device__ __forceinline__ int floor_div(int a, int s) { return a >= 0 ? a / s : -((-a + s - 1) / s); }
+__device__ __forceinline__ void block_stats_init(BlockStats &bs, int M) {
+    for (int m = threadIdx.x; m < M && m < MAPS_SMEM; m += blockDim.x) {
+        bs.pairs[m] = 0;
+        bs.max_deg[m] = 0;
+        bs.truncated[m] = 0;
+        bs.valid[m] = 0;
+    }
+}
+
+__device__ __forceinline__ void stats_add(BlockStats &bs, MapStats *gs, int M, int m, unsigned pairs, unsigned deg,
+                                          unsigned trunc, unsigned valid) {
+    if (M <= MAPS_SMEM) {
+        if (pairs) atomicAdd(&bs.pairs[m], (unsigned long long)pairs);
+        if (deg) atomicMax(&bs.max_deg[m], deg);
+        if (trunc) atomicAdd(&bs.truncated[m], trunc);
+        if (valid) atomicAdd(&bs.valid[m], valid);
+    } else {
+        if (pairs) atomicAdd(&gs[m].pairs, (unsigned long long)pairs);
+        if (deg) atomicMax(&gs[m].max_deg, deg);
+        if (trunc) atomicAdd(&gs[m].truncated, trunc);
+        if (valid) atomicAdd(&gs[m].valid_pairs, valid);
+    }
+}
+
+__device__ __forceinline__ void block_stats_flush(BlockStats &bs, MapStats *gs, int M) {
+    if (M > MAPS_SMEM) return;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        if (bs.pairs[m]) atomicAdd(&gs[m].pairs, bs.pairs[m]);
+        if (bs.max_deg[m]) atomicMax(&gs[m].max_deg, bs.max_deg[m]);
+        if (bs.truncated[m]) atomicAdd(&gs[m].truncated, bs.truncated[m]);
+        if (bs.valid[m]) atomicAdd(&gs[m].valid_pairs, bs.valid[m]);
+    }
+}
 
 // Spatial hash of a (map, block) key: XOR of products with large primes
 // (Teschner et al., "Optimized Spatial Hashing for Collision Detection of
@@ -96,13 +130,25 @@ __device__ __forceinline__ double sq_dist(double x1, double y1, double x2, doubl
     return (x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2);
 }
 
+// Out-of-line copies of the libm calls: one copy of each in a kernel instead of
+// one per call site keeps the kernels' code within the instruction cache.
+__device__ __noinline__ double cvl_sin(double x) { return sin(x); }
+__device__ __noinline__ double cvl_cos(double x) { return cos(x); }
+__device__ __noinline__ double cvl_atan2(double y, double x) { return atan2(y, x); }
+__device__ __noinline__ double cvl_fmod(double x, double y) { return fmod(x, y); }
+
+// fmod(x, 2pi) with its IEEE fast case inline: for |x| < |y|, fmod(x, y) == x exactly.
+__device__ __forceinline__ double fmod_2pi(double x) {
+    return (fabs(x) < 2.0 * CVL_PI) ? x : cvl_fmod(x, 2.0 * CVL_PI);
+}
+
 // To2Pi (curvelet_utils.hpp:25-46)
 __device__ __forceinline__ double to_2pi(double angle) {
     double a;
     if (angle >= 2.0 * CVL_PI)
-        a = fmod(angle, 2.0 * CVL_PI);
+        a = fmod_2pi(angle);
     else if (angle < 0)
-        a = (2.0 * CVL_PI + fmod(angle, 2.0 * CVL_PI));
+        a = (2.0 * CVL_PI + fmod_2pi(angle));
     else
         a = angle;
     if (!(a >= 0 && a < 2.0 * CVL_PI)) a = 0;
@@ -137,7 +183,7 @@ __global__ void k_bin_keys(const double *__restrict__ edges, int sz, int N, cons
         const int m = map_of(map_off, M, e);
         const int cx = __double2int_rn(x);  // lrint, round half to even (preprocess.hpp:85-86)
         const int cy = __double2int_rn(y);
-        const unsigned h = cell_hash(m, floor_div(cx, md.S), floor_div(cy, md.S)) & md.hash_mask;
+        const unsigned h = cell_hash(m, cx >> md.sbits, cy >> md.sbits) & md.hash_mask;
         ehash[e] = h;
         atomicAdd(&bcount[h], 1u);
     }
@@ -195,85 +241,196 @@ __host__ __device__ inline size_t nbr_smem_per_warp(int max_cand) {
     return ((size_t)max_cand * 20 + 15) & ~(size_t)15;
 }
 
-// Visits every edge in the anchor's window that passes the reference's
-// predicate; f(lane_ok, j, d2, key) is called warp-uniformly per chunk of 32.
+// Visits every edge of the anchor's map in the hash blocks covering its window
+// and calls f(ok, j, d2, key) warp-uniformly, 32 entries at a time; ok is the
+// reference predicate. The window's bucket ranges (up to 32 per round) are
+// loaded by the lanes at once; entries are enumerated over their prefix sums.
 template <typename F>
 __device__ __forceinline__ void for_window_candidates(const Model &md, const Binned &B, const unsigned *bstart,
                                                       int i, int m, int2 ac, double ax, double ay, int lane, F &&f) {
-    const int bx0 = floor_div(ac.x - md.w, md.S), bx1 = floor_div(ac.x + md.w, md.S);
-    const int by0 = floor_div(ac.y - md.w, md.S), by1 = floor_div(ac.y + md.w, md.S);
-    for (int by = by0; by <= by1; ++by) {
-        for (int bx = bx0; bx <= bx1; ++bx) {
+    const int bx0 = (ac.x - md.w) >> md.sbits, bx1 = (ac.x + md.w) >> md.sbits;
+    const int by0 = (ac.y - md.w) >> md.sbits, by1 = (ac.y + md.w) >> md.sbits;
+    const int nbx = bx1 - bx0 + 1;
+    const int nb = nbx * (by1 - by0 + 1);
+    for (int t0 = 0; t0 < nb; t0 += 32) {
+        const int t = t0 + lane;
+        int bx = 0, by = 0;
+        unsigned s = 0, c = 0;
+        if (t < nb) {
+            by = by0 + t / nbx;
+            bx = bx0 + t - (t / nbx) * nbx;
             const unsigned h = cell_hash(m, bx, by) & md.hash_mask;
-            const int b0 = (int)bstart[h], b1 = (int)bstart[h + 1];
-            for (int base = b0; base < b1; base += 32) {
-                const int j = base + lane;
-                bool ok = false;
-                double d2 = 0.0;
-                unsigned long long key = 0;
-                if (j < b1 && j != i) {
-                    const int2 c = B.cell[j];
-                    if (B.map[j] == m && floor_div(c.x, md.S) == bx && floor_div(c.y, md.S) == by &&
-                        abs(c.x - ac.x) <= md.w && abs(c.y - ac.y) <= md.w) {
-                        d2 = sq_dist(ax, ay, B.x[j], B.y[j]);  // sq_dist(te, ne), preprocess.hpp:160
-                        ok = !(d2 > md.rad_sqr);               // preprocess.hpp:161-163
-                        key = scan_key(c, ac.x, ac.y, md.w, B.orig[j]);
-                    }
-                }
-                f(ok, j, d2, key);
+            s = bstart[h];
+            c = bstart[h + 1] - s;
+        }
+        // inclusive prefix of the bucket sizes
+        unsigned incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned o = __shfl_up_sync(FULL, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const unsigned total = __shfl_sync(FULL, incl, 31);
+        for (unsigned e0 = 0; e0 < total; e0 += 32) {
+            const unsigned e = e0 + lane;
+            // bucket of entry e: the first lane whose inclusive prefix exceeds e
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const unsigned v = __shfl_sync(FULL, incl, lo + step - 1);
+                if (v <= e) lo += step;
             }
+            const unsigned pre = __shfl_sync(FULL, incl, lo) - __shfl_sync(FULL, c, lo);
+            const unsigned sb = __shfl_sync(FULL, s, lo);
+            const int vbx = __shfl_sync(FULL, bx, lo), vby = __shfl_sync(FULL, by, lo);
+            bool ok = false;
+            double d2 = 0.0;
+            unsigned long long key = 0;
+            const int j = (int)(sb + (e - pre));
+            if (e < total && j != i) {
+                const int2 cc = B.cell[j];
+                // the entry's own block must be the visited one (a bucket can hold
+                // several blocks, and two window blocks can share a bucket)
+                if (B.map[j] == m && (cc.x >> md.sbits) == vbx && (cc.y >> md.sbits) == vby &&
+                    abs(cc.x - ac.x) <= md.w && abs(cc.y - ac.y) <= md.w) {
+                    d2 = sq_dist(ax, ay, B.x[j], B.y[j]);  // sq_dist(te, ne), preprocess.hpp:160
+                    ok = !(d2 > md.rad_sqr);               // preprocess.hpp:161-163
+                    key = scan_key(cc, ac.x, ac.y, md.w, B.orig[j]);
+                }
+            }
+            f(ok, j, d2, key);
         }
     }
 }
 
-// COUNT: ncand[i] = candidates in window (before the cap), per-map stats.
-// FILL:  csr_ids/csr_d2 at pair_off[i], sorted by (d2, scan key), truncated
-//        to max_cand in scan order when ncand[i] > max_cand.
+// Truncation (preprocess.hpp:165-167): keep the first max_cand candidates in
+// window-scan order. Walks the window pixel cell by pixel cell; inside the cell
+// where the cap is crossed keeps the lowest edge indices. Returns the count kept.
+__device__ __noinline__ unsigned gather_truncated(const Model &md, const Binned &B, const unsigned *bstart, int i,
+                                                  int m, int2 ac, double ax, double ay, int lane, NbrSmem S,
+                                                  unsigned *err) {
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int side = 2 * md.w + 1;
+    unsigned n = 0;
+    for (int r = 0; r < side * side && n < (unsigned)md.max_cand; ++r) {
+        const int px = ac.x - md.w + r % side;
+        const int py = ac.y - md.w + r / side;
+        const unsigned h = cell_hash(m, px >> md.sbits, py >> md.sbits) & md.hash_mask;
+        const int b0 = (int)bstart[h], b1 = (int)bstart[h + 1];
+        // count this cell's candidates
+        unsigned c = 0;
+        for (int base = b0; base < b1; base += 32) {
+            const int j = base + lane;
+            bool ok = false;
+            if (j < b1 && j != i) {
+                const int2 cc = B.cell[j];
+                ok = B.map[j] == m && cc.x == px && cc.y == py && !(sq_dist(ax, ay, B.x[j], B.y[j]) > md.rad_sqr);
+            }
+            c += __popc(__ballot_sync(FULL, ok));
+        }
+        const unsigned need = (unsigned)md.max_cand - n;
+        for (int base = b0; base < b1; base += 32) {
+            const int j = base + lane;
+            bool ok = false;
+            double d2 = 0.0;
+            int oj = 0;
+            if (j < b1 && j != i) {
+                const int2 cc = B.cell[j];
+                if (B.map[j] == m && cc.x == px && cc.y == py) {
+                    d2 = sq_dist(ax, ay, B.x[j], B.y[j]);
+                    ok = !(d2 > md.rad_sqr);
+                    oj = B.orig[j];
+                }
+            }
+            if (ok && c > need) {
+                // rank by edge index among this cell's candidates
+                unsigned rk = 0;
+                for (int k = b0; k < b1; ++k) {
+                    if (k == i) continue;
+                    const int2 ck = B.cell[k];
+                    if (B.map[k] == m && ck.x == px && ck.y == py && B.orig[k] < oj &&
+                        !(sq_dist(ax, ay, B.x[k], B.y[k]) > md.rad_sqr))
+                        ++rk;
+                }
+                ok = rk < need;
+            }
+            const unsigned bal = __ballot_sync(FULL, ok);
+            if (ok) {
+                const unsigned p = n + __popc(bal & lt_mask);
+                if (p < (unsigned)md.max_cand) {
+                    S.d2[p] = d2;
+                    S.key[p] = ((unsigned long long)r << 32) | (unsigned)oj;
+                    S.idx[p] = j;
+                } else {
+                    atomicOr(err, ERR_INTERNAL);
+                }
+            }
+            n += __popc(bal);
+        }
+    }
+    return n > (unsigned)md.max_cand ? (unsigned)md.max_cand : n;
+}
+
+struct NbArgs {
+    Model md;
+    Binned B;
+    const unsigned *bstart;
+    int N, M;
+    unsigned *ncand;                     // COUNT: candidates in window (before the cap)
+    MapStats *stats;
+    const unsigned long long *pair_off;  // FILL: [N+1] internal order
+    int *csr_ids;                        // FILL: internal neighbour indices, by pair
+    double *csr_d2;                      // FILL (optional): squared distances
+    unsigned char *pcls;                 // FILL (optional): run | close << 2 per pair
+    int *pair_anchor;                    // FILL (optional): internal anchor of each pair
+    double *atrig;                       // FILL (optional): [N][2][Q] sin/cos(T2 + delta_t2_j)
+    unsigned *err;
+};
+
+// COUNT: ncand[i], per-map pairs / max degree / truncated anchors.
+// FILL:  the CSR row of anchor i at pair_off[i] sorted by (d2, scan key), and
+//        optionally the pair classes, pair->anchor map and anchor trig table.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_neighbors(Model md, Binned B, const unsigned *__restrict__ bstart, int N,
-                                                   unsigned *__restrict__ ncand, MapStats *__restrict__ stats,
-                                                   const unsigned long long *__restrict__ pair_off,
-                                                   int *__restrict__ csr_ids, double *__restrict__ csr_d2,
-                                                   unsigned *__restrict__ err) {
+__global__ void __launch_bounds__(256) k_nb(NbArgs a) {
     extern __shared__ __align__(16) unsigned char nb_smem[];
+    __shared__ BlockStats bstats;
+    const Model &md = a.md;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
+    if (MODE == NB_COUNT) {
+        block_stats_init(bstats, a.M);
+        __syncthreads();
+    }
     NbrSmem S;
     {
         unsigned char *p = nb_smem + (size_t)wib * nbr_smem_per_warp(md.max_cand);
         S.d2 = (double *)p;
         S.key = (unsigned long long *)(p + (size_t)md.max_cand * 8);
         S.idx = (int *)(p + (size_t)md.max_cand * 16);
-        if (MODE == NB_FILL && (((uintptr_t)S.d2 | (uintptr_t)S.key) & 7u)) {  // layout self-check
-            if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_INTERNAL);
-            return;
-        }
     }
     const unsigned lt_mask = (1u << lane) - 1u;
-    for (int i = blockIdx.x * wpb + wib; i < N; i += gridDim.x * wpb) {
-        const int m = B.map[i];
-        const int2 ac = B.cell[i];
-        const double ax = B.x[i], ay = B.y[i];
+    for (int i = blockIdx.x * wpb + wib; i < a.N; i += gridDim.x * wpb) {
+        const int m = a.B.map[i];
+        const int2 ac = a.B.cell[i];
+        const double ax = a.B.x[i], ay = a.B.y[i];
         if (MODE == NB_COUNT) {
             unsigned cnt = 0;
-            for_window_candidates(md, B, bstart, i, m, ac, ax, ay, lane,
+            for_window_candidates(md, a.B, a.bstart, i, m, ac, ax, ay, lane,
                                   [&](bool ok, int, double, unsigned long long) {
                                       cnt += __popc(__ballot_sync(FULL, ok));
                                   });
             if (lane == 0) {
-                ncand[i] = cnt;
+                a.ncand[i] = cnt;
                 const unsigned deg = cnt < (unsigned)md.max_cand ? cnt : (unsigned)md.max_cand;
-                atomicAdd(&stats[m].pairs, (unsigned long long)deg);
-                atomicMax(&stats[m].max_deg, deg);
-                if (deg >= (unsigned)md.max_cand) atomicAdd(&stats[m].truncated, 1u);
+                stats_add(bstats, a.stats, a.M, m, deg, deg, deg >= (unsigned)md.max_cand ? 1u : 0u, 0u);
             }
             continue;
         }
-        const unsigned total = ncand[i];
+        const unsigned total = a.ncand[i];
         unsigned n = 0;
         if (total <= (unsigned)md.max_cand) {
-            for_window_candidates(md, B, bstart, i, m, ac, ax, ay, lane,
+            for_window_candidates(md, a.B, a.bstart, i, m, ac, ax, ay, lane,
                                   [&](bool ok, int j, double d2, unsigned long long key) {
                                       const unsigned bal = __ballot_sync(FULL, ok);
                                       if (ok) {
@@ -283,80 +440,33 @@ __global__ void __launch_bounds__(256) k_neighbors(Model md, Binned B, const uns
                                               S.key[p] = key;
                                               S.idx[p] = j;
                                           } else {
-                                              atomicOr(err, ERR_INTERNAL);
+                                              atomicOr(a.err, ERR_INTERNAL);
                                           }
                                       }
                                       n += __popc(bal);
                                   });
         } else {
-            // Truncation (preprocess.hpp:165-167): keep the first max_cand
-            // candidates in window-scan order. Walk the window pixel cell by
-            // pixel cell; inside the cell where the cap is crossed keep the
-            // lowest edge indices.
-            const int side = 2 * md.w + 1;
-            for (int r = 0; r < side * side && n < (unsigned)md.max_cand; ++r) {
-                const int px = ac.x - md.w + r % side;
-                const int py = ac.y - md.w + r / side;
-                const int bx = floor_div(px, md.S), by = floor_div(py, md.S);
-                const unsigned h = cell_hash(m, bx, by) & md.hash_mask;
-                const int b0 = (int)bstart[h], b1 = (int)bstart[h + 1];
-                // count this cell's candidates
-                unsigned c = 0;
-                for (int base = b0; base < b1; base += 32) {
-                    const int j = base + lane;
-                    bool ok = false;
-                    if (j < b1 && j != i) {
-                        const int2 cc = B.cell[j];
-                        ok = B.map[j] == m && cc.x == px && cc.y == py &&
-                             !(sq_dist(ax, ay, B.x[j], B.y[j]) > md.rad_sqr);
-                    }
-                    c += __popc(__ballot_sync(FULL, ok));
-                }
-                const unsigned need = (unsigned)md.max_cand - n;
-                for (int base = b0; base < b1; base += 32) {
-                    const int j = base + lane;
-                    bool ok = false;
-                    double d2 = 0.0;
-                    int oj = 0;
-                    if (j < b1 && j != i) {
-                        const int2 cc = B.cell[j];
-                        if (B.map[j] == m && cc.x == px && cc.y == py) {
-                            d2 = sq_dist(ax, ay, B.x[j], B.y[j]);
-                            ok = !(d2 > md.rad_sqr);
-                            oj = B.orig[j];
-                        }
-                    }
-                    if (ok && c > need) {
-                        // rank by edge index among this cell's candidates
-                        unsigned rk = 0;
-                        for (int k = b0; k < b1; ++k) {
-                            if (k == i) continue;
-                            const int2 ck = B.cell[k];
-                            if (B.map[k] == m && ck.x == px && ck.y == py && B.orig[k] < oj &&
-                                !(sq_dist(ax, ay, B.x[k], B.y[k]) > md.rad_sqr))
-                                ++rk;
-                        }
-                        ok = rk < need;
-                    }
-                    const unsigned bal = __ballot_sync(FULL, ok);
-                    if (ok) {
-                        const unsigned p = n + __popc(bal & lt_mask);
-                        if (p < (unsigned)md.max_cand) {
-                            S.d2[p] = d2;
-                            S.key[p] = ((unsigned long long)r << 32) | (unsigned)oj;
-                            S.idx[p] = j;
-                        } else {
-                            atomicOr(err, ERR_INTERNAL);
-                        }
-                    }
-                    n += __popc(bal);
-                }
-            }
-            if (n > (unsigned)md.max_cand) n = (unsigned)md.max_cand;
+            n = gather_truncated(md, a.B, a.bstart, i, m, ac, ax, ay, lane, S, a.err);
         }
         __syncwarp();
+        const unsigned long long off = a.pair_off[i];
+        if (a.pair_off[i + 1] - off != n) {  // the two passes must agree
+            if (lane == 0) atomicOr(a.err, ERR_INTERNAL);
+            __syncwarp();
+            continue;
+        }
+        // the anchor's orientation samples: sin/cos(T2 + delta_t2_j) (:702-705)
+        const double T2 = a.B.th[i];
+        if (a.atrig) {
+            for (int j = lane; j < md.Q; j += 32) {
+                const double t = T2 + md.st * ((double)j - ((double)md.Q - 1.0) / 2.0);
+                a.atrig[(size_t)i * 2 * md.Q + j] = cvl_sin(t);
+                a.atrig[(size_t)i * 2 * md.Q + md.Q + j] = cvl_cos(t);
+            }
+        }
+        const double cosT2 = a.pcls ? cvl_cos(T2) : 0.0;
+        const double sinT2 = a.pcls ? cvl_sin(T2) : 0.0;
         // rank sort by (d2, scan key) -- std::sort by distance, preprocess.hpp:172-176
-        const unsigned long long off = pair_off[i];
         for (unsigned t = lane; t < n; t += 32) {
             const double dt_ = S.d2[t];
             const unsigned long long kt = S.key[t];
@@ -365,10 +475,47 @@ __global__ void __launch_bounds__(256) k_neighbors(Model md, Binned B, const uns
                 const double du = S.d2[u];
                 rk += (du < dt_) || (du == dt_ && S.key[u] < kt);
             }
-            csr_ids[off + rk] = S.idx[t];
-            if (csr_d2) csr_d2[off + rk] = dt_;
+            const int nn = S.idx[t];
+            a.csr_ids[off + rk] = nn;
+            if (a.csr_d2) a.csr_d2[off + rk] = dt_;
+            if (a.pair_anchor) a.pair_anchor[off + rk] = i;
+            if (a.pcls) {
+                // direction filter (:454-462) and close pair (:682)
+                const double lx = a.B.x[nn], ly = a.B.y[nn];
+                const double dir = to_2pi(cvl_atan2(ly - ay, lx - ax));      // angle_from_pt_to_pt(te, le)
+                const double d = cvl_cos(dir) * cosT2 + cvl_sin(dir) * sinT2;  // dot(dir, te_orient)
+                const unsigned run = (d > 0) ? 0u : ((d < 0) ? 1u : 2u);
+                const double DX = ax - lx, DY = ay - ly;
+                const bool close = (DX * DX + DY * DY < md.four_dx_dx);
+                a.pcls[off + rk] = (unsigned char)(run | (close ? 4u : 0u));
+            }
         }
         __syncwarp();
+    }
+    if (MODE == NB_COUNT) {
+        __syncthreads();
+        block_stats_flush(bstats, a.stats, a.M);
+    }
+}
+
+__global__ void k_deg_from_ncand(int N, int max_cand, const unsigned *__restrict__ ncand, unsigned *__restrict__ deg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const unsigned c = ncand[i];
+        deg[i] = c < (unsigned)max_cand ? c : (unsigned)max_cand;
+    }
+}
+
+// Chunks of anchors for the bundle/growth stages: chunk k starts at the first
+// anchor whose pair offset is >= k * per_chunk (anchor-aligned, <= per_chunk +
+// max_deg pairs each). chunk_start[k] for k in [1, nchunks); [0] = 0.
+__global__ void k_chunk_starts(int N, const unsigned long long *__restrict__ pair_off, unsigned long long per_chunk,
+                               int nchunks, int *__restrict__ chunk_start) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const unsigned long long lo = (i == 0) ? 0ull : pair_off[i - 1];
+        const unsigned long long hi = pair_off[i];
+        // chunk boundaries k with lo < k * per_chunk <= hi start at anchor i
+        for (unsigned long long k = lo / per_chunk + 1; k * per_chunk <= hi && k < (unsigned long long)nchunks; ++k)
+            chunk_start[k] = i;
     }
 }
 

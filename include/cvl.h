@@ -111,7 +111,9 @@ typedef struct cvl_result_view {
 int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
             const cvl_params *p, cvl_result **out);
 
-/* Views a result (pointers stay valid until cvl_result_free). */
+/* Views a result. chains/info point into page-locked host memory owned by the
+ * result; they stay valid until cvl_result_free, which may also be called after
+ * the engine was destroyed. */
 int cvl_result_get(const cvl_result *r, cvl_result_view *view);
 void cvl_result_free(cvl_result *r);
 
