@@ -228,31 +228,51 @@ def run_reference(args, maps, cfg, world, rank):
     print(json.dumps(line))
 
 
+def _stage_sums(times) -> dict:
+    """Per-stage device ms of one run, summed over chunks."""
+    out = {}
+    for name, ms in times:
+        out[name] = out.get(name, 0.0) + ms
+    return out
+
+
+def _plain_device_ms(eng, maps, steps: int) -> float:
+    """Mean device ms per step of the plain form: one map per launch, maps resident."""
+    singles = [eng.upload_batch([m]) for m in maps]
+    for b in singles[:2]:
+        eng.run_batch(b).close()
+    total = 0.0
+    for _ in range(steps):
+        eng.flush_l2()
+        for b in singles:
+            r = eng.run_batch(b)
+            total += r.stats()["device_ms"]
+            r.close()
+    for b in singles:
+        b.close()
+    return total / steps
+
+
 def run_ours(args, maps, cfg, world, rank, local, pg):
     import curvelet_construction_on_gpu_b200 as cvl
     eng = cvl.Engine(device=local)
     n_edges = int(sum(m.shape[0] for m in maps))
     batch = eng.upload_batch(maps)
-    # pairs that get a full bundle computation (not a close pair), from the neighbour graph
-    nonclose = 0
-    for m in maps:
-        g = eng.build_neighbor_graph(m, 3.5, 3, 128)
-        nonclose += int(np.count_nonzero(g.neighbor_dist2 >= 4 * 0.4 * 0.4))
-        del g
     fp64_peak = eng.fp64_peak_tflops() if rank == 0 else None
 
-    for _ in range(max(args.warmup, 3) if args.warmup >= 3 else args.warmup):
+    for _ in range(args.warmup):
         r = eng.run_batch(batch)
         r.close()
     _barrier(pg)
-    step_ms, kern = [], []
+    step_ms, kern, launches = [], [], 0
     with _Clocks(local) as clk:
         for _ in range(args.steps):
             eng.flush_l2()
             r = eng.run_batch(batch)
             st = r.stats()
             step_ms.append(st["device_ms"])
-            kern.append(dict(eng.kernel_times()))
+            launches = int(st["launches"])
+            kern.append(_stage_sums(eng.kernel_times()))
             r.close()
     _barrier(pg)
     sum_ms = _max_over_ranks(pg, float(np.sum(step_ms)))
@@ -261,30 +281,48 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     last = eng.run_batch(batch)
     stats = last.stats()
     n_curv = int(stats["num_curvelets"])
+    nonclose = int(stats["total_pairs"]) - int(stats["close_pairs"])
     last.close()
 
-    # e2e through the public one-shot call (plain form: one map per call)
+    plain = None
+    if len(maps) > 1:
+        pms = _plain_device_ms(eng, maps, max(1, min(args.steps, 3)))
+        pms = _max_over_ranks(pg, pms)
+        plain = {"value": _sum_over_ranks(pg, float(n_edges)) / (pms / 1e3), "unit": METRIC, "ms_per_step": pms,
+                 "form": "one map per launch, maps resident, same engine"}
+
+    # e2e through the public C ABI with host buffers: the one-shot call for a
+    # single map, the batch calls (upload, run, download every map) for a batch
     e2e = None
     if not args.no_e2e:
         pinned = [_pinned(m) for m in maps]
-        for m in pinned[: min(2, len(pinned))]:
-            eng.run(m)
+        if len(maps) == 1:
+            eng.run(pinned[0])
         _barrier(pg)
         t0 = time.perf_counter()
         bo = 0
         for _ in range(args.steps):
-            for m in pinned:
-                res = eng.run(m)
+            if len(maps) == 1:
+                res = eng.run(pinned[0])
                 bo += res.chains.nbytes + res.info.nbytes
+            else:
+                b = eng.upload_batch(pinned)
+                br = eng.run_batch(b)
+                for mi in range(len(maps)):
+                    res = br.map(mi)
+                    bo += res.chains.nbytes + res.info.nbytes
+                br.close()
+                b.close()
         wall = time.perf_counter() - t0
         wall = _max_over_ranks(pg, wall)
         e2e = {"value": _sum_over_ranks(pg, float(n_edges)) * args.steps / wall, "unit": METRIC,
                "h2d_bytes_per_step": int(sum(m.nbytes for m in maps)), "d2h_bytes_per_step": int(bo // args.steps),
-               "path": "cvl_run (C ABI), one map per call, pinned host edges"}
+               "path": ("cvl_run (C ABI), pinned host edges" if len(maps) == 1 else
+                        "cvl_batch_upload + cvl_batch_run + cvl_batch_result_map (C ABI), pinned host edges")}
 
     if rank != 0:
         return
-    curv_ms = float(np.mean([k.get("curvelets", 0.0) for k in kern]))
+    curv_ms = float(np.mean([k.get("bundles", 0.0) for k in kern]))
     flops = FLOPS_PER_PAIR_CELL * 63 * nonclose
     achieved = flops / (curv_ms / 1e3) / 1e12 if curv_ms > 0 else 0.0
     clocks = clk.summary()
@@ -298,15 +336,18 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
                        valid_pairs_per_gpu=int(stats["valid_pairs"]), parallelism=f"replicas x{world}", **cfg),
         "curvelets_per_s": n_curv * world * args.steps / (sum_ms / 1e3),
         "stage_ms": stage_ms,
-        "roofline": {"bound": "fp64", "kernel": "k_curvelets", "achieved": achieved, "peak": fp64_peak,
+        "roofline": {"bound": "fp64", "kernel": "k_bundles", "achieved": achieved, "peak": fp64_peak,
                      "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if fp64_peak else None,
                      "peak_source": "measured DFMA loop (cvl_measure_fp64_peak), 2 flops per FMA",
                      "work": f"{FLOPS_PER_PAIR_CELL} flops x 63 cells x {nonclose} non-close pairs",
                      "traffic": None},
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "clocks": clocks,
         "e2e": e2e,
     }
+    if plain is not None:
+        line["plain"] = plain
+        line["batched_vs_plain"] = value / plain["value"]
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = _cpu_baseline(maps)
     print(json.dumps(line))

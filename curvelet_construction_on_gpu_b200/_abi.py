@@ -50,6 +50,12 @@ class CvlGraphView(C.Structure):
                 ("neighbor_dist2", C.POINTER(C.c_double))]
 
 
+class CvlBatchStats(C.Structure):
+    _fields_ = [("device_ms", C.c_double), ("num_curvelets", C.c_uint64), ("valid_pairs", C.c_uint64),
+                ("total_pairs", C.c_uint64), ("close_pairs", C.c_uint64), ("max_num_of_neighbors", C.c_uint32),
+                ("truncated_anchors", C.c_uint32), ("num_maps", C.c_uint32), ("launches", C.c_uint32)]
+
+
 # (name, restype, argtypes) of every entry point declared in include/cvl.h
 _vp = C.c_void_p
 _dp = C.POINTER(C.c_double)
@@ -75,8 +81,7 @@ SIGNATURES = [
     ("cvl_batch_free", None, [_vp]),
     ("cvl_batch_run", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.POINTER(_vp)]),
     ("cvl_batch_result_map", C.c_int, [_vp, C.c_int32, C.POINTER(CvlResultView)]),
-    ("cvl_batch_result_stats", C.c_int, [_vp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
-                                         C.POINTER(C.c_uint64)]),
+    ("cvl_batch_result_stats", C.c_int, [_vp, C.POINTER(CvlBatchStats)]),
     ("cvl_batch_result_free", None, [_vp]),
     ("cvl_engine_flush_l2", C.c_int, [_vp]),
     ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),

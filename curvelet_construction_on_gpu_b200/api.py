@@ -292,11 +292,9 @@ class BatchResult:
         self._eng, self._h, self.num_maps = eng, h, num_maps
 
     def stats(self) -> dict:
-        ms = C.c_double(0)
-        nc, vp, tp = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
-        check(self._eng._lib.cvl_batch_result_stats(self._h, C.byref(ms), C.byref(nc), C.byref(vp), C.byref(tp)),
-              "cvl_batch_result_stats")
-        return dict(device_ms=ms.value, num_curvelets=nc.value, valid_pairs=vp.value, total_pairs=tp.value)
+        st = _abi.CvlBatchStats()
+        check(self._eng._lib.cvl_batch_result_stats(self._h, C.byref(st)), "cvl_batch_result_stats")
+        return {name: getattr(st, name) for name, _ in st._fields_}
 
     def map(self, m: int) -> Result:
         v = CvlResultView()

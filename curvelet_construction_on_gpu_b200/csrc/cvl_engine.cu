@@ -255,6 +255,7 @@ struct cvl_batch_result {
     std::vector<MapStats> stats;
     std::vector<unsigned long long> cv_off;  // per-map curvelet offsets [M+1]
     double device_ms = 0.0;
+    int launches = 0;
     bool downloaded = false;
     std::vector<uint32_t> chains;
     std::vector<double> info;
@@ -602,6 +603,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
             ba.bund = (double *)e->bund.p;
             ba.pflag = (unsigned char *)e->pflag.p;
             if (ba.p_end > ba.p_begin) CVL_TRY(bf(e, ba, bblocks));
+            e->mark("bundles");
             GrowthArgs ga{};
             ga.md = md;
             ga.B = B;
@@ -624,8 +626,8 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
             ga.count_only = (mode == 1) ? 1 : 0;
             ga.err = err;
             CVL_TRY(gf(e, ga, gsmem, gblocks));
+            e->mark("growth");
         }
-        e->mark("curvelets");
 
         if (mode == 1) {
             CVL_CUDA(cudaMemcpyAsync(ro.stats.data(), stats, sizeof(MapStats) * M, cudaMemcpyDeviceToHost, s));
@@ -1050,6 +1052,7 @@ int cvl_batch_run(cvl_engine *e, const cvl_batch *b, const cvl_params *p, cvl_ba
     r->stats = ro.stats;
     r->cv_off = ro.cv_off;
     r->device_ms = e->last_device_ms;
+    r->launches = e->last_launches;
     *out = r;
     return CVL_OK;
 }
@@ -1087,18 +1090,21 @@ int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view) 
     return CVL_OK;
 }
 
-int cvl_batch_result_stats(const cvl_batch_result *r, double *device_ms, uint64_t *num_curvelets,
-                           uint64_t *valid_pairs, uint64_t *total_pairs) {
-    if (!r) return fail(CVL_EINVAL, "result is NULL");
-    uint64_t vp = 0, tp = 0;
-    for (const MapStats &s : r->stats) {
-        vp += s.valid_pairs;
-        tp += s.pairs;
+int cvl_batch_result_stats(const cvl_batch_result *r, cvl_batch_stats *out) {
+    if (!r || !out) return fail(CVL_EINVAL, "result/out is NULL");
+    cvl_batch_stats st{};
+    for (const MapStats &m : r->stats) {
+        st.valid_pairs += m.valid_pairs;
+        st.total_pairs += m.pairs;
+        st.close_pairs += m.close_pairs;
+        st.max_num_of_neighbors = std::max<uint32_t>(st.max_num_of_neighbors, m.max_deg);
+        st.truncated_anchors += m.truncated;
     }
-    if (device_ms) *device_ms = r->device_ms;
-    if (num_curvelets) *num_curvelets = r->cv_off[r->num_maps];
-    if (valid_pairs) *valid_pairs = vp;
-    if (total_pairs) *total_pairs = tp;
+    st.device_ms = r->device_ms;
+    st.num_curvelets = r->cv_off[r->num_maps];
+    st.num_maps = (uint32_t)r->num_maps;
+    st.launches = (uint32_t)r->launches;
+    *out = st;
     return CVL_OK;
 }
 

@@ -65,7 +65,7 @@ struct MapStats {
     unsigned max_deg;          // max_num_of_neighbors
     unsigned truncated;        // anchors that reached max_candidates
     unsigned valid_pairs;      // pairs with a valid bundle
-    unsigned pad;
+    unsigned close_pairs;      // pairs that keep the default bundle (no transport)
 };
 
 // Per-block map statistics: accumulated with shared-memory atomics and added to
@@ -76,6 +76,7 @@ struct BlockStats {
     unsigned max_deg[MAPS_SMEM];
     unsigned truncated[MAPS_SMEM];
     unsigned valid[MAPS_SMEM];
+    unsigned close[MAPS_SMEM];
 };
 
 __device__ __forceinline__ void block_stats_init(BlockStats &bs, int M) {
@@ -84,21 +85,24 @@ __device__ __forceinline__ void block_stats_init(BlockStats &bs, int M) {
         bs.max_deg[m] = 0;
         bs.truncated[m] = 0;
         bs.valid[m] = 0;
+        bs.close[m] = 0;
     }
 }
 
 __device__ __forceinline__ void stats_add(BlockStats &bs, MapStats *gs, int M, int m, unsigned pairs, unsigned deg,
-                                          unsigned trunc, unsigned valid) {
+                                          unsigned trunc, unsigned valid, unsigned close = 0u) {
     if (M <= MAPS_SMEM) {
         if (pairs) atomicAdd(&bs.pairs[m], (unsigned long long)pairs);
         if (deg) atomicMax(&bs.max_deg[m], deg);
         if (trunc) atomicAdd(&bs.truncated[m], trunc);
         if (valid) atomicAdd(&bs.valid[m], valid);
+        if (close) atomicAdd(&bs.close[m], close);
     } else {
         if (pairs) atomicAdd(&gs[m].pairs, (unsigned long long)pairs);
         if (deg) atomicMax(&gs[m].max_deg, deg);
         if (trunc) atomicAdd(&gs[m].truncated, trunc);
         if (valid) atomicAdd(&gs[m].valid_pairs, valid);
+        if (close) atomicAdd(&gs[m].close_pairs, close);
     }
 }
 
@@ -109,6 +113,7 @@ __device__ __forceinline__ void block_stats_flush(BlockStats &bs, MapStats *gs, 
         if (bs.max_deg[m]) atomicMax(&gs[m].max_deg, bs.max_deg[m]);
         if (bs.truncated[m]) atomicAdd(&gs[m].truncated, bs.truncated[m]);
         if (bs.valid[m]) atomicAdd(&gs[m].valid_pairs, bs.valid[m]);
+        if (bs.close[m]) atomicAdd(&gs[m].close_pairs, bs.close[m]);
     }
 }
 
@@ -455,17 +460,23 @@ __global__ void __launch_bounds__(256) k_nb(NbArgs a) {
             __syncwarp();
             continue;
         }
-        // the anchor's orientation samples: sin/cos(T2 + delta_t2_j) (:702-705)
+        // the anchor's trig row [2Q + 2]: sin(T2 + delta_t2_j), cos(T2 + delta_t2_j)
+        // for j < Q (:702-705), then cos(T2), sin(T2) (:690 and the dot product)
         const double T2 = a.B.th[i];
+        const double cosT2 = (a.pcls || a.atrig) ? cvl_cos(T2) : 0.0;
+        const double sinT2 = (a.pcls || a.atrig) ? cvl_sin(T2) : 0.0;
         if (a.atrig) {
+            double *row = a.atrig + (size_t)i * (2 * md.Q + 2);
             for (int j = lane; j < md.Q; j += 32) {
                 const double t = T2 + md.st * ((double)j - ((double)md.Q - 1.0) / 2.0);
-                a.atrig[(size_t)i * 2 * md.Q + j] = cvl_sin(t);
-                a.atrig[(size_t)i * 2 * md.Q + md.Q + j] = cvl_cos(t);
+                row[j] = cvl_sin(t);
+                row[md.Q + j] = cvl_cos(t);
+            }
+            if (lane == 0) {
+                row[2 * md.Q] = cosT2;
+                row[2 * md.Q + 1] = sinT2;
             }
         }
-        const double cosT2 = a.pcls ? cvl_cos(T2) : 0.0;
-        const double sinT2 = a.pcls ? cvl_sin(T2) : 0.0;
         // rank sort by (d2, scan key) -- std::sort by distance, preprocess.hpp:172-176
         for (unsigned t = lane; t < n; t += 32) {
             const double dt_ = S.d2[t];

@@ -267,9 +267,14 @@ __global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
         const unsigned long long off = a.pair_off[i];
         const int deg = (int)(a.pair_off[i + 1] - off);
 
-        unsigned valid_cnt = 0;
-        for (int k = lane; k < deg; k += 32) valid_cnt += (a.pflag[off + k] & 1u);
+        unsigned valid_cnt = 0, close_cnt = 0;
+        for (int k = lane; k < deg; k += 32) {
+            const unsigned fl = a.pflag[off + k];
+            valid_cnt += fl & 1u;
+            close_cnt += (fl >> 1) & 1u;
+        }
         valid_cnt = __reduce_add_sync(FULL, valid_cnt);
+        close_cnt = __reduce_add_sync(FULL, close_cnt);
 
         unsigned n_out = 0;
         for (int f = 0; f < 2; ++f) {
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
         }
         if (lane == 0) {
             if (!a.count_only) a.count[orig] = n_out;
-            stats_add(bstats, a.stats, a.M, m, 0u, 0u, 0u, valid_cnt);
+            stats_add(bstats, a.stats, a.M, m, 0u, 0u, 0u, valid_cnt, close_cnt);
         }
         __syncwarp();
     }

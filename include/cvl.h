@@ -169,9 +169,19 @@ typedef struct cvl_batch_result cvl_batch_result;
 int cvl_batch_run(cvl_engine *e, const cvl_batch *b, const cvl_params *p, cvl_batch_result **out);
 /* Downloads (once) and views map m of a batch result. */
 int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view);
-/* Device time (ms) of the batch compute, and the totals over all maps. */
-int cvl_batch_result_stats(const cvl_batch_result *r, double *device_ms, uint64_t *num_curvelets,
-                           uint64_t *valid_pairs, uint64_t *total_pairs);
+/* Totals of a batch run over all its maps. */
+typedef struct cvl_batch_stats {
+    double device_ms;              /* device time of the batch compute (CUDA events) */
+    uint64_t num_curvelets;
+    uint64_t valid_pairs;          /* pairs with a valid bundle */
+    uint64_t total_pairs;          /* neighbour pairs */
+    uint64_t close_pairs;          /* pairs closer than 2 dx: default bundle, no transport (cpu_curvelet.hpp:682) */
+    uint32_t max_num_of_neighbors;
+    uint32_t truncated_anchors;
+    uint32_t num_maps;
+    uint32_t launches;             /* kernels launched by the run */
+} cvl_batch_stats;
+int cvl_batch_result_stats(const cvl_batch_result *r, cvl_batch_stats *out);
 void cvl_batch_result_free(cvl_batch_result *r);
 
 /* Writes a buffer larger than the L2 cache on the engine's stream and waits
