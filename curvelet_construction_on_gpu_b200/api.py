@@ -326,6 +326,34 @@ def default_engine() -> Engine:
     return _default_engine
 
 
+def pair_bundles_noalloc(pairs, params: CurveletParams | None = None, dt_rad: float = 0.0):
+    """Engine.pair_bundles through cvl_pair_bundles_noalloc: no engine, no device
+    allocation, a fixed per-device scratch (at most 15,872 pairs of the default
+    63-cell grid per call). Returns (bmin [n, cells], bmax [n, cells], valid [n]
+    bool, valid_pairs)."""
+    lib = _abi.load()
+    params = params or CurveletParams()
+    q = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1, 6)
+    n = q.shape[0]
+    p = params.to_c(dt_rad)
+    cells = C.c_int32(0)
+    count = C.c_uint32(0)
+    u8p = C.POINTER(C.c_uint8)
+    one = np.zeros(1)
+    # n = 0 sizes the grid without touching the device
+    check(lib.cvl_pair_bundles_noalloc(q.ctypes.data_as(_abi._dp), 0, C.byref(p), one.ctypes.data_as(_abi._dp),
+                                       one.ctypes.data_as(_abi._dp), np.zeros(1, np.uint8).ctypes.data_as(u8p),
+                                       C.byref(count), C.byref(cells)), "cvl_pair_bundles_noalloc")
+    nc = cells.value
+    bmin = np.zeros((max(n, 1), nc))
+    bmax = np.zeros((max(n, 1), nc))
+    valid = np.zeros(max(n, 1), np.uint8)
+    check(lib.cvl_pair_bundles_noalloc(q.ctypes.data_as(_abi._dp), n, C.byref(p), bmin.ctypes.data_as(_abi._dp),
+                                       bmax.ctypes.data_as(_abi._dp), valid.ctypes.data_as(u8p), C.byref(count),
+                                       C.byref(cells)), "cvl_pair_bundles_noalloc")
+    return bmin[:n], bmax[:n], valid[:n].astype(bool), int(count.value)
+
+
 @dataclass
 class GPUNeighborGraph:
     """CPUNeighborGraph<T> (preprocess.hpp:18-31): CSR over anchors in input order,

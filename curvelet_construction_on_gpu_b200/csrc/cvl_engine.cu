@@ -299,7 +299,7 @@ int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nb
     md.w = (int)nbr_radius;
     {
         // hash block edge: a power of two (the block of a pixel cell is cell >> sbits)
-        const int S = e->cell_size > 0 ? e->cell_size : 4;
+        const int S = (e && e->cell_size > 0) ? e->cell_size : 4;
         int sb = 0;
         while ((1 << sb) < S && sb < 6) ++sb;
         if ((1 << sb) != S) return fail(CVL_EINVAL, "cell_size must be a power of two in [1, 64]");
@@ -1156,6 +1156,151 @@ int cvl_measure_fp64_peak(cvl_engine *e, double *tflops) {
     if (ce != cudaSuccess) return fail(CVL_ECUDA, std::string("fp64 probe: ") + cudaGetErrorString(ce));
     const double fmas = (double)blocks * threads * iters * 16.0 * 8.0;
     *tflops = 2.0 * fmas / (ms * 1e-3) / 1e12;
+    return CVL_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================
+// Pair bundles without any allocation (cvl_pair_bundles_noalloc)
+// =============================================================================
+namespace {
+
+// Per-device scratch of cvl_pair_bundles_noalloc, laid out per call as
+//   [0, 256)  valid-pair counter (u32; cleared by every call)
+//   pairs [n][6] f64 | bmin [n][cells] f64 | bmax [n][cells] f64 | valid [n] u8,
+// each piece starting on a 256-byte boundary.
+__device__ __align__(256) unsigned char g_noalloc_scratch[CVL_NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+
+inline size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t noalloc_bytes(size_t n, size_t cells) {
+    return 256 + round256(48 * n) + 2 * round256(8 * n * cells) + round256(n);
+}
+
+// k_pair_bundles with the valid pairs counted: warp per pair, one atomic per
+// valid pair into the scratch counter.
+__global__ void __launch_bounds__(128) k_pair_bundles_counted(Model md, const double *__restrict__ pairs, int n,
+                                                              double *__restrict__ bmin_out,
+                                                              double *__restrict__ bmax_out,
+                                                              unsigned char *__restrict__ valid_out,
+                                                              unsigned *__restrict__ valid_count) {
+    __shared__ double tab[4][4 * QMAX];
+    __shared__ double cell_dx2[CELLS_MAX];
+    __shared__ unsigned char cell_j[CELLS_MAX];
+    __shared__ unsigned short cell_rank[CELLS_MAX];
+    cell_tables_init(md, cell_dx2, cell_j, cell_rank);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *sT = tab[wib], *cT = sT + QMAX, *sM = cT + QMAX, *sP = sM + QMAX;
+    for (int p = blockIdx.x * 4 + wib; p < n; p += gridDim.x * 4) {
+        const double *q = pairs + (size_t)p * 6;
+        const double te_x = q[0], te_y = q[1], T2 = q[2], le_x = q[3], le_y = q[4], T0 = q[5];
+        for (int j = lane; j < md.Q; j += 32) {
+            const double t = T2 + md.st * ((double)j - ((double)md.Q - 1.0) / 2.0);
+            sT[j] = sin(t);
+            cT[j] = cos(t);
+            sM[j] = sin(t - (T0 - md.dt));
+            sP[j] = sin(t - (T0 + md.dt));
+        }
+        __syncwarp();
+        const double t_p = T0 + md.dt, t_m = T0 - md.dt;
+        const PairGeom g = pair_geom(md, te_x, te_y, cos(T2), sin(T2), le_x, le_y, sin(t_p), cos(t_p), sin(t_m),
+                                     cos(t_m));
+        bool lv = false;
+        for (int c = lane; c < md.cells; c += 32) {
+            double bmin = -md.max_k, bmax = md.max_k;
+            if (!g.close) {
+                const int jj = cell_j[c];
+                const double tt = sT[jj] * g.DX - cT[jj] * g.DY;
+                bundle_cell_tt(md, g.DX2, g.DY2, g.sin_p_DY, g.cos_p_DX, g.sin_m_DY, g.cos_m_DX, g.branch1,
+                               cell_dx2[c], tt, sM[jj], sP[jj], bmin, bmax);
+            }
+            lv = lv || (bmax > bmin);
+            bmin_out[(size_t)p * md.cells + c] = bmin;
+            bmax_out[(size_t)p * md.cells + c] = bmax;
+        }
+        const bool valid = g.close ? true : (bool)__any_sync(FULL, lv);
+        if (lane == 0) {
+            valid_out[p] = valid ? 1 : 0;
+            if (valid) atomicAdd(valid_count, 1u);
+        }
+        __syncwarp();
+    }
+}
+
+// Set-up, once per device, with that device current: the scratch's address.
+int noalloc_scratch(int dev, unsigned char **out) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(CVL_EUNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+        void *ptr = nullptr;
+        const cudaError_t ce = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (ce != cudaSuccess || !ptr)
+            return fail(CVL_ECUDA, std::string("scratch address: ") + cudaGetErrorString(ce));
+        g_noalloc_base[dev] = (unsigned char *)ptr;
+    }
+    *out = g_noalloc_base[dev];
+    return CVL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cvl_pair_bundles_noalloc(const double *pairs, int32_t n, const cvl_params *p, double *bmin, double *bmax,
+                             uint8_t *valid, uint32_t *valid_pairs, int32_t *cells) {
+    if (!pairs || !bmin || !bmax || !valid || !valid_pairs || !cells || n < 0)
+        return fail(CVL_EINVAL, "invalid argument");
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(nullptr, p, p ? p->nrad : 0.0, 3u, p ? std::max(p->max_candidates, 1u) : 1u, md, cpl));
+    *cells = md.cells;
+    *valid_pairs = 0;
+    const size_t need = noalloc_bytes((size_t)n, (size_t)md.cells);
+    if (need > CVL_NOALLOC_SCRATCH_BYTES) {
+        size_t max_n = 0;
+        while (noalloc_bytes(max_n + 1, (size_t)md.cells) <= CVL_NOALLOC_SCRATCH_BYTES) ++max_n;
+        return fail(CVL_EOVERFLOW, std::to_string(n) + " pairs need " + std::to_string(need) +
+                                       " bytes of scratch; the fixed scratch holds " +
+                                       std::to_string((size_t)CVL_NOALLOC_SCRATCH_BYTES) + " bytes, at most " +
+                                       std::to_string(max_n) + " pairs of " + std::to_string(md.cells) + " cells");
+    }
+    if (n == 0) return CVL_OK;
+    int dev = 0, ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(CVL_ENODEV, "no CUDA device");
+    }
+    CVL_CUDA(cudaGetDevice(&dev));
+    unsigned char *base = nullptr;
+    CVL_TRY(noalloc_scratch(dev, &base));
+    int sms = 0;
+    CVL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+
+    const size_t cells_n = (size_t)n * md.cells;
+    unsigned *d_count = (unsigned *)base;
+    double *d_pairs = (double *)(base + 256);
+    double *d_bmin = (double *)((unsigned char *)d_pairs + round256(48 * (size_t)n));
+    double *d_bmax = (double *)((unsigned char *)d_bmin + round256(8 * cells_n));
+    unsigned char *d_valid = (unsigned char *)d_bmax + round256(8 * cells_n);
+
+    cudaStream_t s = cudaStreamPerThread;
+    CVL_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned), s));
+    CVL_CUDA(cudaMemcpyAsync(d_pairs, pairs, 48 * (size_t)n, cudaMemcpyHostToDevice, s));
+    long long blocks = ((long long)n + 3) / 4;
+    blocks = std::max(1LL, std::min(blocks, (long long)sms * 16));
+    k_pair_bundles_counted<<<(int)blocks, 128, 0, s>>>(md, d_pairs, n, d_bmin, d_bmax, d_valid, d_count);
+    CVL_TRY(check_launch("k_pair_bundles_counted"));
+    CVL_CUDA(cudaMemcpyAsync(bmin, d_bmin, 8 * cells_n, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(bmax, d_bmax, 8 * cells_n, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(valid, d_valid, (size_t)n, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(valid_pairs, d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaStreamSynchronize(s));
     return CVL_OK;
 }
 

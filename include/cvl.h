@@ -152,6 +152,37 @@ int cvl_build_curvelets(cvl_engine *e, const cvl_graph *g, const cvl_params *p, 
 int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p,
                      double *bmin, double *bmax, uint8_t *valid, int32_t *cells);
 
+/* ---- pair bundles without any allocation ------------------------------ */
+/* No reference counterpart. The same computation and outputs as
+ * cvl_pair_bundles, plus the number of valid pairs (the count
+ * form_pairwise_bundles keeps, cpu_curvelet.hpp:305-361). It needs no engine
+ * and allocates no device memory: no cudaMalloc/cudaFree and no library
+ * allocator (on success it makes no host allocation either; a failure stores
+ * its message in a thread-local string). Device work goes through one fixed scratch area per
+ * device, a static device array of CVL_NOALLOC_SCRATCH_BYTES, on the calling
+ * thread's default stream (cudaStreamPerThread), on the current device.
+ *
+ * It is for callers that must not allocate device memory during the call:
+ * cudaFree synchronises the whole device, and cudaMalloc can fail or stall
+ * once a framework allocator has reserved the memory. Examples are a process
+ * whose memory is already fully reserved, and a latency-bound loop.
+ *
+ * Limit: the scratch holds the call's pairs, bundles and flags at once:
+ *   256 + a(48 n) + 2 a(8 n cells) + a(n) <= CVL_NOALLOC_SCRATCH_BYTES,
+ * where a(x) rounds x up to 256. That is 15,872 pairs for the default
+ * 7 x 9 = 63-cell grid. Larger n returns CVL_EOVERFLOW and does no work; split
+ * the pairs over several calls.
+ *
+ * The first call on a device does the set-up (it looks up the scratch's
+ * address with the device current). Make that call before any stream capture
+ * on the device. Calls that overlap in time on one device, from several host
+ * threads, share the scratch and race: serialise them. Each call clears its
+ * valid-pair counter before use and returns after its results are in the
+ * caller's host buffers. */
+#define CVL_NOALLOC_SCRATCH_BYTES (16u << 20)
+int cvl_pair_bundles_noalloc(const double *pairs, int32_t n, const cvl_params *p, double *bmin, double *bmax,
+                             uint8_t *valid, uint32_t *valid_pairs, int32_t *cells);
+
 /* ---- device-resident maps (benchmarks, batching) ---------------------- */
 /* A ragged batch of edge maps kept in device memory: maps[m] has counts[m]
  * rows of edge_data_sz doubles, concatenated in edges. */
