@@ -382,7 +382,16 @@ struct RunOut {
 
 template <int CPL>
 int launch_bundles(cvl_engine *e, BundleArgs &a, int blocks) {
-    k_bundles<CPL><<<blocks, 256, 0, e->stream>>>(a);
+    // one resident wave: the kernel strides over the chunk's pairs
+    static thread_local int per_sm = 0;
+    if (per_sm <= 0) {
+        CVL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bundles<CPL>, BUNDLE_THREADS, 0));
+        if (per_sm <= 0) per_sm = 1;
+    }
+    const long long ppb = BUNDLE_THREADS / a.md.Q;
+    const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
+    blocks = (int)std::max(1LL, std::min<long long>(need, (long long)e->prop.multiProcessorCount * per_sm));
+    k_bundles<CPL><<<blocks, BUNDLE_THREADS, 0, e->stream>>>(a);
     return check_launch("k_bundles");
 }
 

@@ -115,12 +115,22 @@ __device__ __forceinline__ void cell_tables_init(const Model &md, double *dx2, u
 }
 
 // ---------------------------------------------------------------------------
-// (c) k_bundles: the transport of every pair of a chunk. Lane (pair, j) of a
-// warp computes the pair's geometry, its two sin(T2t_j - T0 -+ dt) (:728-729)
-// and tt_j (:705) once, then the P cells (i, j) of its column into the pair's
-// bundle (mins then maxes, cell c at index c); one ballot gives validity
-// (bundle_valid_check, :821-830). Close pairs keep the default bundle
-// (:682-687) and are flagged, not written.
+// (c) k_bundles: the transport of every pair of a chunk. The block's threads are
+// (pair, j) lanes over PPB = blockDim / Q pairs at a time (252 of 256 threads busy
+// for Q = 9). A lane computes the pair's geometry, its two sin(T2t_j - T0 -+ dt)
+// (:728-729) and tt_j (:705) once, then the P cells (i, j) of its column into the
+// pair's bundle (mins then maxes, cell c at index c). Validity (bundle_valid_check,
+// :821-830) is the OR of the pair's lanes through shared memory. Close pairs keep
+// the default bundle (:682-687) and are flagged, not written.
+//
+// The per-cell arithmetic is rewritten into fewer operations that give the same
+// correctly rounded values as :693-809 (round-to-nearest is odd-symmetric, and
+// scaling by 2 is exact without overflow or underflow):
+//   e1  = (((DX2 - (2 dx2) tt) + DY2) - dx^2) + dx2^2          (branch 1's eq, :706)
+//   branch 2's eq (:770) is -(-e1)/2 = e1 * 0.5 exactly, so its
+//   (ttmdx2 -+ dx) / eq == (2 (ttmdx2 -+ dx)) / e1, branch 1's k_dx (:707-708);
+//   2 (ttmdx2 -+ dx) = (2 tt - 2 dx2) -+ 2 dx exactly.
+// Only the k_dt clamp order differs between the branches.
 // ---------------------------------------------------------------------------
 struct BundleArgs {
     Model md;
@@ -134,29 +144,38 @@ struct BundleArgs {
     unsigned char *pflag;               // [P]: bit 0 valid, bit 1 close
 };
 
+constexpr int BUNDLE_THREADS = 256;
+
 template <int CPL>
-__global__ void __launch_bounds__(256) k_bundles(BundleArgs a) {
+__global__ void __launch_bounds__(BUNDLE_THREADS, 4) k_bundles(BundleArgs a) {
     const Model &md = a.md;
-    const int lane = threadIdx.x & 31;
-    const int jl = lane % md.Q;
-    const int ppl = lane / md.Q;
-    const int PPP = 32 / md.Q;
-    const unsigned qmask = (md.Q >= 32) ? FULL : ((1u << md.Q) - 1u);
+    __shared__ double s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
+    __shared__ unsigned char s_open[2][BUNDLE_THREADS];
+    for (int i = threadIdx.x; i < md.P; i += blockDim.x) {
+        const double d = md.sx * ((double)i - ((double)md.P - 1.0) / 2.0);  // delta_x2 (:697)
+        s_dx2[i] = d;
+        s_dx2_2[i] = 2.0 * d;
+        s_dx2sq[i] = d * d;
+    }
+    for (int t = threadIdx.x; t < 2 * BUNDLE_THREADS; t += blockDim.x) (&s_open[0][0])[t] = 0;
+    __syncthreads();
     constexpr int BW = 2 * 32 * CPL;
-    const double half = ((double)md.P - 1.0) / 2.0;
+    const int t = threadIdx.x;
+    const int PPB = BUNDLE_THREADS / md.Q;
+    const int pl = t / md.Q, jl = t - pl * md.Q;
+    const bool lane_on = pl < PPB;
     const double delta_t2 = md.st * ((double)jl - ((double)md.Q - 1.0) / 2.0);  // :698
+    const double dx_2 = 2.0 * md.dx;
     const int A2 = 2 * md.Q + 2;
     const unsigned long long np = a.p_end - a.p_begin;
-    const unsigned long long gw = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
-    for (unsigned long long g = gw * PPP; g < np; g += nw * PPP) {
-        const unsigned long long q = g + ppl;
-        const bool act = ppl < PPP && q < np;
-        bool open = false, closep = false;
-        if (act) {
+    int it = 0;
+    for (unsigned long long g = (unsigned long long)blockIdx.x * PPB; g < np;
+         g += (unsigned long long)gridDim.x * PPB, ++it) {
+        const int buf = it & 1;
+        const unsigned long long q = g + pl;
+        if (lane_on && q < np) {
             const unsigned long long p = a.p_begin + q;
-            closep = (a.pcls[p] & 4u) != 0;
-            if (!closep) {
+            if (!(a.pcls[p] & 4u)) {
                 const int ia = a.pair_anchor[p];
                 const int nn = a.csr_ids[p];
                 const double *at = a.atrig + (size_t)ia * A2;
@@ -169,24 +188,43 @@ __global__ void __launch_bounds__(256) k_bundles(BundleArgs a) {
                 const double s_m = cvl_sin(T2t - (T0 - md.dt));   // :728
                 const double s_p = cvl_sin(T2t - (T0 + md.dt));   // :729
                 const double tt = sTj * g2.DX - cTj * g2.DY;     // :705
+                const double tt2 = 2.0 * tt;
                 double *dst = a.bund + q * BW;
-                double di = 0.0;
-#pragma unroll 3
-                for (int i = 0; i < md.P; ++i, di += 1.0) {
-                    const double delta_x2 = md.sx * (di - half);  // :697
+                bool open = false;
+#pragma unroll 2
+                for (int i = 0; i < md.P; ++i) {
+                    const double delta_x2 = s_dx2[i], dx2_2 = s_dx2_2[i];
+                    const double ttmdx2_2 = tt2 - dx2_2;                         // 2 ttmdx2
+                    const double lo2 = ttmdx2_2 - dx_2, hi2 = ttmdx2_2 + dx_2;  // 2 (ttmdx2 -+ dx)
+                    const double e1 = (((g2.DX2 - dx2_2 * tt) + g2.DY2) - md.dx2) + s_dx2sq[i];
+                    const double k_dx_min = lo2 / e1;
+                    const double k_dx_max = hi2 / e1;
+                    const double km = s_m / (-s_m * delta_x2 + g2.cos_m_DX + g2.sin_m_DY);
+                    const double kp = s_p / (-s_p * delta_x2 + g2.cos_p_DX + g2.sin_p_DY);
                     double bmin = -md.max_k, bmax = md.max_k;
-                    bundle_cell_tt(md, g2.DX2, g2.DY2, g2.sin_p_DY, g2.cos_p_DX, g2.sin_m_DY, g2.cos_m_DX,
-                                   g2.branch1, delta_x2, tt, s_m, s_p, bmin, bmax);
+                    if (bmin < k_dx_min) bmin = k_dx_min;
+                    if (bmax > k_dx_max) bmax = k_dx_max;
+                    const double k2min = g2.branch1 ? km : kp;
+                    const double k2max = g2.branch1 ? kp : km;
+                    if (bmin < k2min) bmin = k2min;
+                    if (bmax > k2max) bmax = k2max;
                     open = open || (bmax > bmin);
                     dst[i * md.Q + jl] = bmin;
                     dst[32 * CPL + i * md.Q + jl] = bmax;
                 }
+                if (open) s_open[buf][pl] = 1;
             }
         }
-        const unsigned ob = __ballot_sync(FULL, open);
-        if (act && jl == 0) {
-            const bool valid = closep || (ob & (qmask << (ppl * md.Q))) != 0;
-            a.pflag[a.p_begin + q] = (unsigned char)((valid ? 1u : 0u) | (closep ? 2u : 0u));
+        __syncthreads();
+        if (t < PPB) {
+            const unsigned long long qq = g + t;
+            if (qq < np) {
+                const unsigned long long p = a.p_begin + qq;
+                const bool closep = (a.pcls[p] & 4u) != 0;
+                const bool valid = closep || s_open[buf][t] != 0;
+                a.pflag[p] = (unsigned char)((valid ? 1u : 0u) | (closep ? 2u : 0u));
+            }
+            s_open[buf][t] = 0;
         }
     }
 }
@@ -339,9 +377,17 @@ __global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
                             for (int u = 0; u < CPL; ++u) cmin[q][u] = cmax[q][u] = 0.0;
                         }
                     }
+                    // the walk's bundles, one ahead: r + 1 loads while r is intersected
+                    double nmin[CPL], nmax[CPL];
+                    load_bundle(0, nmin, nmax);
                     for (int r = 0; r < ns && done != (1u << K) - 1u; ++r) {
                         double rmin[CPL], rmax[CPL];
-                        load_bundle(r, rmin, rmax);
+#pragma unroll
+                        for (int u = 0; u < CPL; ++u) {
+                            rmin[u] = nmin[u];
+                            rmax[u] = nmax[u];
+                        }
+                        if (r + 1 < ns) load_bundle(r + 1, nmin, nmax);
                         unsigned bits = 0;
 #pragma unroll
                         for (int q = 0; q < K; ++q) {
