@@ -6,9 +6,15 @@ A step is one pass of the whole path (spatial hash -> neighbour CSR -> pairwise
 curve bundles -> chain growth, dedup, record -> compacted chains + info) over
 one batch of seeded synthetic edges. Workloads:
 
-  plain_hd    one 1920x1080 map, ~242k edges, one map per launch (default)
+  mixed64     64 maps of uneven size (640x480 .. 3840x2160, 8k .. 3.8M edges,
+              33.7M in all) in one ragged batch (default). The same line reports
+              the plain form (the 64 maps one per launch, same GPU), and a served
+              run: an open-loop Poisson stream of maps drawn from the same 64
+              through cvl_server_* (continuous batching, 40 GB admission budget),
+              with p50/p95/p99 latency.
+  plain_hd    one 1920x1080 map, ~242k edges, one map per launch
   plain_small one 480x320 map (~4.5k edges)
-  mixed64     64 maps of uneven size (640x480 .. 3840x2160) in one ragged batch
+  served      only the served stream, at each rate of --rates
 
 value: edges/s with the edges already in HBM (CUDA events on the engine's
 stream around each step, L2 flushed between steps). e2e: the same metric
@@ -46,9 +52,14 @@ def _args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="plain_hd", choices=["plain_hd", "plain_small", "mixed64"])
+    ap.add_argument("--workload", default="mixed64", choices=["mixed64", "plain_hd", "plain_small", "served"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--rate", type=float, default=100.0, help="served stream: offered maps/s")
+    ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")
+    ap.add_argument("--requests", type=int, default=600, help="served stream: requests per rate")
+    ap.add_argument("--workers", type=int, default=2, help="served stream: server workers")
     return ap.parse_args()
 
 
@@ -58,8 +69,10 @@ def _workload(name: str, rank: int):
         return [synth.plain_hd(1000 + rank)], {"image": "1920x1080", "curves": 1500, "clutter": 0.2}
     if name == "plain_small":
         return [synth.plain_small(0 + rank)], {"image": "480x320", "curves": 50, "clutter": 0.1}
+    # mixed64 and served share the pool of 64 seeded maps
     maps = synth.mixed64(2000 + 64 * rank, 64)
-    return maps, {"maps": 64, "images": "640x480..3840x2160", "clutter": 0.2}
+    images = [synth.mixed_map_image(2000 + 64 * rank + i) for i in range(64)]
+    return maps, {"maps": 64, "images": "640x480..3840x2160", "clutter": 0.2, "_images": images}
 
 
 class _Clocks:
@@ -111,17 +124,42 @@ class _Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+_PINNED_KEEP = []  # the torch tensors behind the page-locked arrays handed out
+
+
 def _pinned(a: np.ndarray) -> np.ndarray:
     """A page-locked copy of a (torch's pinned allocator), for the e2e copies."""
-    try:
-        import torch
-        t = torch.empty(a.size, dtype=torch.float64).pin_memory()
-        out = t.numpy().reshape(a.shape)
-        out[...] = a
-        out._keep = t  # type: ignore[attr-defined]
-        return out
-    except Exception:
-        return np.ascontiguousarray(a)
+    import torch
+    t = torch.empty(a.size, dtype=torch.float64).pin_memory()
+    _PINNED_KEEP.append(t)
+    out = t.numpy().reshape(a.shape)
+    out[...] = a
+    return out
+
+
+def _progress(msg: str) -> None:
+    print(f"[bench] {time.strftime('%H:%M:%S')} {msg}", file=sys.stderr, flush=True)
+
+
+# The reference sizes its outputs as num_edges * (max_degree + 1) * 2 * 10 in
+# 32-bit unsigned arithmetic (cpu_curvelet.hpp:64-67). That product wraps, and
+# the info array is under-allocated, once a map is large enough: above 2^32 /
+# (2 * 10 * (max_candidates + 1)) = 1,664,804 edges it can wrap at any degree.
+# The CPU timings therefore run on whole maps below that size.
+REF_SAFE_EDGES = (1 << 32) // (2 * 10 * (128 + 1))
+
+
+def _ref_sample(maps, max_edges: int):
+    """Whole maps the reference can hold, in workload order, until max_edges."""
+    out, tot = [], 0
+    for m in maps:
+        if m.shape[0] >= REF_SAFE_EDGES:
+            continue
+        out.append(m)
+        tot += m.shape[0]
+        if tot >= max_edges:
+            break
+    return out, tot
 
 
 def _dist_init(args):
@@ -173,7 +211,10 @@ def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
     edges = 0
     secs = 0.0
     used = 0
-    for m in maps:
+    cand, _ = _ref_sample(maps, 1 << 62)
+    for m in cand:
+        if m.shape[0] > 600_000:  # keep the sample within the time budget
+            continue
         t0 = time.perf_counter()
         if kind == "reference":
             r = O.ref_run(m, nthreads=threads, want_outputs=False)
@@ -187,8 +228,9 @@ def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
         if secs > budget_s:
             break
     return {"value": edges / secs, "unit": METRIC, "cores": threads, "kind": kind,
-            "sample": f"{used} of {len(maps)} map(s), {edges} edges, timed as the reference's own "
-                      f"CSR + form_pairwise_bundles + build_curvelets_greedy phases (file I/O excluded)"}
+            "sample": f"{used} of {len(maps)} map(s) (whole maps of at most 600k edges, in workload order), "
+                      f"{edges} edges, timed as the reference's own CSR + form_pairwise_bundles + "
+                      f"build_curvelets_greedy phases (file I/O excluded)"}
 
 
 def run_reference(args, maps, cfg, world, rank):
@@ -200,13 +242,9 @@ def run_reference(args, maps, cfg, world, rank):
                           "(the reference sources were absent at build time)"}))
         return
     threads = os.cpu_count() or 1
-    # each step: the whole workload when it is small enough, else a bounded sample of whole maps
-    sample, tot = [], 0
-    for m in maps:
-        sample.append(m)
-        tot += m.shape[0]
-        if tot >= 300_000:
-            break
+    # each step: the whole workload when it is small enough, else a bounded sample
+    # of whole maps that the reference can hold (REF_SAFE_EDGES)
+    sample, tot = _ref_sample(maps, 300_000)
     for _ in range(args.warmup):
         O.ref_run(sample[0], nthreads=threads, want_outputs=False)
     step_s = []
@@ -221,7 +259,8 @@ def run_reference(args, maps, cfg, world, rank):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": dict(workload=args.workload, edges=tot, maps=len(sample), **cfg),
+            "config": dict(workload=args.workload, edges=tot, maps=len(sample),
+                           **{k: v for k, v in cfg.items() if not k.startswith("_")}),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
                              "sample": f"{len(sample)} of {len(maps)} map(s), {tot} edges per step"},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -253,10 +292,69 @@ def _plain_device_ms(eng, maps, steps: int) -> float:
     return total / steps
 
 
+def _served(maps, images, rate: float, n_req: int, workers: int, device: int, seed: int = 7) -> dict:
+    """Open-loop Poisson stream through cvl_server_*: n_req maps drawn (with
+    replacement) from `maps`, arrivals at `rate` maps/s, submitted on schedule
+    by one thread while another collects the results. Latency is the server's
+    own clock from the submit call to the result being ready in host memory."""
+    import threading
+
+    import curvelet_construction_on_gpu_b200 as cvl
+    rng = np.random.default_rng(seed)
+    picks = rng.integers(0, len(maps), n_req)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    srv = cvl.Server(device=device, workers=workers)
+    try:
+        # warm-up (workspace growth): the largest and a small map through every worker
+        order = np.argsort([m.shape[0] for m in maps])
+        warm = [srv.submit(maps[int(order[-1])]) for _ in range(workers)]
+        warm += [srv.submit(maps[int(order[0])]) for _ in range(workers)]
+        for w in warm:
+            srv.wait(w)
+        n_warm = len(warm)
+        ids = [None] * n_req
+        t0 = time.perf_counter()
+
+        def submitter():
+            for k in range(n_req):
+                dt = t0 + arrivals[k] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids[k] = srv.submit(maps[int(picks[k])])
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        for k in range(n_req):
+            while ids[k] is None:
+                time.sleep(0.0002)
+            srv.wait(ids[k])
+        th.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        ms, ed = srv.latencies()
+    finally:
+        srv.close()
+    ms, ed = ms[n_warm:], ed[n_warm:]
+    hd_edges = {int(maps[i].shape[0]) for i in range(len(maps)) if images[i] == (1920, 1080)}
+    hd = np.array([m for m, e in zip(ms, ed) if int(e) in hd_edges])
+
+    def pct(a, q):
+        return float(np.percentile(a, q, method="inverted_cdf")) if len(a) else None
+
+    edges = float(np.sum(ed))
+    return {"rate_maps_per_s": rate, "requests": n_req, "workers": workers, "wall_s": wall,
+            "edges_per_s": edges / wall, "maps_per_s": len(ms) / wall,
+            "p50_ms": pct(ms, 50), "p95_ms": pct(ms, 95), "p99_ms": pct(ms, 99), "max_ms": float(np.max(ms)),
+            "hd_1920x1080": {"requests": int(len(hd)), "p50_ms": pct(hd, 50), "p99_ms": pct(hd, 99)},
+            "launches": int(st["launches"]) - n_warm, "failed": int(st["failed"]),
+            "admission": "40 GiB budget, 2048 B per edge", "pool": f"{len(maps)} seeded maps"}
+
+
 def run_ours(args, maps, cfg, world, rank, local, pg):
     import curvelet_construction_on_gpu_b200 as cvl
     eng = cvl.Engine(device=local)
     n_edges = int(sum(m.shape[0] for m in maps))
+    _progress(f"{len(maps)} map(s), {n_edges} edges: upload")
     batch = eng.upload_batch(maps)
     fp64_peak = eng.fp64_peak_tflops() if rank == 0 else None
 
@@ -264,6 +362,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
         r = eng.run_batch(batch)
         r.close()
     _barrier(pg)
+    _progress("timed steps")
     step_ms, kern, launches = [], [], 0
     with _Clocks(local) as clk:
         for _ in range(args.steps):
@@ -286,6 +385,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
 
     plain = None
     if len(maps) > 1:
+        _progress("plain form (one map per launch)")
         pms = _plain_device_ms(eng, maps, max(1, min(args.steps, 3)))
         pms = _max_over_ranks(pg, pms)
         plain = {"value": _sum_over_ranks(pg, float(n_edges)) / (pms / 1e3), "unit": METRIC, "ms_per_step": pms,
@@ -295,22 +395,34 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     # single map, the batch calls (upload, run, download every map) for a batch
     e2e = None
     if not args.no_e2e:
-        pinned = [_pinned(m) for m in maps]
+        _progress("e2e through the C ABI")
         if len(maps) == 1:
-            eng.run(pinned[0])
+            pinned = _pinned(maps[0])
+            eng.run(pinned)
+        else:
+            pinned = _pinned(np.concatenate(maps, axis=0))
+            counts = np.array([m.shape[0] for m in maps], np.int32)
+            # untimed pass: the result pool's page-locked blocks are allocated once
+            b = eng.upload_ragged(pinned, counts)
+            br = eng.run_batch(b)
+            held = [br.take_map(mi) for mi in range(len(maps))]
+            del held
+            br.close()
+            b.close()
         _barrier(pg)
         t0 = time.perf_counter()
         bo = 0
         for _ in range(args.steps):
             if len(maps) == 1:
-                res = eng.run(pinned[0])
+                res = eng.run(pinned)
                 bo += res.chains.nbytes + res.info.nbytes
             else:
-                b = eng.upload_batch(pinned)
+                b = eng.upload_ragged(pinned, counts)
                 br = eng.run_batch(b)
                 for mi in range(len(maps)):
-                    res = br.map(mi)
+                    res = br.take_map(mi)
                     bo += res.chains.nbytes + res.info.nbytes
+                    del res
                 br.close()
                 b.close()
         wall = time.perf_counter() - t0
@@ -318,7 +430,15 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
         e2e = {"value": _sum_over_ranks(pg, float(n_edges)) * args.steps / wall, "unit": METRIC,
                "h2d_bytes_per_step": int(sum(m.nbytes for m in maps)), "d2h_bytes_per_step": int(bo // args.steps),
                "path": ("cvl_run (C ABI), pinned host edges" if len(maps) == 1 else
-                        "cvl_batch_upload + cvl_batch_run + cvl_batch_result_map (C ABI), pinned host edges")}
+                        "cvl_batch_upload + cvl_batch_run + cvl_batch_result_take_map per map (C ABI), "
+                        "pinned host edges")}
+
+    served = None
+    if len(maps) > 1 and not args.no_served and cfg.get("_images"):
+        _progress(f"served stream at {args.rate} maps/s")
+        batch.close()
+        eng.close()
+        served = _served(maps, cfg["_images"], args.rate, args.requests, args.workers, local)
 
     if rank != 0:
         return
@@ -348,10 +468,30 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     if plain is not None:
         line["plain"] = plain
         line["batched_vs_plain"] = value / plain["value"]
+    if served is not None:
+        line["served"] = served
     if world == 1 and not args.no_cpu_baseline:
+        _progress("cpu baseline")
         line["cpu_baseline"] = _cpu_baseline(maps)
+    line["config"].pop("_images", None)
     print(json.dumps(line))
     eng.close()
+
+
+def run_served(args, maps, cfg, world, rank, local, pg):
+    """The served stream alone, swept over --rates (one JSON line)."""
+    rates = [float(r) for r in args.rates.split(",") if r]
+    sweep = [_served(maps, cfg["_images"], r, args.requests, args.workers, local) for r in rates]
+    if rank != 0:
+        return
+    best = max(sweep, key=lambda d: d["edges_per_s"])
+    cfg = {k: v for k, v in cfg.items() if not k.startswith("_")}
+    print(json.dumps({
+        "metric": METRIC, "value": best["edges_per_s"], "unit": METRIC, "n_gpus": world, "steps": len(rates),
+        "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded generators, curvelet_construction_on_gpu_b200/synth.py)",
+        "config": dict(workload="served", requests_per_rate=args.requests, rates=rates, **cfg),
+        "served": sweep}))
 
 
 def main():
@@ -361,6 +501,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, maps, cfg, world, rank)
+        elif args.workload == "served":
+            run_served(args, maps, cfg, world, rank, local, pg)
         else:
             run_ours(args, maps, cfg, world, rank, local, pg)
     finally:

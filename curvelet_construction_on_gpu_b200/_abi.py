@@ -56,6 +56,19 @@ class CvlBatchStats(C.Structure):
                 ("truncated_anchors", C.c_uint32), ("num_maps", C.c_uint32), ("launches", C.c_uint32)]
 
 
+class CvlServerCfg(C.Structure):
+    _fields_ = [("device", C.c_int), ("workers", C.c_int), ("mem_budget_bytes", C.c_size_t),
+                ("admit_bytes_per_edge", C.c_size_t), ("max_batch_edges", C.c_int64),
+                ("large_map_edges", C.c_int64)]
+
+
+class CvlServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("queued", C.c_uint64), ("in_flight", C.c_uint64), ("launches", C.c_uint64),
+                ("edges_completed", C.c_uint64), ("admitted_bytes", C.c_size_t), ("p50_ms", C.c_double),
+                ("p95_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double)]
+
+
 # (name, restype, argtypes) of every entry point declared in include/cvl.h
 _vp = C.c_void_p
 _dp = C.POINTER(C.c_double)
@@ -80,11 +93,21 @@ SIGNATURES = [
     ("cvl_pair_bundles_noalloc", C.c_int, [_dp, C.c_int32, C.POINTER(CvlParams), _dp, _dp, C.POINTER(C.c_uint8),
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
     ("cvl_batch_upload", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    ("cvl_batch_refill", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32]),
     ("cvl_batch_free", None, [_vp]),
     ("cvl_batch_run", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.POINTER(_vp)]),
     ("cvl_batch_result_map", C.c_int, [_vp, C.c_int32, C.POINTER(CvlResultView)]),
+    ("cvl_batch_result_take_map", C.c_int, [_vp, C.c_int32, C.POINTER(_vp)]),
     ("cvl_batch_result_stats", C.c_int, [_vp, C.POINTER(CvlBatchStats)]),
     ("cvl_batch_result_free", None, [_vp]),
+    ("cvl_server_cfg_default", None, [C.POINTER(CvlServerCfg)]),
+    ("cvl_server_create", C.c_int, [C.POINTER(CvlServerCfg), C.POINTER(CvlParams), C.POINTER(_vp)]),
+    ("cvl_server_submit", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.POINTER(C.c_uint64)]),
+    ("cvl_server_poll", C.c_int, [_vp, C.c_uint64, C.POINTER(_vp)]),
+    ("cvl_server_wait", C.c_int, [_vp, C.c_uint64, C.c_int64, C.POINTER(_vp)]),
+    ("cvl_server_stats_get", C.c_int, [_vp, C.POINTER(CvlServerStats)]),
+    ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.c_int64]),
+    ("cvl_server_destroy", None, [_vp]),
     ("cvl_engine_flush_l2", C.c_int, [_vp]),
     ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),
     ("cvl_engine_last_launch_count", C.c_int, [_vp]),

@@ -107,6 +107,13 @@ def _view_to_result(v: CvlResultView, owner: "_Owner | None" = None) -> Result:
                   int(v.truncated_anchors), int(v.num_edges), float(v.device_ms))
 
 
+def _result_from_handle(lib, r) -> Result:
+    owner = _Owner(lib, r, "cvl_result_free")
+    v = CvlResultView()
+    check(lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
+    return _view_to_result(v, owner)
+
+
 class _OwnedArray(np.ndarray):
     """An ndarray view that keeps the buffer's owner alive."""
 
@@ -240,6 +247,18 @@ class Engine:
               "cvl_batch_upload")
         return Batch(self, b, counts)
 
+    def upload_ragged(self, edges, counts) -> "Batch":
+        """A batch from maps already concatenated: edges [sum(counts), sz] (page-locked
+        memory, when it is, is copied to the device without staging)."""
+        e = _edges(edges)
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        if int(c.sum()) != e.shape[0]:
+            raise ValueError("counts must sum to the number of edge rows")
+        b = C.c_void_p()
+        check(self._lib.cvl_batch_upload(self._h, e.ctypes.data_as(_abi._dp), c.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         len(c), e.shape[1], C.byref(b)), "cvl_batch_upload")
+        return Batch(self, b, c)
+
     def run_batch(self, batch: "Batch", params: CurveletParams | None = None) -> "BatchResult":
         params = params or CurveletParams()
         p = params.to_c()
@@ -252,12 +271,16 @@ class Engine:
         check(self._lib.cvl_engine_flush_l2(self._h), "cvl_engine_flush_l2")
 
     def kernel_times(self) -> list[tuple[str, float]]:
-        names = (C.c_char_p * 64)()
-        ms = (C.c_double * 64)()
-        n = self._lib.cvl_engine_last_kernel_times(self._h, names, ms, 64)
+        n = self._lib.cvl_engine_last_kernel_times(self._h, None, None, 0)
         if n < 0:
             check(n, "cvl_engine_last_kernel_times")
-        return [(names[k].decode(), float(ms[k])) for k in range(min(n, 64))]
+        cap = max(n, 1)
+        names = (C.c_char_p * cap)()
+        ms = (C.c_double * cap)()
+        n = self._lib.cvl_engine_last_kernel_times(self._h, names, ms, cap)
+        if n < 0:
+            check(n, "cvl_engine_last_kernel_times")
+        return [(names[k].decode(), float(ms[k])) for k in range(min(n, cap))]
 
     def launch_count(self) -> int:
         n = self._lib.cvl_engine_last_launch_count(self._h)
@@ -276,9 +299,10 @@ class Batch:
         self._eng, self._h, self.counts = eng, h, counts
 
     def close(self):
-        if self._h:
+        # a batch's device memory goes with its engine; after Engine.close there is nothing to free
+        if self._h and getattr(self._eng, "_h", None):
             self._eng._lib.cvl_batch_free(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -297,14 +321,102 @@ class BatchResult:
         return {name: getattr(st, name) for name, _ in st._fields_}
 
     def map(self, m: int) -> Result:
+        """Map m, copied out of the batch's downloaded outputs."""
         v = CvlResultView()
         check(self._eng._lib.cvl_batch_result_map(self._h, m, C.byref(v)), "cvl_batch_result_map")
         return _view_to_result(v)
+
+    def take_map(self, m: int) -> Result:
+        """Map m as an independent result: only its rows are copied to page-locked
+        memory, and the arrays are views onto it."""
+        lib = self._eng._lib
+        r = C.c_void_p()
+        check(lib.cvl_batch_result_take_map(self._h, m, C.byref(r)), "cvl_batch_result_take_map")
+        return _result_from_handle(lib, r)
 
     def close(self):
         if self._h:
             self._eng._lib.cvl_batch_result_free(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Serving: continuous batching with memory-budget admission (cvl_server_*)
+# ---------------------------------------------------------------------------
+class Server:
+    """Requests in, results out; workers fold waiting maps into shared launches.
+    submit() copies the map and returns at once; wait()/poll() hand the result
+    out once."""
+
+    def __init__(self, params: CurveletParams | None = None, device: int = 0, workers: int = 2,
+                 mem_budget_bytes: int = 40 << 30, admit_bytes_per_edge: int = 2048,
+                 max_batch_edges: int = 4 << 20, large_map_edges: int = 1_000_000):
+        lib = _abi.load()
+        self._lib = lib
+        cfg = _abi.CvlServerCfg()
+        lib.cvl_server_cfg_default(C.byref(cfg))
+        cfg.device, cfg.workers, cfg.mem_budget_bytes = device, workers, mem_budget_bytes
+        cfg.admit_bytes_per_edge, cfg.max_batch_edges, cfg.large_map_edges = (admit_bytes_per_edge, max_batch_edges,
+                                                                              large_map_edges)
+        self._p = (params or CurveletParams()).to_c()
+        h = C.c_void_p()
+        check(lib.cvl_server_create(C.byref(cfg), C.byref(self._p), C.byref(h)), "cvl_server_create")
+        self._h = h
+
+    def submit(self, edges) -> int:
+        e = _edges(edges)
+        rid = C.c_uint64(0)
+        check(self._lib.cvl_server_submit(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1],
+                                          C.byref(rid)), "cvl_server_submit")
+        return int(rid.value)
+
+    def poll(self, rid: int) -> Result | None:
+        r = C.c_void_p()
+        rc = self._lib.cvl_server_poll(self._h, rid, C.byref(r))
+        if rc == _abi.CVL_EAGAIN:
+            return None
+        check(rc, "cvl_server_poll")
+        return _result_from_handle(self._lib, r)
+
+    def wait(self, rid: int, timeout_s: float | None = None) -> Result:
+        """The result; raises CvlError(CVL_ETIMEDOUT) if it is not ready in time."""
+        r = C.c_void_p()
+        us = -1 if timeout_s is None else int(timeout_s * 1e6)
+        check(self._lib.cvl_server_wait(self._h, rid, us, C.byref(r)), "cvl_server_wait")
+        return _result_from_handle(self._lib, r)
+
+    def stats(self) -> dict:
+        st = _abi.CvlServerStats()
+        check(self._lib.cvl_server_stats_get(self._h, C.byref(st)), "cvl_server_stats_get")
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def latencies(self) -> tuple[np.ndarray, np.ndarray]:
+        """(ms, edges) of every completed request, in completion order."""
+        n = int(self.stats()["completed"])
+        ms = np.zeros(max(n, 1))
+        ed = np.zeros(max(n, 1), np.int64)
+        k = self._lib.cvl_server_latencies(self._h, ms.ctypes.data_as(_abi._dp),
+                                           ed.ctypes.data_as(C.POINTER(C.c_int64)), n)
+        if k < 0:
+            check(int(k), "cvl_server_latencies")
+        return ms[:k], ed[:k]
+
+    def close(self):
+        if self._h:
+            self._lib.cvl_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

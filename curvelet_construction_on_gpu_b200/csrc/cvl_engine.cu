@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/cvl.h"
+#include "cvl_internal.h"
 #include "cvl_path.cuh"
 #include "cvl_scan.cuh"
 
@@ -62,6 +63,8 @@ inline unsigned next_pow2(unsigned long long v) {
 }
 
 }  // namespace
+
+int cvl_fail(int code, const std::string &msg) { return fail(code, msg); }
 
 // Page-locked host buffers for results, reused across runs: device-to-host
 // copies at full PCIe/C2C rate and no per-call host allocation. Shared by the
@@ -126,6 +129,7 @@ struct cvl_engine {
     DBuf chains, info, stats, err, work, scratch, scratch_chain, scratch_res, scan_tmp, flush, deg_orig, off_orig,
         gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start;
     unsigned long long chunk_pairs = CHUNK_PAIRS_DEFAULT;  // pairs per bundle chunk
+    std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
     DBuf pairs_in, pb_min, pb_max, pb_valid;
 
@@ -238,6 +242,8 @@ struct cvl_batch {
     cvl_engine *eng = nullptr;
     void *d_edges = nullptr;
     void *d_map_off = nullptr;
+    size_t edges_cap = 0;    // bytes allocated at d_edges
+    size_t map_off_cap = 0;  // entries allocated at d_map_off
     int num_maps = 0;
     int sz = 4;
     int n = 0;
@@ -247,7 +253,7 @@ struct cvl_batch {
 struct cvl_batch_result {
     cvl_engine *eng = nullptr;
     unsigned long long generation = 0;
-    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
+    std::shared_ptr<PinnedPool> pinned;
     int num_maps = 0;
     int n = 0;
     int width = 0;
@@ -257,9 +263,15 @@ struct cvl_batch_result {
     double device_ms = 0.0;
     int launches = 0;
     bool downloaded = false;
-    std::vector<uint32_t> chains;
-    std::vector<double> info;
+    uint32_t *chains = nullptr;  // pinned, from the engine's pool (all maps)
+    double *info = nullptr;
     bool truncated_any = false;
+    ~cvl_batch_result() {
+        if (pinned) {
+            pinned->put(chains);
+            pinned->put(info);
+        }
+    }
 };
 
 namespace {
@@ -803,6 +815,7 @@ void cvl_engine_destroy(cvl_engine *e) {
     if (!e) return;
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
+    while (!e->batches.empty()) cvl_batch_free(e->batches.back());
     e->release_all();
     for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
     cudaStreamDestroy(e->stream);
@@ -989,11 +1002,10 @@ int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_pa
 }
 
 // ---- device-resident batches -----------------------------------------------------
-int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps, int32_t edge_data_sz,
-                     cvl_batch **out) {
-    if (!e || !edges || !counts || !out || num_maps <= 0 || edge_data_sz < 4)
-        return fail(CVL_EINVAL, "invalid batch arguments");
-    *out = nullptr;
+int cvl_batch_refill(cvl_batch *b, const double *edges, const int32_t *counts, int32_t num_maps,
+                     int32_t edge_data_sz) {
+    if (!b || !edges || !counts || num_maps <= 0 || edge_data_sz < 4) return fail(CVL_EINVAL, "invalid batch arguments");
+    cvl_engine *e = b->eng;
     std::vector<int32_t> mo(num_maps + 1, 0);
     for (int m = 0; m < num_maps; ++m) {
         if (counts[m] <= 0) return fail(CVL_EINVAL, "every map needs at least one edge");
@@ -1001,27 +1013,63 @@ int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, 
         mo[m + 1] = mo[m] + counts[m];
     }
     CVL_CUDA(cudaSetDevice(e->device));
-    cvl_batch *b = new cvl_batch();
-    b->eng = e;
+    const size_t eb = sizeof(double) * (size_t)mo[num_maps] * edge_data_sz;
+    if (eb > b->edges_cap) {
+        // grow-only: a refill that fits reuses the buffer (no cudaFree, which would
+        // synchronise the whole device)
+        const size_t want = std::max(eb, b->edges_cap + b->edges_cap / 4);
+        if (b->d_edges) {
+            cudaFree(b->d_edges);
+            e->held -= b->edges_cap;
+            b->d_edges = nullptr;
+            b->edges_cap = 0;
+        }
+        if (e->budget && e->held + want > e->budget) return fail(CVL_ENOMEM, "batch exceeds the device memory budget");
+        if (cudaMalloc(&b->d_edges, want) != cudaSuccess) {
+            cudaGetLastError();
+            b->d_edges = nullptr;
+            return fail(CVL_ENOMEM, "batch allocation failed");
+        }
+        b->edges_cap = want;
+        e->held += want;
+    }
+    if ((size_t)mo.size() > b->map_off_cap) {
+        const size_t want = std::max(mo.size(), b->map_off_cap * 2);
+        if (b->d_map_off) cudaFree(b->d_map_off);
+        b->d_map_off = nullptr;
+        b->map_off_cap = 0;
+        if (cudaMalloc(&b->d_map_off, sizeof(int) * want) != cudaSuccess) {
+            cudaGetLastError();
+            b->d_map_off = nullptr;
+            return fail(CVL_ENOMEM, "batch allocation failed");
+        }
+        b->map_off_cap = want;
+    }
     b->num_maps = num_maps;
     b->sz = edge_data_sz;
     b->n = mo[num_maps];
     b->map_off = mo;
-    const size_t eb = sizeof(double) * (size_t)b->n * edge_data_sz;
-    if ((e->budget && e->held + eb > e->budget) || cudaMalloc(&b->d_edges, eb) != cudaSuccess ||
-        cudaMalloc(&b->d_map_off, sizeof(int) * mo.size()) != cudaSuccess) {
-        cudaGetLastError();
-        if (b->d_edges) cudaFree(b->d_edges);
-        delete b;
-        return fail(CVL_ENOMEM, "batch allocation failed");
-    }
-    e->held += eb;
-    cudaMemcpyAsync(b->d_edges, edges, eb, cudaMemcpyHostToDevice, e->stream);
-    cudaMemcpyAsync(b->d_map_off, mo.data(), sizeof(int) * mo.size(), cudaMemcpyHostToDevice, e->stream);
-    cudaError_t ce = cudaStreamSynchronize(e->stream);
-    if (ce != cudaSuccess) {
+    CVL_CUDA(cudaMemcpyAsync(b->d_edges, edges, eb, cudaMemcpyHostToDevice, e->stream));
+    CVL_CUDA(cudaMemcpyAsync(b->d_map_off, b->map_off.data(), sizeof(int) * mo.size(), cudaMemcpyHostToDevice,
+                             e->stream));
+    const cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return fail(CVL_ECUDA, std::string("batch upload: ") + cudaGetErrorString(ce));
+    return CVL_OK;
+}
+
+int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps, int32_t edge_data_sz,
+                     cvl_batch **out) {
+    if (!e || !edges || !counts || !out || num_maps <= 0 || edge_data_sz < 4)
+        return fail(CVL_EINVAL, "invalid batch arguments");
+    *out = nullptr;
+    cvl_batch *b = new cvl_batch();
+    b->eng = e;
+    e->batches.push_back(b);
+    const int rc = cvl_batch_refill(b, edges, counts, num_maps, edge_data_sz);
+    if (rc != CVL_OK) {
+        const std::string msg = g_err;
         cvl_batch_free(b);
-        return fail(CVL_ECUDA, std::string("batch upload: ") + cudaGetErrorString(ce));
+        return fail(rc, msg);
     }
     *out = b;
     return CVL_OK;
@@ -1029,10 +1077,12 @@ int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, 
 
 void cvl_batch_free(cvl_batch *b) {
     if (!b) return;
+    auto &bs = b->eng->batches;
+    bs.erase(std::remove(bs.begin(), bs.end(), b), bs.end());
     cudaSetDevice(b->eng->device);
     if (b->d_edges) {
         cudaFree(b->d_edges);
-        b->eng->held -= sizeof(double) * (size_t)b->n * b->sz;
+        b->eng->held -= b->edges_cap;
     }
     if (b->d_map_off) cudaFree(b->d_map_off);
     delete b;
@@ -1071,13 +1121,16 @@ int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view) 
     if (!r->downloaded) {
         if (r->eng->generation != r->generation)
             return fail(CVL_EINVAL, "batch result outputs were overwritten by a later run on the engine");
+        CVL_CUDA(cudaSetDevice(r->eng->device));
         const unsigned long long C = r->cv_off[r->num_maps];
-        r->chains.resize(C * r->width);
-        r->info.resize(C * 10);
+        r->pinned = r->eng->pinned;
+        r->chains = (uint32_t *)r->pinned->get(sizeof(unsigned) * (C ? C : 1) * r->width);
+        r->info = (double *)r->pinned->get(sizeof(double) * (C ? C : 1) * 10);
+        if (!r->chains || !r->info) return fail(CVL_ENOMEM, "page-locked result buffers could not be allocated");
         if (C) {
-            CVL_CUDA(cudaMemcpyAsync(r->chains.data(), r->eng->chains.p, sizeof(unsigned) * C * r->width,
+            CVL_CUDA(cudaMemcpyAsync(r->chains, r->eng->chains.p, sizeof(unsigned) * C * r->width,
                                      cudaMemcpyDeviceToHost, r->eng->stream));
-            CVL_CUDA(cudaMemcpyAsync(r->info.data(), r->eng->info.p, sizeof(double) * C * 10, cudaMemcpyDeviceToHost,
+            CVL_CUDA(cudaMemcpyAsync(r->info, r->eng->info.p, sizeof(double) * C * 10, cudaMemcpyDeviceToHost,
                                      r->eng->stream));
         }
         CVL_CUDA(cudaStreamSynchronize(r->eng->stream));
@@ -1087,8 +1140,8 @@ int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view) 
     cvl_result_view &v = *view;
     v.num_curvelets = (uint32_t)(c1 - c0);
     v.chain_width = (uint32_t)r->width;
-    v.chains = r->chains.data() + c0 * r->width;
-    v.info = r->info.data() + c0 * 10;
+    v.chains = r->chains + c0 * r->width;
+    v.info = r->info + c0 * 10;
     v.valid_pairs = r->stats[m].valid_pairs;
     v.total_neighbor_pairs = (int64_t)r->stats[m].pairs;
     v.max_num_of_neighbors = r->stats[m].max_deg;
@@ -1096,6 +1149,55 @@ int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view) 
     v.num_edges = (uint32_t)(r->map_off[m + 1] - r->map_off[m]);
     v.flags = v.truncated_anchors ? CVL_FLAG_TRUNCATED : 0u;
     v.device_ms = r->device_ms;
+    return CVL_OK;
+}
+
+int cvl_batch_result_take_map(cvl_batch_result *r, int32_t m, cvl_result **out) {
+    if (!r || !out || m < 0 || m >= r->num_maps) return fail(CVL_EINVAL, "invalid batch result arguments");
+    *out = nullptr;
+    if (!r->downloaded && r->eng->generation != r->generation)
+        return fail(CVL_EINVAL, "batch result outputs were overwritten by a later run on the engine");
+    cvl_engine *e = r->eng;
+    CVL_CUDA(cudaSetDevice(e->device));
+    const unsigned long long c0 = r->cv_off[m], c1 = r->cv_off[m + 1], C = c1 - c0;
+    cvl_result *res = new cvl_result();
+    res->pool = e->pinned;
+    res->chains_p = e->pinned->get(sizeof(unsigned) * (C ? C : 1) * r->width);
+    res->info_p = e->pinned->get(sizeof(double) * (C ? C : 1) * 10);
+    if (!res->chains_p || !res->info_p) {
+        delete res;
+        return fail(CVL_ENOMEM, "page-locked result buffers could not be allocated");
+    }
+    if (C) {
+        if (r->downloaded) {
+            std::memcpy(res->chains_p, r->chains + c0 * r->width, sizeof(unsigned) * C * r->width);
+            std::memcpy(res->info_p, r->info + c0 * 10, sizeof(double) * C * 10);
+        } else {
+            cudaError_t ce = cudaMemcpyAsync(res->chains_p, (const unsigned *)e->chains.p + c0 * r->width,
+                                             sizeof(unsigned) * C * r->width, cudaMemcpyDeviceToHost, e->stream);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(res->info_p, (const double *)e->info.p + c0 * 10, sizeof(double) * C * 10,
+                                     cudaMemcpyDeviceToHost, e->stream);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+            if (ce != cudaSuccess) {
+                delete res;
+                return fail(CVL_ECUDA, std::string("result download: ") + cudaGetErrorString(ce));
+            }
+        }
+    }
+    cvl_result_view &v = res->v;
+    v.num_curvelets = (uint32_t)C;
+    v.chain_width = (uint32_t)r->width;
+    v.chains = (const uint32_t *)res->chains_p;
+    v.info = (const double *)res->info_p;
+    v.valid_pairs = r->stats[m].valid_pairs;
+    v.total_neighbor_pairs = (int64_t)r->stats[m].pairs;
+    v.max_num_of_neighbors = r->stats[m].max_deg;
+    v.truncated_anchors = r->stats[m].truncated;
+    v.num_edges = (uint32_t)(r->map_off[m + 1] - r->map_off[m]);
+    v.flags = v.truncated_anchors ? CVL_FLAG_TRUNCATED : 0u;
+    v.device_ms = r->device_ms;
+    *out = res;
     return CVL_OK;
 }
 

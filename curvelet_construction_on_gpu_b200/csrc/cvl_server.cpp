@@ -1,0 +1,395 @@
+// cvl_server.cpp -- continuous batching over libcvl engines (cvl_server_* in
+// include/cvl.h).
+//
+// Requests are queued on the host. Each worker (one engine: its own stream and
+// workspace on the server's device) runs a loop in its own host thread:
+//   1. Take waiting requests from one lane, in arrival order, while they fit the
+//      launch (max_batch_edges) and the admission budget.
+//   2. Concatenate them into the worker's page-locked staging buffer.
+//   3. Refill the worker's device batch; the buffer is grow-only, so there is
+//      no cudaFree and no device-wide synchronisation.
+//   4. Run the whole path over the ragged batch.
+//   5. Copy each map's rows into its own page-locked result.
+//   6. Release the budget.
+// Workers run concurrently, so one batch's copies and kernels overlap another's.
+// Small and large maps have separate lanes, so a small map never waits behind a
+// 4K map in the same launch.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/cvl.h"
+#include "cvl_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    std::vector<double> edges;
+    int32_t n = 0, sz = 4;
+    size_t charge = 0;
+    int lane = 0;
+    Clock::time_point t_submit;
+    bool done = false;
+    int status = CVL_OK;
+    std::string err;
+    cvl_result *res = nullptr;
+};
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+struct cvl_server {
+    cvl_server_cfg cfg{};
+    cvl_params params{};
+    std::vector<cvl_engine *> engines;
+    std::vector<std::thread> threads;
+
+    std::mutex mu;
+    std::condition_variable cv_work;  // workers: requests queued or stop
+    std::condition_variable cv_done;  // waiters: a request finished
+    std::deque<Request *> lanes[2];   // 0 small, 1 large
+    std::unordered_map<uint64_t, Request *> reqs;
+    uint64_t next_id = 1;
+    size_t admitted = 0;
+    bool stop = false;
+
+    uint64_t submitted = 0, completed = 0, failed = 0, in_flight = 0, launches = 0, edges_completed = 0;
+    std::vector<double> lat_ms;
+    std::vector<int64_t> lat_edges;
+
+    // the lane a worker serves first (the last worker prefers large maps when there are several)
+    int preferred_lane(int w) const { return (cfg.workers >= 2 && w == cfg.workers - 1) ? 1 : 0; }
+
+    // lane whose head request fits the remaining budget, preferred lane first; -1 if none
+    int lane_to_take(int w) const {
+        const int pref = preferred_lane(w);
+        for (int k = 0; k < 2; ++k) {
+            const int l = k == 0 ? pref : 1 - pref;
+            if (!lanes[l].empty() && admitted + lanes[l].front()->charge <= cfg.mem_budget_bytes) return l;
+        }
+        return -1;
+    }
+
+    void finish(Request *r, int status, const std::string &err, cvl_result *res) {
+        // called with mu held
+        r->done = true;
+        r->status = status;
+        r->err = err;
+        r->res = res;
+        admitted -= r->charge;
+        --in_flight;
+        if (status == CVL_OK) {
+            ++completed;
+            edges_completed += (uint64_t)r->n;
+            lat_ms.push_back(ms_between(r->t_submit, Clock::now()));
+            lat_edges.push_back(r->n);
+        } else {
+            ++failed;
+        }
+    }
+
+    void worker(int w);
+};
+
+void cvl_server::worker(int w) {
+    cudaSetDevice(cfg.device);
+    cvl_engine *e = engines[w];
+    cvl_batch *batch = nullptr;
+    double *staging = nullptr;  // page-locked, grow-only
+    size_t staging_cap = 0;
+    std::vector<Request *> take;
+    std::vector<int32_t> counts;
+    while (true) {
+        take.clear();
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_work.wait(lk, [&] { return stop || lane_to_take(w) >= 0; });
+            if (stop) break;
+            const int l = lane_to_take(w);
+            int64_t sum = 0;
+            while (!lanes[l].empty()) {
+                Request *r = lanes[l].front();
+                if (!take.empty() && sum + r->n > cfg.max_batch_edges) break;
+                if (admitted + r->charge > cfg.mem_budget_bytes) break;
+                lanes[l].pop_front();
+                admitted += r->charge;
+                ++in_flight;
+                take.push_back(r);
+                sum += r->n;
+            }
+            ++launches;
+        }
+        // one edge_data_sz per launch: a request with another width goes alone
+        size_t cut = 1;
+        while (cut < take.size() && take[cut]->sz == take[0]->sz) ++cut;
+        if (cut < take.size()) {
+            std::lock_guard<std::mutex> lk(mu);
+            for (size_t k = take.size(); k-- > cut;) {
+                Request *r = take[k];
+                admitted -= r->charge;
+                --in_flight;
+                lanes[r->lane].push_front(r);
+            }
+            take.resize(cut);
+            cv_work.notify_all();
+        }
+        const int32_t sz = take[0]->sz;
+        size_t total = 0;
+        counts.clear();
+        for (Request *r : take) {
+            total += (size_t)r->n * sz;
+            counts.push_back(r->n);
+        }
+        int rc = CVL_OK;
+        std::string err;
+        if (total * sizeof(double) > staging_cap) {
+            if (staging) cudaFreeHost(staging);
+            staging = nullptr;
+            staging_cap = std::max(total * sizeof(double), staging_cap + staging_cap / 4);
+            if (cudaMallocHost((void **)&staging, staging_cap) != cudaSuccess) {
+                cudaGetLastError();
+                staging = nullptr;
+                staging_cap = 0;
+                rc = CVL_ENOMEM;
+                err = "page-locked staging buffer could not be allocated";
+            }
+        }
+        cvl_batch_result *br = nullptr;
+        if (rc == CVL_OK) {
+            size_t o = 0;
+            for (Request *r : take) {
+                std::memcpy(staging + o, r->edges.data(), sizeof(double) * (size_t)r->n * sz);
+                o += (size_t)r->n * sz;
+            }
+            rc = batch ? cvl_batch_refill(batch, staging, counts.data(), (int32_t)counts.size(), sz)
+                       : cvl_batch_upload(e, staging, counts.data(), (int32_t)counts.size(), sz, &batch);
+            if (rc == CVL_OK) rc = cvl_batch_run(e, batch, &params, &br);
+            if (rc != CVL_OK) err = cvl_last_error();
+        }
+        std::vector<cvl_result *> outs(take.size(), nullptr);
+        std::vector<int> st(take.size(), rc);
+        std::vector<std::string> errs(take.size(), err);
+        if (rc == CVL_OK) {
+            for (size_t m = 0; m < take.size(); ++m) {
+                st[m] = cvl_batch_result_take_map(br, (int32_t)m, &outs[m]);
+                if (st[m] != CVL_OK) errs[m] = cvl_last_error();
+            }
+        }
+        if (br) cvl_batch_result_free(br);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (size_t m = 0; m < take.size(); ++m) {
+                take[m]->edges.clear();
+                take[m]->edges.shrink_to_fit();
+                finish(take[m], st[m], errs[m], outs[m]);
+            }
+        }
+        cv_done.notify_all();
+        cv_work.notify_all();  // budget freed
+    }
+    if (batch) cvl_batch_free(batch);
+    if (staging) cudaFreeHost(staging);
+}
+
+extern "C" {
+
+void cvl_server_cfg_default(cvl_server_cfg *c) {
+    if (!c) return;
+    c->device = 0;
+    c->workers = 2;
+    c->mem_budget_bytes = (size_t)40 << 30;
+    c->admit_bytes_per_edge = 2048;
+    c->max_batch_edges = 4 << 20;
+    c->large_map_edges = 1000000;
+}
+
+int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out) {
+    if (!out || !p) return cvl_fail(CVL_EINVAL, "out/params is NULL");
+    *out = nullptr;
+    cvl_server_cfg c;
+    cvl_server_cfg_default(&c);
+    if (cfg) c = *cfg;
+    if (c.workers < 1 || c.workers > 16) return cvl_fail(CVL_EINVAL, "workers must be in [1, 16]");
+    if (c.mem_budget_bytes == 0 || c.admit_bytes_per_edge == 0 || c.max_batch_edges <= 0 || c.large_map_edges <= 0)
+        return cvl_fail(CVL_EINVAL, "budget, admission charge and batch sizes must be > 0");
+    cvl_server *s = new cvl_server();
+    s->cfg = c;
+    s->params = *p;
+    for (int w = 0; w < c.workers; ++w) {
+        cvl_engine_cfg ec;
+        cvl_engine_cfg_default(&ec);
+        ec.device = c.device;
+        cvl_engine *e = nullptr;
+        const int rc = cvl_engine_create(&ec, &e);
+        if (rc != CVL_OK) {
+            const std::string msg = cvl_last_error();
+            for (cvl_engine *x : s->engines) cvl_engine_destroy(x);
+            delete s;
+            return cvl_fail(rc, msg);
+        }
+        s->engines.push_back(e);
+    }
+    for (int w = 0; w < c.workers; ++w) s->threads.emplace_back(&cvl_server::worker, s, w);
+    *out = s;
+    return CVL_OK;
+}
+
+int cvl_server_submit(cvl_server *s, const double *edges, int32_t num_edges, int32_t edge_data_sz, uint64_t *id) {
+    const Clock::time_point t_call = Clock::now();  // latency counts the copy below
+    if (!s || !edges || !id) return cvl_fail(CVL_EINVAL, "server/edges/id is NULL");
+    if (num_edges <= 0 || edge_data_sz < 4) return cvl_fail(CVL_EINVAL, "num_edges <= 0 or edge_data_sz < 4");
+    const size_t charge = (size_t)num_edges * s->cfg.admit_bytes_per_edge;
+    if (charge > s->cfg.mem_budget_bytes)
+        return cvl_fail(CVL_ENOMEM, "a map of " + std::to_string(num_edges) + " edges needs " + std::to_string(charge) +
+                                        " bytes of admission budget; the budget is " +
+                                        std::to_string(s->cfg.mem_budget_bytes));
+    Request *r = new Request();
+    r->edges.assign(edges, edges + (size_t)num_edges * edge_data_sz);
+    r->n = num_edges;
+    r->sz = edge_data_sz;
+    r->charge = charge;
+    r->lane = (num_edges >= s->cfg.large_map_edges) ? 1 : 0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+            delete r;
+            return cvl_fail(CVL_EINVAL, "server is stopping");
+        }
+        r->id = s->next_id++;
+        r->t_submit = t_call;
+        s->reqs[r->id] = r;
+        s->lanes[r->lane].push_back(r);
+        ++s->submitted;
+        *id = r->id;
+    }
+    s->cv_work.notify_all();
+    return CVL_OK;
+}
+
+namespace {
+
+// hands out a finished request's result and forgets the request (mu held)
+int hand_out(cvl_server *s, std::unordered_map<uint64_t, Request *>::iterator it, cvl_result **out) {
+    Request *r = it->second;
+    s->reqs.erase(it);
+    const int st = r->status;
+    const std::string err = r->err;
+    *out = r->res;
+    delete r;
+    if (st != CVL_OK) return cvl_fail(st, err);
+    return CVL_OK;
+}
+
+}  // namespace
+
+int cvl_server_poll(cvl_server *s, uint64_t id, cvl_result **out) {
+    if (!s || !out) return cvl_fail(CVL_EINVAL, "server/out is NULL");
+    *out = nullptr;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return cvl_fail(CVL_EINVAL, "unknown request id (or its result was handed out)");
+    if (!it->second->done) return cvl_fail(CVL_EAGAIN, "request not finished");
+    return hand_out(s, it, out);
+}
+
+int cvl_server_wait(cvl_server *s, uint64_t id, int64_t timeout_us, cvl_result **out) {
+    if (!s || !out) return cvl_fail(CVL_EINVAL, "server/out is NULL");
+    *out = nullptr;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return cvl_fail(CVL_EINVAL, "unknown request id (or its result was handed out)");
+    Request *r = it->second;
+    auto ready = [&] { return r->done; };
+    if (timeout_us < 0) {
+        s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), ready)) {
+        return cvl_fail(CVL_ETIMEDOUT, "request not finished within the timeout");
+    }
+    return hand_out(s, s->reqs.find(id), out);
+}
+
+int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out) {
+    if (!s || !out) return cvl_fail(CVL_EINVAL, "server/out is NULL");
+    std::vector<double> l;
+    cvl_server_stats st{};
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        st.submitted = s->submitted;
+        st.completed = s->completed;
+        st.failed = s->failed;
+        st.queued = s->lanes[0].size() + s->lanes[1].size();
+        st.in_flight = s->in_flight;
+        st.launches = s->launches;
+        st.edges_completed = s->edges_completed;
+        st.admitted_bytes = s->admitted;
+        l = s->lat_ms;
+    }
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double q) {  // nearest rank
+            size_t k = (size_t)std::ceil(q * (double)l.size());
+            return l[std::min(l.size() - 1, k ? k - 1 : 0)];
+        };
+        st.p50_ms = pct(0.50);
+        st.p95_ms = pct(0.95);
+        st.p99_ms = pct(0.99);
+        st.max_ms = l.back();
+    }
+    *out = st;
+    return CVL_OK;
+}
+
+int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, int64_t cap) {
+    if (!s || cap < 0 || (cap > 0 && (!ms || !edges))) return cvl_fail(CVL_EINVAL, "invalid arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int64_t n = std::min<int64_t>(cap, (int64_t)s->lat_ms.size());
+    for (int64_t k = 0; k < n; ++k) {
+        ms[k] = s->lat_ms[k];
+        edges[k] = s->lat_edges[k];
+    }
+    return n;
+}
+
+void cvl_server_destroy(cvl_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        for (auto &q : s->lanes) {
+            for (Request *r : q) {
+                r->done = true;
+                r->status = CVL_EINVAL;
+                r->err = "server stopped before the request was admitted";
+                ++s->failed;
+            }
+            q.clear();
+        }
+    }
+    s->cv_work.notify_all();
+    for (std::thread &t : s->threads) t.join();
+    s->cv_done.notify_all();
+    for (auto &kv : s->reqs) {
+        if (kv.second->res) cvl_result_free(kv.second->res);
+        delete kv.second;
+    }
+    for (cvl_engine *e : s->engines) cvl_engine_destroy(e);
+    delete s;
+}
+
+}  // extern "C"

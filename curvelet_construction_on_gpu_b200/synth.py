@@ -130,6 +130,12 @@ def mixed_map(seed: int) -> np.ndarray:
     return _assemble(rng, _hd_curves(rng, n, W, H), W, H, 0.20)
 
 
+def mixed_map_image(seed: int) -> tuple[int, int]:
+    """The image size (W, H) that mixed_map(seed) draws."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return IMAGE_SIZES[int(rng.integers(0, len(IMAGE_SIZES)))]
+
+
 def mixed64(base_seed: int = 2000, n_maps: int = 64) -> list[np.ndarray]:
     return [mixed_map(base_seed + i) for i in range(n_maps)]
 

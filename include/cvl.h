@@ -75,6 +75,8 @@ typedef struct cvl_engine_cfg {
 
 void cvl_engine_cfg_default(cvl_engine_cfg *cfg);
 int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out);
+/* Also frees the engine's batches that are still alive (their handles become
+ * invalid), and any batch result of the engine can then no longer be read. */
 void cvl_engine_destroy(cvl_engine *e);
 
 /* One-line description of the calling thread's last error ("" if none). */
@@ -190,6 +192,11 @@ typedef struct cvl_batch cvl_batch;
 
 int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps,
                      int32_t edge_data_sz, cvl_batch **out);
+/* Replaces a batch's maps with new ones. The device buffer is reused when it is
+ * large enough (grow-only), so a steady stream of batches makes no device
+ * allocation and no device-wide synchronisation. */
+int cvl_batch_refill(cvl_batch *b, const double *edges, const int32_t *counts, int32_t num_maps,
+                     int32_t edge_data_sz);
 void cvl_batch_free(cvl_batch *b);
 
 /* Runs the whole path over every map of a device-resident batch in one pass
@@ -198,8 +205,12 @@ void cvl_batch_free(cvl_batch *b);
  * filled. Per-map results are read with cvl_batch_result_*. */
 typedef struct cvl_batch_result cvl_batch_result;
 int cvl_batch_run(cvl_engine *e, const cvl_batch *b, const cvl_params *p, cvl_batch_result **out);
-/* Downloads (once) and views map m of a batch result. */
+/* Downloads (once, into page-locked memory) and views map m of a batch result;
+ * the view lives as long as the batch result. */
 int cvl_batch_result_map(cvl_batch_result *r, int32_t m, cvl_result_view *view);
+/* Map m of a batch result as an independent result (its own page-locked
+ * copy, freed with cvl_result_free): only that map's rows cross PCIe. */
+int cvl_batch_result_take_map(cvl_batch_result *r, int32_t m, cvl_result **out);
 /* Totals of a batch run over all its maps. */
 typedef struct cvl_batch_stats {
     double device_ms;              /* device time of the batch compute (CUDA events) */
@@ -214,6 +225,66 @@ typedef struct cvl_batch_stats {
 } cvl_batch_stats;
 int cvl_batch_result_stats(const cvl_batch_result *r, cvl_batch_stats *out);
 void cvl_batch_result_free(cvl_batch_result *r);
+
+/* ---- serving: continuous batching with memory-budget admission ----------
+ * No reference counterpart (the reference runs one map per process). A server
+ * owns `workers` engines on one device, each with its own stream and
+ * workspace. Each engine works in its own host thread:
+ *   1. It takes waiting requests from its lane's queue in arrival order, up to
+ *      max_batch_edges per launch, while the admission budget allows.
+ *   2. It uploads them as one ragged batch and runs the whole path.
+ *   3. It hands each map's result to its request.
+ * Requests that arrive while others are on the GPU are folded into the next
+ * launch of a free worker, and the workers' launches overlap on the device.
+ *
+ * Maps of at least large_map_edges edges go to a separate lane, so small
+ * maps do not queue behind them. With two or more workers, the last worker
+ * prefers the large lane and the others the small one; an idle worker takes
+ * from the other lane.
+ *
+ * Admission: a request holds admit_bytes_per_edge × its edges of the budget
+ * from upload to result. A request that can never fit is refused at submit
+ * with CVL_ENOMEM. One server serves one cvl_params. */
+typedef struct cvl_server cvl_server;
+typedef struct cvl_server_cfg {
+    int device;                    /* CUDA device ordinal (0) */
+    int workers;                   /* engines working concurrently (2) */
+    size_t mem_budget_bytes;       /* device bytes that admitted requests may hold at once (40 GiB) */
+    size_t admit_bytes_per_edge;   /* admission charge per edge (2048: about twice the path's measured
+                                      footprint per edge, edges + hash + neighbour pairs + curvelets) */
+    int64_t max_batch_edges;       /* edges folded into one launch at most; a larger map runs alone (4 Mi) */
+    int64_t large_map_edges;       /* maps with at least this many edges use the large lane (1,000,000) */
+} cvl_server_cfg;
+
+typedef struct cvl_server_stats {
+    uint64_t submitted, completed, failed;
+    uint64_t queued;               /* waiting for admission */
+    uint64_t in_flight;            /* admitted, result not ready */
+    uint64_t launches;             /* batch runs */
+    uint64_t edges_completed;
+    size_t admitted_bytes;         /* budget held right now */
+    double p50_ms, p95_ms, p99_ms; /* submit -> result ready, over completed requests */
+    double max_ms;
+} cvl_server_stats;
+
+void cvl_server_cfg_default(cvl_server_cfg *cfg);
+int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out);
+/* Copies the map (AoS rows of edge_data_sz doubles) and queues it; never blocks
+ * on the device. *id names the request. */
+int cvl_server_submit(cvl_server *s, const double *edges, int32_t num_edges, int32_t edge_data_sz, uint64_t *id);
+/* The request's result (caller frees it with cvl_result_free), or CVL_EAGAIN
+ * while it is queued or running. A request's result is handed out once. */
+int cvl_server_poll(cvl_server *s, uint64_t id, cvl_result **out);
+/* As poll, waiting up to timeout_us microseconds (< 0: no limit); CVL_ETIMEDOUT
+ * if the result is not ready by then (the request stays queued). */
+int cvl_server_wait(cvl_server *s, uint64_t id, int64_t timeout_us, cvl_result **out);
+int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out);
+/* Latency (ms, submit -> result ready) and edge count of each completed
+ * request, in completion order; returns how many were written (<= cap). */
+int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, int64_t cap);
+/* Finishes the requests already admitted, drops the queued ones, stops the
+ * workers and releases everything. */
+void cvl_server_destroy(cvl_server *s);
 
 /* Writes a buffer larger than the L2 cache on the engine's stream and waits
  * (timing hygiene between benchmark iterations). */

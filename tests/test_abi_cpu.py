@@ -90,3 +90,28 @@ def test_cli_flags_without_gpu(tmp_path):
     run_dir.mkdir()
     r = subprocess.run([cli, "--edge-file", "nope.txt"], capture_output=True, text=True, cwd=run_dir)
     assert r.returncode == 1 and "input file does not exist: ../test_files/nope.txt" in r.stderr
+
+
+def test_server_defaults_and_argument_checks():
+    lib = _abi.load()
+    cfg = _abi.CvlServerCfg()
+    lib.cvl_server_cfg_default(C.byref(cfg))
+    assert (cfg.device, cfg.workers, cfg.mem_budget_bytes) == (0, 2, 40 << 30)
+    assert (cfg.admit_bytes_per_edge, cfg.max_batch_edges, cfg.large_map_edges) == (2048, 4 << 20, 1_000_000)
+    h = C.c_void_p()
+    p = cvl.CurveletParams().to_c()
+    assert lib.cvl_server_create(C.byref(cfg), None, C.byref(h)) == _abi.CVL_EINVAL
+    bad = _abi.CvlServerCfg()
+    lib.cvl_server_cfg_default(C.byref(bad))
+    bad.workers = 0
+    assert lib.cvl_server_create(C.byref(bad), C.byref(p), C.byref(h)) == _abi.CVL_EINVAL
+    rid = C.c_uint64(0)
+    assert lib.cvl_server_submit(None, None, 1, 4, C.byref(rid)) == _abi.CVL_EINVAL
+    assert lib.cvl_server_wait(None, 1, 0, C.byref(h)) == _abi.CVL_EINVAL
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU failure path")
+def test_server_without_gpu_fails_loudly():
+    with pytest.raises(cvl.CvlError) as ei:
+        cvl.Server()
+    assert ei.value.code == _abi.CVL_ENODEV
