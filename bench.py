@@ -56,7 +56,7 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--rate", type=float, default=100.0, help="served stream: offered maps/s")
+    ap.add_argument("--rate", type=float, default=50.0, help="served stream: offered maps/s")
     ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")
     ap.add_argument("--requests", type=int, default=600, help="served stream: requests per rate")
     ap.add_argument("--workers", type=int, default=2, help="served stream: server workers")
@@ -300,18 +300,21 @@ def _served(maps, images, rate: float, n_req: int, workers: int, device: int, se
     import threading
 
     import curvelet_construction_on_gpu_b200 as cvl
+    from curvelet_construction_on_gpu_b200 import _abi
     rng = np.random.default_rng(seed)
     picks = rng.integers(0, len(maps), n_req)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     srv = cvl.Server(device=device, workers=workers)
     try:
-        # warm-up (workspace growth): the largest and a small map through every worker
+        # warm-up (workspace and page-locked arena growth): the largest map once per
+        # worker, then every map of the pool once
         order = np.argsort([m.shape[0] for m in maps])
         warm = [srv.submit(maps[int(order[-1])]) for _ in range(workers)]
-        warm += [srv.submit(maps[int(order[0])]) for _ in range(workers)]
-        for w in warm:
-            srv.wait(w)
+        warm += [srv.submit(m) for m in maps]
+        for _ in warm:
+            srv.next()
         n_warm = len(warm)
+        warm_stats = srv.stats()
         ids = [None] * n_req
         t0 = time.perf_counter()
 
@@ -324,14 +327,25 @@ def _served(maps, images, rate: float, n_req: int, workers: int, device: int, se
 
         th = threading.Thread(target=submitter)
         th.start()
-        for k in range(n_req):
-            while ids[k] is None:
+        # results are taken in completion order (as each client would take its own)
+        got = 0
+        while got < n_req:
+            try:
+                r = srv.next(timeout_s=0.5)
+            except cvl.CvlError as e:
+                if e.code == _abi.CVL_ETIMEDOUT:
+                    continue
+                raise
+            if r is None:  # nothing submitted yet
                 time.sleep(0.0002)
-            srv.wait(ids[k])
+                continue
+            got += 1
+            del r
         th.join()
         wall = time.perf_counter() - t0
         st = srv.stats()
         ms, ed = srv.latencies()
+        st0 = warm_stats
     finally:
         srv.close()
     ms, ed = ms[n_warm:], ed[n_warm:]
@@ -346,7 +360,9 @@ def _served(maps, images, rate: float, n_req: int, workers: int, device: int, se
             "edges_per_s": edges / wall, "maps_per_s": len(ms) / wall,
             "p50_ms": pct(ms, 50), "p95_ms": pct(ms, 95), "p99_ms": pct(ms, 99), "max_ms": float(np.max(ms)),
             "hd_1920x1080": {"requests": int(len(hd)), "p50_ms": pct(hd, 50), "p99_ms": pct(hd, 99)},
-            "launches": int(st["launches"]) - n_warm, "failed": int(st["failed"]),
+            "launches": int(st["launches"] - st0["launches"]), "failed": int(st["failed"]),
+            "worker_ms": {k: float(st[k] - st0[k]) for k in ("upload_ms", "run_ms", "device_ms", "result_ms")},
+            "queue_ms_mean": float(st["queue_ms"] - st0["queue_ms"]) / max(1, len(ms)),
             "admission": "40 GiB budget, 2048 B per edge", "pool": f"{len(maps)} seeded maps"}
 
 

@@ -32,7 +32,8 @@ class CvlParams(C.Structure):
 
 class CvlEngineCfg(C.Structure):
     _fields_ = [("device", C.c_int), ("mem_budget_bytes", C.c_size_t), ("cell_size", C.c_int),
-                ("seeds_per_group", C.c_int), ("bundle_slots", C.c_int), ("warps_per_block", C.c_int)]
+                ("seeds_per_group", C.c_int), ("bundle_slots", C.c_int), ("warps_per_block", C.c_int),
+                ("stream_priority", C.c_int)]
 
 
 class CvlResultView(C.Structure):
@@ -66,7 +67,9 @@ class CvlServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("queued", C.c_uint64), ("in_flight", C.c_uint64), ("launches", C.c_uint64),
                 ("edges_completed", C.c_uint64), ("admitted_bytes", C.c_size_t), ("p50_ms", C.c_double),
-                ("p95_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double)]
+                ("p95_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("upload_ms", C.c_double), ("run_ms", C.c_double), ("device_ms", C.c_double),
+                ("result_ms", C.c_double), ("queue_ms", C.c_double)]
 
 
 # (name, restype, argtypes) of every entry point declared in include/cvl.h
@@ -94,6 +97,7 @@ SIGNATURES = [
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
     ("cvl_batch_upload", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_vp)]),
     ("cvl_batch_refill", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32]),
+    ("cvl_batch_refill_parts", C.c_int, [_vp, C.POINTER(_dp), C.POINTER(C.c_int32), C.c_int32, C.c_int32]),
     ("cvl_batch_free", None, [_vp]),
     ("cvl_batch_run", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.POINTER(_vp)]),
     ("cvl_batch_result_map", C.c_int, [_vp, C.c_int32, C.POINTER(CvlResultView)]),
@@ -105,6 +109,7 @@ SIGNATURES = [
     ("cvl_server_submit", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.POINTER(C.c_uint64)]),
     ("cvl_server_poll", C.c_int, [_vp, C.c_uint64, C.POINTER(_vp)]),
     ("cvl_server_wait", C.c_int, [_vp, C.c_uint64, C.c_int64, C.POINTER(_vp)]),
+    ("cvl_server_next", C.c_int, [_vp, C.c_int64, C.POINTER(C.c_uint64), C.POINTER(_vp)]),
     ("cvl_server_stats_get", C.c_int, [_vp, C.POINTER(CvlServerStats)]),
     ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.c_int64]),
     ("cvl_server_destroy", None, [_vp]),

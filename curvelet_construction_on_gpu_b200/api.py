@@ -391,6 +391,18 @@ class Server:
         check(self._lib.cvl_server_wait(self._h, rid, us, C.byref(r)), "cvl_server_wait")
         return _result_from_handle(self._lib, r)
 
+    def next(self, timeout_s: float | None = None) -> tuple[int, Result] | None:
+        """(id, result) of the earliest finished request not handed out yet, in
+        completion order; None when nothing is queued or running."""
+        r = C.c_void_p()
+        rid = C.c_uint64(0)
+        us = -1 if timeout_s is None else int(timeout_s * 1e6)
+        rc = self._lib.cvl_server_next(self._h, us, C.byref(rid), C.byref(r))
+        if rc == _abi.CVL_EAGAIN:
+            return None
+        check(rc, "cvl_server_next")
+        return int(rid.value), _result_from_handle(self._lib, r)
+
     def stats(self) -> dict:
         st = _abi.CvlServerStats()
         check(self._lib.cvl_server_stats_get(self._h, C.byref(st)), "cvl_server_stats_get")

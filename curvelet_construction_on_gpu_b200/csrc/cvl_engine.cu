@@ -19,6 +19,7 @@
 
 #include "../../include/cvl.h"
 #include "cvl_internal.h"
+#include "cvl_pinned.h"
 #include "cvl_path.cuh"
 #include "cvl_scan.cuh"
 
@@ -66,49 +67,10 @@ inline unsigned next_pow2(unsigned long long v) {
 
 int cvl_fail(int code, const std::string &msg) { return fail(code, msg); }
 
-// Page-locked host buffers for results, reused across runs: device-to-host
-// copies at full PCIe/C2C rate and no per-call host allocation. Shared by the
+// Results live in page-locked memory (cvl::PinnedArena): device-to-host copies
+// at full PCIe/C2C rate and no per-call pinning. The arena is shared by the
 // engine and its live results, so a result may outlive its engine.
-struct PinnedPool {
-    struct Block {
-        void *p;
-        size_t bytes;
-        bool used;
-    };
-    std::mutex mu;
-    std::vector<Block> blocks;
-    ~PinnedPool() {
-        for (Block &b : blocks) cudaFreeHost(b.p);
-    }
-    void *get(size_t bytes) {
-        std::lock_guard<std::mutex> g(mu);
-        int best = -1;
-        for (size_t k = 0; k < blocks.size(); ++k)
-            if (!blocks[k].used && blocks[k].bytes >= bytes && (best < 0 || blocks[k].bytes < blocks[best].bytes))
-                best = (int)k;
-        if (best >= 0) {
-            blocks[best].used = true;
-            return blocks[best].p;
-        }
-        void *p = nullptr;
-        const size_t want = std::max(bytes + bytes / 8, (size_t)1 << 16);
-        if (cudaMallocHost(&p, want) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        blocks.push_back({p, want, true});
-        return p;
-    }
-    void put(void *p) {
-        if (!p) return;
-        std::lock_guard<std::mutex> g(mu);
-        for (Block &b : blocks)
-            if (b.p == p) {
-                b.used = false;
-                return;
-            }
-    }
-};
+using PinnedPool = cvl::PinnedArena;
 
 struct cvl_engine {
     int device = 0;
@@ -127,7 +89,7 @@ struct cvl_engine {
     DBuf bx, by, bth, bsp, bcp, bsm, bcm, bcell, bmap;
     DBuf ncand, deg, pair_off, csr_ids, csr_d2, rec_ids, rec_k, rec_meta, count, out_off;
     DBuf chains, info, stats, err, work, scratch, scratch_chain, scratch_res, scan_tmp, flush, deg_orig, off_orig,
-        gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start;
+        gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start, crank;
     unsigned long long chunk_pairs = CHUNK_PAIRS_DEFAULT;  // pairs per bundle chunk
     std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
@@ -143,7 +105,7 @@ struct cvl_engine {
     int alloc(DBuf &b, size_t bytes) {
         if (bytes == 0) bytes = 16;
         if (b.bytes >= bytes) return CVL_OK;
-        size_t want = std::max(bytes, b.bytes + b.bytes / 4);
+        size_t want = std::max(bytes, b.bytes + b.bytes / 2);
         want = (want + 255) & ~(size_t)255;
         if (b.p) {
             cudaFree(b.p);
@@ -202,7 +164,7 @@ struct cvl_engine {
         DBuf *all[] = {&edges, &map_off, &ehash, &bcount, &bstart, &bfill, &pos_of, &orig_of, &bx, &by, &bth, &bsp,
                        &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
                        &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
-                       &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
+                       &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
                        &pb_max, &pb_valid};
         for (DBuf *b : all) {
             if (b->p) cudaFree(b->p);
@@ -341,6 +303,28 @@ int check_launch(const char *what) {
     return CVL_OK;
 }
 
+// Host<->device copies in pieces of at most 32 MiB: the copy engines take
+// commands in turn across streams, so a large map's transfer does not hold up
+// a small map's for the whole of its length.
+inline cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+    constexpr size_t PIECE = (size_t)32 << 20;
+    for (size_t o = 0; o < bytes; o += PIECE) {
+        const cudaError_t ce =
+            cudaMemcpyAsync((char *)dst + o, (const char *)src + o, std::min(PIECE, bytes - o), kind, s);
+        if (ce != cudaSuccess) return ce;
+    }
+    return cudaSuccess;
+}
+
+// Grids of short blocks: `per_block` work items per block and no cap, so a
+// kernel of a large map never holds an SM for long and a higher-priority
+// stream's blocks start as soon as any block ends (the kernels stride over
+// their items, so any grid is correct).
+inline int short_grid(long long n, long long per_block) {
+    long long g = (n + per_block - 1) / per_block;
+    return (int)std::max(1LL, std::min(g, 0x7fffffffLL));
+}
+
 inline int grid_for(const cvl_engine *e, long long n, int threads, int per_sm = 16) {
     long long g = (n + threads - 1) / threads;
     const long long cap = (long long)e->prop.multiProcessorCount * per_sm;
@@ -394,15 +378,11 @@ struct RunOut {
 
 template <int CPL>
 int launch_bundles(cvl_engine *e, BundleArgs &a, int blocks) {
-    // one resident wave: the kernel strides over the chunk's pairs
-    static thread_local int per_sm = 0;
-    if (per_sm <= 0) {
-        CVL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bundles<CPL>, BUNDLE_THREADS, 0));
-        if (per_sm <= 0) per_sm = 1;
-    }
+    // one block per PPB pairs and no grid stride: short blocks, so that a
+    // higher-priority stream's blocks get SMs as soon as any block ends
     const long long ppb = BUNDLE_THREADS / a.md.Q;
     const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
-    blocks = (int)std::max(1LL, std::min<long long>(need, (long long)e->prop.multiProcessorCount * per_sm));
+    blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
     k_bundles<CPL><<<blocks, BUNDLE_THREADS, 0, e->stream>>>(a);
     return check_launch("k_bundles");
 }
@@ -410,6 +390,10 @@ int launch_bundles(cvl_engine *e, BundleArgs &a, int blocks) {
 template <int CPL, int K>
 int launch_growth(cvl_engine *e, GrowthArgs &a, size_t smem, int blocks) {
     CVL_CUDA(cudaFuncSetAttribute(k_growth<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // a warp per anchor, 4 anchors per warp: short blocks (a higher-priority
+    // stream's blocks get SMs as soon as any block ends) with the per-block
+    // set-up spread over 16 anchors
+    blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + 15) / 16, 0x7fffffffLL));
     k_growth<CPL, K><<<blocks, 128, smem, e->stream>>>(a);
     return check_launch("k_growth");
 }
@@ -488,7 +472,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     CVL_CUDA(cudaMemsetAsync(e->work.p, 0, sizeof(unsigned long long) * 2, s));
 
     // ---- (a) binning
-    const int gb = grid_for(e, n, 256);
+    const int gb = short_grid(n, 256);
     k_bin_keys<<<gb, 256, 0, s>>>(d_edges, sz, n, d_map_off, M, md, (unsigned *)e->ehash.p, (unsigned *)e->bcount.p,
                                   err);
     CVL_TRY(check_launch("k_bin_keys"));
@@ -503,7 +487,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     const size_t nb_smem = (size_t)nb_wpb * nbr_smem_per_warp(md.max_cand);
     CVL_CUDA(cudaFuncSetAttribute(k_nb<NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
     CVL_CUDA(cudaFuncSetAttribute(k_nb<NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
-    const int gn = grid_for(e, n, nb_wpb, 16);
+    const int gn = short_grid(n, (long long)nb_wpb * 4);  // a warp per anchor, 4 anchors per warp
     NbArgs na{};
     na.md = md;
     na.B = B;
@@ -600,6 +584,9 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
         } else {
             cap = 0;
         }
+        CVL_TRY(e->alloc(e->crank, sizeof(unsigned short) * CELLS_MAX));
+        k_cell_ranks<<<1, 128, 0, s>>>(md, (unsigned short *)e->crank.p);
+        CVL_TRY(check_launch("k_cell_ranks"));
         Records rec;
         rec.ids = (unsigned *)e->rec_ids.p;
         rec.k = (double *)e->rec_k.p;
@@ -646,6 +633,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
             ga.stats = stats;
             ga.count_only = (mode == 1) ? 1 : 0;
             ga.err = err;
+            ga.cell_rank = (const unsigned short *)e->crank.p;
             CVL_TRY(gf(e, ga, gsmem, gblocks));
             e->mark("growth");
         }
@@ -770,6 +758,7 @@ void cvl_engine_cfg_default(cvl_engine_cfg *c) {
     c->cell_size = 0;
     c->seeds_per_group = 0;
     c->bundle_slots = 0;
+    c->stream_priority = 0;
     c->warps_per_block = 0;
 }
 
@@ -797,7 +786,13 @@ int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out) {
     e->slots = c.bundle_slots > 0 ? c.bundle_slots : 10;
     cudaError_t ce = cudaSetDevice(e->device);
     if (ce == cudaSuccess) ce = cudaGetDeviceProperties(&e->prop, e->device);
-    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) {
+        int least = 0, greatest = 0;
+        ce = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        // lower numbers are higher priorities; clamp to the device's range
+        const int prio = std::min(std::max(c.stream_priority, greatest), least);
+        if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, prio);
+    }
     if (ce != cudaSuccess) {
         delete e;
         return fail(CVL_ECUDA, std::string("engine init: ") + cudaGetErrorString(ce));
@@ -1002,9 +997,11 @@ int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_pa
 }
 
 // ---- device-resident batches -----------------------------------------------------
-int cvl_batch_refill(cvl_batch *b, const double *edges, const int32_t *counts, int32_t num_maps,
-                     int32_t edge_data_sz) {
-    if (!b || !edges || !counts || num_maps <= 0 || edge_data_sz < 4) return fail(CVL_EINVAL, "invalid batch arguments");
+int cvl_batch_refill_parts(cvl_batch *b, const double *const *parts, const int32_t *counts, int32_t num_maps,
+                           int32_t edge_data_sz) {
+    if (!b || !parts || !counts || num_maps <= 0 || edge_data_sz < 4) return fail(CVL_EINVAL, "invalid batch arguments");
+    for (int m = 0; m < num_maps; ++m)
+        if (!parts[m]) return fail(CVL_EINVAL, "a map's edges are NULL");
     cvl_engine *e = b->eng;
     std::vector<int32_t> mo(num_maps + 1, 0);
     for (int m = 0; m < num_maps; ++m) {
@@ -1049,12 +1046,32 @@ int cvl_batch_refill(cvl_batch *b, const double *edges, const int32_t *counts, i
     b->sz = edge_data_sz;
     b->n = mo[num_maps];
     b->map_off = mo;
-    CVL_CUDA(cudaMemcpyAsync(b->d_edges, edges, eb, cudaMemcpyHostToDevice, e->stream));
+    // one copy per contiguous run of parts (a single copy for one concatenated buffer)
+    for (int m = 0; m < num_maps;) {
+        int k = m + 1;
+        while (k < num_maps && parts[k] == parts[k - 1] + (size_t)counts[k - 1] * edge_data_sz) ++k;
+        CVL_CUDA(copy_pieces((double *)b->d_edges + (size_t)mo[m] * edge_data_sz, parts[m],
+                             sizeof(double) * (size_t)(mo[k] - mo[m]) * edge_data_sz, cudaMemcpyHostToDevice,
+                             e->stream));
+        m = k;
+    }
     CVL_CUDA(cudaMemcpyAsync(b->d_map_off, b->map_off.data(), sizeof(int) * mo.size(), cudaMemcpyHostToDevice,
                              e->stream));
     const cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) return fail(CVL_ECUDA, std::string("batch upload: ") + cudaGetErrorString(ce));
     return CVL_OK;
+}
+
+int cvl_batch_refill(cvl_batch *b, const double *edges, const int32_t *counts, int32_t num_maps,
+                     int32_t edge_data_sz) {
+    if (!b || !edges || !counts || num_maps <= 0 || edge_data_sz < 4) return fail(CVL_EINVAL, "invalid batch arguments");
+    std::vector<const double *> parts(num_maps);
+    size_t o = 0;
+    for (int m = 0; m < num_maps; ++m) {
+        parts[m] = edges + o;
+        o += (size_t)std::max(counts[m], 0) * edge_data_sz;
+    }
+    return cvl_batch_refill_parts(b, parts.data(), counts, num_maps, edge_data_sz);
 }
 
 int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps, int32_t edge_data_sz,
@@ -1173,11 +1190,11 @@ int cvl_batch_result_take_map(cvl_batch_result *r, int32_t m, cvl_result **out) 
             std::memcpy(res->chains_p, r->chains + c0 * r->width, sizeof(unsigned) * C * r->width);
             std::memcpy(res->info_p, r->info + c0 * 10, sizeof(double) * C * 10);
         } else {
-            cudaError_t ce = cudaMemcpyAsync(res->chains_p, (const unsigned *)e->chains.p + c0 * r->width,
-                                             sizeof(unsigned) * C * r->width, cudaMemcpyDeviceToHost, e->stream);
+            cudaError_t ce = copy_pieces(res->chains_p, (const unsigned *)e->chains.p + c0 * r->width,
+                                         sizeof(unsigned) * C * r->width, cudaMemcpyDeviceToHost, e->stream);
             if (ce == cudaSuccess)
-                ce = cudaMemcpyAsync(res->info_p, (const double *)e->info.p + c0 * 10, sizeof(double) * C * 10,
-                                     cudaMemcpyDeviceToHost, e->stream);
+                ce = copy_pieces(res->info_p, (const double *)e->info.p + c0 * 10, sizeof(double) * C * 10,
+                                 cudaMemcpyDeviceToHost, e->stream);
             if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
             if (ce != cudaSuccess) {
                 delete res;

@@ -256,7 +256,18 @@ struct GrowthArgs {
     MapStats *stats;
     int count_only;
     unsigned *err;
+    const unsigned short *cell_rank;    // [CELLS_MAX] best-cell rank of each cell (k_cell_ranks)
 };
+
+// The best-cell ranks of fill_curvelet_info (:202-219), once per run.
+__global__ void k_cell_ranks(Model md, unsigned short *__restrict__ out) {
+    __shared__ double dx2[CELLS_MAX];
+    __shared__ unsigned char cj[CELLS_MAX];
+    __shared__ unsigned short rank[CELLS_MAX];
+    cell_tables_init(md, dx2, cj, rank);
+    __syncthreads();
+    for (int c = threadIdx.x; c < CELLS_MAX; c += blockDim.x) out[c] = rank[c];
+}
 
 __host__ __device__ inline size_t growth_smem_per_warp(int max_cand, int gms) {
     size_t b = (size_t)max_cand * 3 * 8;                          // per-seed results: k_max, k_min, meta
@@ -270,16 +281,12 @@ template <int CPL, int K>
 __global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
     extern __shared__ __align__(16) unsigned char gr_smem[];
     __shared__ BlockStats bstats;
-    __shared__ unsigned short cell_rank[CELLS_MAX];
-    __shared__ double cell_dx2_unused[CELLS_MAX];
-    __shared__ unsigned char cell_j_unused[CELLS_MAX];
     const Model &md = a.md;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
     block_stats_init(bstats, a.M);
-    cell_tables_init(md, cell_dx2_unused, cell_j_unused, cell_rank);
     __syncthreads();
 
     unsigned char *base = gr_smem + (size_t)wib * growth_smem_per_warp(md.max_cand, md.gms);
@@ -296,7 +303,7 @@ __global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
     for (int u = 0; u < CPL; ++u) {
         const int c = lane + 32 * u;
         on_l[u] = c < md.cells;
-        rank_l[u] = on_l[u] ? (unsigned)cell_rank[c] : 0xffffu;
+        rank_l[u] = on_l[u] ? (unsigned)a.cell_rank[c] : 0xffffu;
     }
 
     for (int i = a.a_begin + blockIdx.x * wpb + wib; i < a.a_end; i += gridDim.x * wpb) {

@@ -5,12 +5,12 @@
 // workspace on the server's device) runs a loop in its own host thread:
 //   1. Take waiting requests from one lane, in arrival order, while they fit the
 //      launch (max_batch_edges) and the admission budget.
-//   2. Concatenate them into the worker's page-locked staging buffer.
-//   3. Refill the worker's device batch; the buffer is grow-only, so there is
-//      no cudaFree and no device-wide synchronisation.
-//   4. Run the whole path over the ragged batch.
-//   5. Copy each map's rows into its own page-locked result.
-//   6. Release the budget.
+//   2. Refill the worker's device batch straight from the requests'
+//      page-locked blocks. The buffer is grow-only, so there is no cudaFree and
+//      no device-wide synchronisation.
+//   3. Run the whole path over the ragged batch.
+//   4. Copy each map's rows into its own page-locked result.
+//   5. Release the budget.
 // Workers run concurrently, so one batch's copies and kernels overlap another's.
 // Small and large maps have separate lanes, so a small map never waits behind a
 // 4K map in the same launch.
@@ -30,6 +30,7 @@
 
 #include "../../include/cvl.h"
 #include "cvl_internal.h"
+#include "cvl_pinned.h"
 
 namespace {
 
@@ -37,7 +38,7 @@ using Clock = std::chrono::steady_clock;
 
 struct Request {
     uint64_t id = 0;
-    std::vector<double> edges;
+    double *edges = nullptr;  // page-locked, from the server's arena
     int32_t n = 0, sz = 4;
     size_t charge = 0;
     int lane = 0;
@@ -59,17 +60,20 @@ struct cvl_server {
     cvl_params params{};
     std::vector<cvl_engine *> engines;
     std::vector<std::thread> threads;
+    cvl::PinnedArena host;
 
     std::mutex mu;
     std::condition_variable cv_work;  // workers: requests queued or stop
     std::condition_variable cv_done;  // waiters: a request finished
     std::deque<Request *> lanes[2];   // 0 small, 1 large
     std::unordered_map<uint64_t, Request *> reqs;
+    std::deque<uint64_t> finished;    // ids in completion order, not handed out yet
     uint64_t next_id = 1;
     size_t admitted = 0;
     bool stop = false;
 
     uint64_t submitted = 0, completed = 0, failed = 0, in_flight = 0, launches = 0, edges_completed = 0;
+    double upload_ms = 0, run_ms = 0, device_ms = 0, result_ms = 0, queue_ms = 0;
     std::vector<double> lat_ms;
     std::vector<int64_t> lat_edges;
 
@@ -94,6 +98,7 @@ struct cvl_server {
         r->res = res;
         admitted -= r->charge;
         --in_flight;
+        finished.push_back(r->id);
         if (status == CVL_OK) {
             ++completed;
             edges_completed += (uint64_t)r->n;
@@ -111,10 +116,9 @@ void cvl_server::worker(int w) {
     cudaSetDevice(cfg.device);
     cvl_engine *e = engines[w];
     cvl_batch *batch = nullptr;
-    double *staging = nullptr;  // page-locked, grow-only
-    size_t staging_cap = 0;
     std::vector<Request *> take;
     std::vector<int32_t> counts;
+    std::vector<const double *> parts;
     while (true) {
         take.clear();
         {
@@ -128,6 +132,7 @@ void cvl_server::worker(int w) {
                 if (!take.empty() && sum + r->n > cfg.max_batch_edges) break;
                 if (admitted + r->charge > cfg.mem_budget_bytes) break;
                 lanes[l].pop_front();
+                queue_ms += ms_between(r->t_submit, Clock::now());
                 admitted += r->charge;
                 ++in_flight;
                 take.push_back(r);
@@ -150,37 +155,29 @@ void cvl_server::worker(int w) {
             cv_work.notify_all();
         }
         const int32_t sz = take[0]->sz;
-        size_t total = 0;
         counts.clear();
+        parts.clear();
         for (Request *r : take) {
-            total += (size_t)r->n * sz;
             counts.push_back(r->n);
+            parts.push_back(r->edges);
         }
         int rc = CVL_OK;
         std::string err;
-        if (total * sizeof(double) > staging_cap) {
-            if (staging) cudaFreeHost(staging);
-            staging = nullptr;
-            staging_cap = std::max(total * sizeof(double), staging_cap + staging_cap / 4);
-            if (cudaMallocHost((void **)&staging, staging_cap) != cudaSuccess) {
-                cudaGetLastError();
-                staging = nullptr;
-                staging_cap = 0;
-                rc = CVL_ENOMEM;
-                err = "page-locked staging buffer could not be allocated";
-            }
-        }
         cvl_batch_result *br = nullptr;
-        if (rc == CVL_OK) {
-            size_t o = 0;
-            for (Request *r : take) {
-                std::memcpy(staging + o, r->edges.data(), sizeof(double) * (size_t)r->n * sz);
-                o += (size_t)r->n * sz;
-            }
-            rc = batch ? cvl_batch_refill(batch, staging, counts.data(), (int32_t)counts.size(), sz)
-                       : cvl_batch_upload(e, staging, counts.data(), (int32_t)counts.size(), sz, &batch);
-            if (rc == CVL_OK) rc = cvl_batch_run(e, batch, &params, &br);
-            if (rc != CVL_OK) err = cvl_last_error();
+        const Clock::time_point t0 = Clock::now();
+        if (!batch) {
+            // the first launch makes the worker's batch; later ones refill it
+            rc = cvl_batch_upload(e, parts[0], counts.data(), 1, sz, &batch);
+        }
+        if (rc == CVL_OK) rc = cvl_batch_refill_parts(batch, parts.data(), counts.data(), (int32_t)counts.size(), sz);
+        const Clock::time_point t1 = Clock::now();
+        if (rc == CVL_OK) rc = cvl_batch_run(e, batch, &params, &br);
+        if (rc != CVL_OK) err = cvl_last_error();
+        const Clock::time_point t2 = Clock::now();
+        double dev_ms = 0.0;
+        if (br) {
+            cvl_batch_stats bst;
+            if (cvl_batch_result_stats(br, &bst) == CVL_OK) dev_ms = bst.device_ms;
         }
         std::vector<cvl_result *> outs(take.size(), nullptr);
         std::vector<int> st(take.size(), rc);
@@ -192,11 +189,16 @@ void cvl_server::worker(int w) {
             }
         }
         if (br) cvl_batch_result_free(br);
+        const Clock::time_point t3 = Clock::now();
         {
             std::lock_guard<std::mutex> lk(mu);
+            upload_ms += ms_between(t0, t1);
+            run_ms += ms_between(t1, t2);
+            device_ms += dev_ms;
+            result_ms += ms_between(t2, t3);
             for (size_t m = 0; m < take.size(); ++m) {
-                take[m]->edges.clear();
-                take[m]->edges.shrink_to_fit();
+                host.put(take[m]->edges);
+                take[m]->edges = nullptr;
                 finish(take[m], st[m], errs[m], outs[m]);
             }
         }
@@ -204,7 +206,6 @@ void cvl_server::worker(int w) {
         cv_work.notify_all();  // budget freed
     }
     if (batch) cvl_batch_free(batch);
-    if (staging) cudaFreeHost(staging);
 }
 
 extern "C" {
@@ -235,6 +236,9 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
         cvl_engine_cfg ec;
         cvl_engine_cfg_default(&ec);
         ec.device = c.device;
+        // small-lane workers first on the device (the lowest number is the highest priority)
+        const bool small_lane = !(c.workers >= 2 && w == c.workers - 1);
+        ec.stream_priority = small_lane ? -1000 : 0;
         cvl_engine *e = nullptr;
         const int rc = cvl_engine_create(&ec, &e);
         if (rc != CVL_OK) {
@@ -260,7 +264,13 @@ int cvl_server_submit(cvl_server *s, const double *edges, int32_t num_edges, int
                                         " bytes of admission budget; the budget is " +
                                         std::to_string(s->cfg.mem_budget_bytes));
     Request *r = new Request();
-    r->edges.assign(edges, edges + (size_t)num_edges * edge_data_sz);
+    const size_t nval = (size_t)num_edges * edge_data_sz;
+    r->edges = (double *)s->host.get(sizeof(double) * nval);
+    if (!r->edges) {
+        delete r;
+        return cvl_fail(CVL_ENOMEM, "page-locked request buffer could not be allocated");
+    }
+    std::memcpy(r->edges, edges, sizeof(double) * nval);
     r->n = num_edges;
     r->sz = edge_data_sz;
     r->charge = charge;
@@ -268,6 +278,7 @@ int cvl_server_submit(cvl_server *s, const double *edges, int32_t num_edges, int
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) {
+            s->host.put(r->edges);
             delete r;
             return cvl_fail(CVL_EINVAL, "server is stopping");
         }
@@ -288,6 +299,8 @@ namespace {
 int hand_out(cvl_server *s, std::unordered_map<uint64_t, Request *>::iterator it, cvl_result **out) {
     Request *r = it->second;
     s->reqs.erase(it);
+    auto f = std::find(s->finished.begin(), s->finished.end(), r->id);
+    if (f != s->finished.end()) s->finished.erase(f);
     const int st = r->status;
     const std::string err = r->err;
     *out = r->res;
@@ -324,6 +337,21 @@ int cvl_server_wait(cvl_server *s, uint64_t id, int64_t timeout_us, cvl_result *
     return hand_out(s, s->reqs.find(id), out);
 }
 
+int cvl_server_next(cvl_server *s, int64_t timeout_us, uint64_t *id, cvl_result **out) {
+    if (!s || !id || !out) return cvl_fail(CVL_EINVAL, "server/id/out is NULL");
+    *out = nullptr;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto ready = [&] { return !s->finished.empty() || s->reqs.empty(); };
+    if (timeout_us < 0) {
+        s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), ready)) {
+        return cvl_fail(CVL_ETIMEDOUT, "no request finished within the timeout");
+    }
+    if (s->finished.empty()) return cvl_fail(CVL_EAGAIN, "no request is queued or running");
+    *id = s->finished.front();
+    return hand_out(s, s->reqs.find(*id), out);
+}
+
 int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out) {
     if (!s || !out) return cvl_fail(CVL_EINVAL, "server/out is NULL");
     std::vector<double> l;
@@ -338,6 +366,11 @@ int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out) {
         st.launches = s->launches;
         st.edges_completed = s->edges_completed;
         st.admitted_bytes = s->admitted;
+        st.upload_ms = s->upload_ms;
+        st.run_ms = s->run_ms;
+        st.device_ms = s->device_ms;
+        st.result_ms = s->result_ms;
+        st.queue_ms = s->queue_ms;
         l = s->lat_ms;
     }
     if (!l.empty()) {
@@ -373,6 +406,8 @@ void cvl_server_destroy(cvl_server *s) {
         s->stop = true;
         for (auto &q : s->lanes) {
             for (Request *r : q) {
+                s->host.put(r->edges);
+                r->edges = nullptr;
                 r->done = true;
                 r->status = CVL_EINVAL;
                 r->err = "server stopped before the request was admitted";

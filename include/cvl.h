@@ -71,6 +71,8 @@ typedef struct cvl_engine_cfg {
     int seeds_per_group;      /* chain-growth seeds walked together per warp: 4 or 8; 0 = auto */
     int bundle_slots;         /* bundles kept in shared memory per warp; 0 = auto */
     int warps_per_block;      /* 0 = auto */
+    int stream_priority;      /* the engine stream's priority: 0 = default, negative = higher
+                                 (clamped to cudaDeviceGetStreamPriorityRange) (0) */
 } cvl_engine_cfg;
 
 void cvl_engine_cfg_default(cvl_engine_cfg *cfg);
@@ -197,6 +199,10 @@ int cvl_batch_upload(cvl_engine *e, const double *edges, const int32_t *counts, 
  * allocation and no device-wide synchronisation. */
 int cvl_batch_refill(cvl_batch *b, const double *edges, const int32_t *counts, int32_t num_maps,
                      int32_t edge_data_sz);
+/* The same with map m's rows at parts[m] (counts[m] rows each): the maps are
+ * copied straight from where they are, with no host-side concatenation. */
+int cvl_batch_refill_parts(cvl_batch *b, const double *const *parts, const int32_t *counts, int32_t num_maps,
+                           int32_t edge_data_sz);
 void cvl_batch_free(cvl_batch *b);
 
 /* Runs the whole path over every map of a device-resident batch in one pass
@@ -240,7 +246,10 @@ void cvl_batch_result_free(cvl_batch_result *r);
  * Maps of at least large_map_edges edges go to a separate lane, so small
  * maps do not queue behind them. With two or more workers, the last worker
  * prefers the large lane and the others the small one; an idle worker takes
- * from the other lane.
+ * from the other lane. Small-lane workers run on the device's highest stream
+ * priority, so their kernels go ahead of a large map's between its blocks.
+ * A request's edges are copied at submit into page-locked memory that the
+ * server reuses, and go from there to the device.
  *
  * Admission: a request holds admit_bytes_per_edge × its edges of the budget
  * from upload to result. A request that can never fit is refused at submit
@@ -265,6 +274,12 @@ typedef struct cvl_server_stats {
     size_t admitted_bytes;         /* budget held right now */
     double p50_ms, p95_ms, p99_ms; /* submit -> result ready, over completed requests */
     double max_ms;
+    /* where the workers' time went, summed over launches (ms of host wall time) */
+    double upload_ms;              /* requests' edges to the device */
+    double run_ms;                 /* cvl_batch_run */
+    double device_ms;              /* of which the device time of the runs (CUDA events) */
+    double result_ms;              /* each map's rows to its page-locked result */
+    double queue_ms;               /* summed over requests: submit -> taken by a worker */
 } cvl_server_stats;
 
 void cvl_server_cfg_default(cvl_server_cfg *cfg);
@@ -278,6 +293,11 @@ int cvl_server_poll(cvl_server *s, uint64_t id, cvl_result **out);
 /* As poll, waiting up to timeout_us microseconds (< 0: no limit); CVL_ETIMEDOUT
  * if the result is not ready by then (the request stays queued). */
 int cvl_server_wait(cvl_server *s, uint64_t id, int64_t timeout_us, cvl_result **out);
+/* The earliest finished request whose result was not handed out yet, in
+ * completion order: *id names it and *out is its result. Waits up to
+ * timeout_us (< 0: no limit); CVL_ETIMEDOUT if none finished by then, CVL_EAGAIN
+ * at once if no request is queued or running. */
+int cvl_server_next(cvl_server *s, int64_t timeout_us, uint64_t *id, cvl_result **out);
 int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out);
 /* Latency (ms, submit -> result ready) and edge count of each completed
  * request, in completion order; returns how many were written (<= cap). */

@@ -98,6 +98,9 @@ def test_server_defaults_and_argument_checks():
     lib.cvl_server_cfg_default(C.byref(cfg))
     assert (cfg.device, cfg.workers, cfg.mem_budget_bytes) == (0, 2, 40 << 30)
     assert (cfg.admit_bytes_per_edge, cfg.max_batch_edges, cfg.large_map_edges) == (2048, 4 << 20, 1_000_000)
+    ec = _abi.CvlEngineCfg()
+    lib.cvl_engine_cfg_default(C.byref(ec))
+    assert ec.stream_priority == 0
     h = C.c_void_p()
     p = cvl.CurveletParams().to_c()
     assert lib.cvl_server_create(C.byref(cfg), None, C.byref(h)) == _abi.CVL_EINVAL

@@ -92,3 +92,17 @@ def test_server_admission_budget(engine):
         _same(engine.run(m), g)
     assert st["completed"] == 6 and st["launches"] == 6 and st["admitted_bytes"] == 0
     assert len(ms) == 6 and sorted(ed.tolist()) == sorted(m.shape[0] for m in maps)
+
+
+def test_server_next_hands_out_in_completion_order(engine):
+    maps = [synth.plain_small(s) for s in range(5)]
+    with cvl.Server(workers=2) as srv:
+        ids = [srv.submit(m) for m in maps]
+        seen = {}
+        for _ in maps:
+            rid, res = srv.next(timeout_s=120.0)
+            seen[rid] = res
+        assert srv.next(timeout_s=1.0) is None  # nothing queued or running
+    assert sorted(seen) == sorted(ids)
+    for rid, m in zip(ids, maps):
+        _same(engine.run(m), seen[rid])
