@@ -259,7 +259,7 @@ def run_reference(args, maps, cfg, world, rank):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": dict(workload=args.workload, edges=tot, maps=len(sample),
+            "config": dict(workload=args.workload, sample_edges=tot, sample_maps=len(sample),
                            **{k: v for k, v in cfg.items() if not k.startswith("_")}),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
                              "sample": f"{len(sample)} of {len(maps)} map(s), {tot} edges per step"},
