@@ -56,6 +56,7 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-map-per-launch comparison")
     ap.add_argument("--rate", type=float, default=50.0, help="served stream: offered maps/s")
     ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")
     ap.add_argument("--requests", type=int, default=600, help="served stream: requests per rate")
@@ -400,7 +401,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     last.close()
 
     plain = None
-    if len(maps) > 1:
+    if len(maps) > 1 and not args.no_plain:
         _progress("plain form (one map per launch)")
         pms = _plain_device_ms(eng, maps, max(1, min(args.steps, 3)))
         pms = _max_over_ranks(pg, pms)

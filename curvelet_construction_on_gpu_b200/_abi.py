@@ -72,6 +72,13 @@ class CvlServerStats(C.Structure):
                 ("result_ms", C.c_double), ("queue_ms", C.c_double)]
 
 
+class CvlTuning(C.Structure):
+    _fields_ = [("cell_size", C.c_int), ("bundle_blocks_per_sm", C.c_int), ("growth_blocks_per_sm", C.c_int),
+                ("seeds_per_group", C.c_int), ("anchors_per_warp", C.c_int), ("chunk_pairs", C.c_int64)]
+
+
+CVL_TUNING_BUCKETS = 4
+
 # (name, restype, argtypes) of every entry point declared in include/cvl.h
 _vp = C.c_void_p
 _dp = C.POINTER(C.c_double)
@@ -113,6 +120,10 @@ SIGNATURES = [
     ("cvl_server_stats_get", C.c_int, [_vp, C.POINTER(CvlServerStats)]),
     ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.c_int64]),
     ("cvl_server_destroy", None, [_vp]),
+    ("cvl_tuning_bucket", C.c_int, [C.c_int64]),
+    ("cvl_engine_get_tuning", C.c_int, [_vp, C.c_int, C.POINTER(CvlTuning)]),
+    ("cvl_engine_set_tuning", C.c_int, [_vp, C.c_int, C.POINTER(CvlTuning)]),
+    ("cvl_engine_autotune", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.c_int, C.POINTER(CvlTuning), _dp]),
     ("cvl_engine_flush_l2", C.c_int, [_vp]),
     ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),
     ("cvl_engine_last_launch_count", C.c_int, [_vp]),

@@ -266,6 +266,28 @@ class Engine:
         check(self._lib.cvl_batch_run(self._h, batch._h, C.byref(p), C.byref(r)), "cvl_batch_run")
         return BatchResult(self, r, len(batch.counts))
 
+    # ---- tuning (every tuning gives the same results; only the time changes)
+    def get_tuning(self, bucket: int) -> dict:
+        t = _abi.CvlTuning()
+        check(self._lib.cvl_engine_get_tuning(self._h, bucket, C.byref(t)), "cvl_engine_get_tuning")
+        return {name: getattr(t, name) for name, _ in t._fields_}
+
+    def set_tuning(self, bucket: int, **knobs) -> None:
+        """Sets knobs of one bucket (-1: every bucket); unnamed knobs keep their values."""
+        cur = self.get_tuning(max(bucket, 0))
+        cur.update(knobs)
+        t = _abi.CvlTuning(**cur)
+        check(self._lib.cvl_engine_set_tuning(self._h, bucket, C.byref(t)), "cvl_engine_set_tuning")
+
+    def autotune(self, batch: "Batch", params: CurveletParams | None = None, passes: int = 1) -> tuple[dict, float]:
+        """Coordinate descent over the batch's bucket; installs and returns (tuning, device ms)."""
+        p = (params or CurveletParams()).to_c()
+        t = _abi.CvlTuning()
+        ms = C.c_double(0.0)
+        check(self._lib.cvl_engine_autotune(self._h, batch._h, C.byref(p), passes, C.byref(t), C.byref(ms)),
+              "cvl_engine_autotune")
+        return {name: getattr(t, name) for name, _ in t._fields_}, float(ms.value)
+
     # ---- measurement helpers
     def flush_l2(self) -> None:
         check(self._lib.cvl_engine_flush_l2(self._h), "cvl_engine_flush_l2")

@@ -90,7 +90,7 @@ struct cvl_engine {
     DBuf ncand, deg, pair_off, csr_ids, csr_d2, rec_ids, rec_k, rec_meta, count, out_off;
     DBuf chains, info, stats, err, work, scratch, scratch_chain, scratch_res, scan_tmp, flush, deg_orig, off_orig,
         gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start, crank;
-    unsigned long long chunk_pairs = CHUNK_PAIRS_DEFAULT;  // pairs per bundle chunk
+    cvl_tuning tune[CVL_TUNING_BUCKETS];                   // per size bucket of the batch
     std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
     DBuf pairs_in, pb_min, pb_max, pb_valid;
@@ -238,6 +238,39 @@ struct cvl_batch_result {
 
 namespace {
 
+// ---- tuning -------------------------------------------------------------------
+int bucket_of(long long n) {
+    if (n <= (64LL << 10)) return 0;
+    if (n <= (512LL << 10)) return 1;
+    if (n <= (4LL << 20)) return 2;
+    return 3;
+}
+
+cvl_tuning default_tuning(int cell_size, int seeds_per_group) {
+    cvl_tuning t;
+    t.cell_size = cell_size;
+    t.bundle_blocks_per_sm = 4;
+    t.growth_blocks_per_sm = 4;
+    t.seeds_per_group = seeds_per_group;
+    t.anchors_per_warp = 4;
+    t.chunk_pairs = (int64_t)CHUNK_PAIRS_DEFAULT;
+    return t;
+}
+
+int check_tuning(const cvl_tuning &t) {
+    if (t.cell_size != 2 && t.cell_size != 4 && t.cell_size != 8)
+        return fail(CVL_EINVAL, "tuning: cell_size must be 2, 4 or 8");
+    if (t.bundle_blocks_per_sm != 3 && t.bundle_blocks_per_sm != 4)
+        return fail(CVL_EINVAL, "tuning: bundle_blocks_per_sm must be 3 or 4");
+    if (t.growth_blocks_per_sm != 4 && t.growth_blocks_per_sm != 6)
+        return fail(CVL_EINVAL, "tuning: growth_blocks_per_sm must be 4 or 6");
+    if (t.seeds_per_group != 4 && t.seeds_per_group != 8) return fail(CVL_EINVAL, "tuning: seeds_per_group must be 4 or 8");
+    if (t.anchors_per_warp < 1 || t.anchors_per_warp > 32) return fail(CVL_EINVAL, "tuning: anchors_per_warp in [1, 32]");
+    if (t.chunk_pairs < (1 << 16) || t.chunk_pairs > (1LL << 30))
+        return fail(CVL_EINVAL, "tuning: chunk_pairs in [65536, 2^30]");
+    return CVL_OK;
+}
+
 // ---- parameters -> model ---------------------------------------------------
 int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nbr_radius, unsigned max_cand, Model &md,
                int &cpl) {
@@ -376,37 +409,56 @@ struct RunOut {
     unsigned max_deg = 0;
 };
 
-template <int CPL>
+template <int CPL, int MINB>
 int launch_bundles(cvl_engine *e, BundleArgs &a, int blocks) {
     // one block per PPB pairs and no grid stride: short blocks, so that a
     // higher-priority stream's blocks get SMs as soon as any block ends
     const long long ppb = BUNDLE_THREADS / a.md.Q;
     const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
     blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
-    k_bundles<CPL><<<blocks, BUNDLE_THREADS, 0, e->stream>>>(a);
+    k_bundles<CPL, MINB><<<blocks, BUNDLE_THREADS, 0, e->stream>>>(a);
     return check_launch("k_bundles");
 }
 
-template <int CPL, int K>
+template <int CPL, int K, int MINB>
 int launch_growth(cvl_engine *e, GrowthArgs &a, size_t smem, int blocks) {
-    CVL_CUDA(cudaFuncSetAttribute(k_growth<CPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CVL_CUDA(cudaFuncSetAttribute(k_growth<CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // a warp per anchor, 4 anchors per warp: short blocks (a higher-priority
     // stream's blocks get SMs as soon as any block ends) with the per-block
     // set-up spread over 16 anchors
-    blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + 15) / 16, 0x7fffffffLL));
-    k_growth<CPL, K><<<blocks, 128, smem, e->stream>>>(a);
+    const long long per_block = 4LL * a.anchors_per_warp;
+    blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + per_block - 1) / per_block,
+                                                    0x7fffffffLL));
+    k_growth<CPL, K, MINB><<<blocks, 128, smem, e->stream>>>(a);
     return check_launch("k_growth");
 }
 
 typedef int (*bundles_fn)(cvl_engine *, BundleArgs &, int);
 typedef int (*growth_fn)(cvl_engine *, GrowthArgs &, size_t, int);
 
-void pick_kernels(int cpl, bundles_fn &bf, growth_fn &gf) {
+// The kernel variants a tuning selects (seeds_per_group 8 only for grids of up to
+// 64 cells, where its register footprint fits).
+void pick_kernels(int cpl, const cvl_tuning &t, bundles_fn &bf, growth_fn &gf) {
+    const bool b3 = t.bundle_blocks_per_sm == 3;
+    const bool g6 = t.growth_blocks_per_sm == 6;
+    const bool k8 = t.seeds_per_group == 8 && cpl <= 2;
     switch (cpl) {
-        case 1: bf = launch_bundles<1>; gf = launch_growth<1, 4>; break;
-        case 3: bf = launch_bundles<3>; gf = launch_growth<3, 4>; break;
-        case 4: bf = launch_bundles<4>; gf = launch_growth<4, 4>; break;
-        default: bf = launch_bundles<2>; gf = launch_growth<2, 4>; break;
+        case 1:
+            bf = b3 ? launch_bundles<1, 3> : launch_bundles<1, 4>;
+            gf = k8 ? launch_growth<1, 8, 4> : (g6 ? launch_growth<1, 4, 6> : launch_growth<1, 4, 4>);
+            break;
+        case 3:
+            bf = b3 ? launch_bundles<3, 3> : launch_bundles<3, 4>;
+            gf = g6 ? launch_growth<3, 4, 6> : launch_growth<3, 4, 4>;
+            break;
+        case 4:
+            bf = b3 ? launch_bundles<4, 3> : launch_bundles<4, 4>;
+            gf = g6 ? launch_growth<4, 4, 6> : launch_growth<4, 4, 4>;
+            break;
+        default:
+            bf = b3 ? launch_bundles<2, 3> : launch_bundles<2, 4>;
+            gf = k8 ? launch_growth<2, 8, 4> : (g6 ? launch_growth<2, 4, 6> : launch_growth<2, 4, 4>);
+            break;
     }
 }
 
@@ -420,6 +472,8 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     g_launches = 0;
     e->mark("start");
 
+    const cvl_tuning &tn = e->tune[bucket_of(n)];
+    md.sbits = tn.cell_size == 2 ? 1 : (tn.cell_size == 8 ? 3 : 2);
     const unsigned T = next_pow2(std::max<unsigned long long>((unsigned long long)n, 1024ull));
     md.hash_mask = T - 1;
 
@@ -505,7 +559,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->deg.p, n,
                                                 (unsigned long long *)e->pair_off.p)));
     // chunk boundaries over anchors: a chunk holds at most CHUNK_PAIRS + max_deg pairs
-    const unsigned long long per_chunk = std::max<unsigned long long>(e->chunk_pairs, 1024ull);
+    const unsigned long long per_chunk = std::max<unsigned long long>((unsigned long long)tn.chunk_pairs, 1024ull);
     const int max_chunks = 4096;
     CVL_TRY(e->alloc(e->chunk_start, sizeof(int) * (max_chunks + 1)));
     CVL_CUDA(cudaMemsetAsync(e->chunk_start.p, 0, sizeof(int) * (max_chunks + 1), s));
@@ -561,7 +615,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     // ---- (c) + (d) per chunk
     bundles_fn bf;
     growth_fn gf;
-    pick_kernels(cpl, bf, gf);
+    pick_kernels(cpl, tn, bf, gf);
     const size_t gsmem = (size_t)4 * growth_smem_per_warp(md.max_cand, md.gms);
     int gbps = 0;
     {
@@ -634,6 +688,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
             ga.count_only = (mode == 1) ? 1 : 0;
             ga.err = err;
             ga.cell_rank = (const unsigned short *)e->crank.p;
+            ga.anchors_per_warp = tn.anchors_per_warp;
             CVL_TRY(gf(e, ga, gsmem, gblocks));
             e->mark("growth");
         }
@@ -783,6 +838,10 @@ int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out) {
     e->budget = c.mem_budget_bytes;
     e->cell_size = c.cell_size > 0 ? c.cell_size : 4;
     e->seeds_per_group = (c.seeds_per_group == 8) ? 8 : 4;
+    {
+        const int cs = (e->cell_size == 2 || e->cell_size == 8) ? e->cell_size : 4;
+        for (cvl_tuning &t : e->tune) t = default_tuning(cs, e->seeds_per_group);
+    }
     e->slots = c.bundle_slots > 0 ? c.bundle_slots : 10;
     cudaError_t ce = cudaSetDevice(e->device);
     if (ce == cudaSuccess) ce = cudaGetDeviceProperties(&e->prop, e->device);
@@ -1237,6 +1296,94 @@ int cvl_batch_result_stats(const cvl_batch_result *r, cvl_batch_stats *out) {
 }
 
 void cvl_batch_result_free(cvl_batch_result *r) { delete r; }
+
+int cvl_tuning_bucket(int64_t num_edges) { return bucket_of((long long)num_edges); }
+
+int cvl_engine_get_tuning(cvl_engine *e, int bucket, cvl_tuning *t) {
+    if (!e || !t || bucket < 0 || bucket >= CVL_TUNING_BUCKETS) return fail(CVL_EINVAL, "invalid tuning arguments");
+    *t = e->tune[bucket];
+    return CVL_OK;
+}
+
+int cvl_engine_set_tuning(cvl_engine *e, int bucket, const cvl_tuning *t) {
+    if (!e || !t || bucket < -1 || bucket >= CVL_TUNING_BUCKETS) return fail(CVL_EINVAL, "invalid tuning arguments");
+    CVL_TRY(check_tuning(*t));
+    if (bucket < 0) {
+        for (cvl_tuning &x : e->tune) x = *t;
+    } else {
+        e->tune[bucket] = *t;
+    }
+    return CVL_OK;
+}
+
+int cvl_engine_autotune(cvl_engine *e, const cvl_batch *b, const cvl_params *p, int passes, cvl_tuning *best,
+                        double *best_ms) {
+    if (!e || !b || !p || !best || !best_ms || passes < 1) return fail(CVL_EINVAL, "invalid autotune arguments");
+    const int bucket = bucket_of(b->n);
+    // one untimed run (workspace growth), then the median of three device times
+    auto time_it = [&](const cvl_tuning &t, double &ms) -> int {
+        e->tune[bucket] = t;
+        double v[4];
+        for (int k = 0; k < 4; ++k) {
+            cvl_batch_result *r = nullptr;
+            CVL_TRY(cvl_batch_run(e, b, p, &r));
+            v[k] = r->device_ms;
+            cvl_batch_result_free(r);
+        }
+        std::sort(v + 1, v + 4);
+        ms = v[2];
+        return CVL_OK;
+    };
+    cvl_tuning cur = e->tune[bucket];
+    double cur_ms = 0.0;
+    CVL_TRY(time_it(cur, cur_ms));
+    const int64_t chunks[] = {1LL << 20, 4LL << 20, 16LL << 20};
+    const int apws[] = {1, 2, 4, 8, 16};
+    const int cells[] = {2, 4, 8};
+    const int growth[][2] = {{4, 4}, {4, 6}, {8, 4}};  // (seeds_per_group, blocks per SM)
+    for (int pass = 0; pass < passes; ++pass) {
+        auto consider = [&](const cvl_tuning &t) -> int {
+            if (std::memcmp(&t, &cur, sizeof(t)) == 0) return CVL_OK;
+            double ms = 0.0;
+            CVL_TRY(time_it(t, ms));
+            if (ms < cur_ms * 0.99) {
+                cur = t;
+                cur_ms = ms;
+            }
+            return CVL_OK;
+        };
+        for (int v : {3, 4}) {
+            cvl_tuning t = cur;
+            t.bundle_blocks_per_sm = v;
+            CVL_TRY(consider(t));
+        }
+        for (const auto &g : growth) {
+            cvl_tuning t = cur;
+            t.seeds_per_group = g[0];
+            t.growth_blocks_per_sm = g[1];
+            CVL_TRY(consider(t));
+        }
+        for (int v : apws) {
+            cvl_tuning t = cur;
+            t.anchors_per_warp = v;
+            CVL_TRY(consider(t));
+        }
+        for (int v : cells) {
+            cvl_tuning t = cur;
+            t.cell_size = v;
+            CVL_TRY(consider(t));
+        }
+        for (int64_t v : chunks) {
+            cvl_tuning t = cur;
+            t.chunk_pairs = v;
+            CVL_TRY(consider(t));
+        }
+    }
+    e->tune[bucket] = cur;
+    *best = cur;
+    *best_ms = cur_ms;
+    return CVL_OK;
+}
 
 int cvl_engine_flush_l2(cvl_engine *e) {
     if (!e) return fail(CVL_EINVAL, "engine is NULL");

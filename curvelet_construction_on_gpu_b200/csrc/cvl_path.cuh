@@ -146,8 +146,9 @@ struct BundleArgs {
 
 constexpr int BUNDLE_THREADS = 256;
 
-template <int CPL>
-__global__ void __launch_bounds__(BUNDLE_THREADS, 4) k_bundles(BundleArgs a) {
+// MINB: the resident blocks per SM the register allocation is capped for (3 or 4)
+template <int CPL, int MINB>
+__global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgs a) {
     const Model &md = a.md;
     __shared__ double s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
     __shared__ unsigned char s_open[2][BUNDLE_THREADS];
@@ -257,6 +258,7 @@ struct GrowthArgs {
     int count_only;
     unsigned *err;
     const unsigned short *cell_rank;    // [CELLS_MAX] best-cell rank of each cell (k_cell_ranks)
+    int anchors_per_warp;               // the grid is ceil((a_end - a_begin) / (warps per block * this))
 };
 
 // The best-cell ranks of fill_curvelet_info (:202-219), once per run.
@@ -277,17 +279,16 @@ __host__ __device__ inline size_t growth_smem_per_warp(int max_cand, int gms) {
     return (b + 15) & ~(size_t)15;
 }
 
-template <int CPL, int K>
-__global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
+// K: seeds walked together; MINB: the resident blocks per SM the register
+// allocation is capped for
+template <int CPL, int K, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_growth(GrowthArgs a) {
     extern __shared__ __align__(16) unsigned char gr_smem[];
-    __shared__ BlockStats bstats;
     const Model &md = a.md;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
-    block_stats_init(bstats, a.M);
-    __syncthreads();
 
     unsigned char *base = gr_smem + (size_t)wib * growth_smem_per_warp(md.max_cand, md.gms);
     double *res = (double *)base;                                      // [max_cand][3]
@@ -306,7 +307,13 @@ __global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
         rank_l[u] = on_l[u] ? (unsigned)a.cell_rank[c] : 0xffffu;
     }
 
-    for (int i = a.a_begin + blockIdx.x * wpb + wib; i < a.a_end; i += gridDim.x * wpb) {
+    int acc_map = -1;
+    unsigned acc_valid = 0u, acc_close = 0u;
+    // each warp takes a contiguous run of anchors_per_warp anchors (the grid covers the chunk)
+    const long long w0 = ((long long)blockIdx.x * wpb + wib) * a.anchors_per_warp + a.a_begin;
+    const long long w1 = w0 + a.anchors_per_warp;
+    const int i_end = (int)(w1 < (long long)a.a_end ? w1 : (long long)a.a_end);
+    for (int i = (int)(w0 < (long long)a.a_end ? w0 : (long long)a.a_end); i < i_end; ++i) {
         const int m = a.B.map[i];
         const int orig = a.B.orig[i];
         const unsigned long long off = a.pair_off[i];
@@ -539,14 +546,24 @@ __global__ void __launch_bounds__(128) k_growth(GrowthArgs a) {
             n_out += n_fit;
             __syncwarp();
         }
-        if (lane == 0) {
-            if (!a.count_only) a.count[orig] = n_out;
-            stats_add(bstats, a.stats, a.M, m, 0u, 0u, 0u, valid_cnt, close_cnt);
+        if (lane == 0 && !a.count_only) a.count[orig] = n_out;
+        // the warp's map counts, flushed when the map changes (one atomic pair per map run)
+        if (m != acc_map) {
+            if (lane == 0 && acc_map >= 0 && (acc_valid | acc_close)) {
+                atomicAdd(&a.stats[acc_map].valid_pairs, acc_valid);
+                atomicAdd(&a.stats[acc_map].close_pairs, acc_close);
+            }
+            acc_map = m;
+            acc_valid = acc_close = 0u;
         }
+        acc_valid += valid_cnt;
+        acc_close += close_cnt;
         __syncwarp();
     }
-    __syncthreads();
-    block_stats_flush(bstats, a.stats, a.M);
+    if (lane == 0 && acc_map >= 0 && (acc_valid | acc_close)) {
+        atomicAdd(&a.stats[acc_map].valid_pairs, acc_valid);
+        atomicAdd(&a.stats[acc_map].close_pairs, acc_close);
+    }
 }
 
 // (e) finalize: records -> chain rows + info rows at anchor-major positions

@@ -67,10 +67,10 @@ typedef struct cvl_engine cvl_engine;
 typedef struct cvl_engine_cfg {
     int device;               /* CUDA device ordinal (0) */
     size_t mem_budget_bytes;  /* device memory the engine may hold; 0 = no limit */
-    int cell_size;            /* spatial-hash cell edge in pixel cells; 0 = auto (4) */
-    int seeds_per_group;      /* chain-growth seeds walked together per warp: 4 or 8; 0 = auto */
-    int bundle_slots;         /* bundles kept in shared memory per warp; 0 = auto */
-    int warps_per_block;      /* 0 = auto */
+    int cell_size;            /* initial spatial-hash block edge of every tuning bucket: 2, 4 or 8; 0 = 4 */
+    int seeds_per_group;      /* initial seeds per group of every tuning bucket: 4 or 8; 0 = 4 */
+    int bundle_slots;         /* reserved, unused (0) */
+    int warps_per_block;      /* reserved, unused (0) */
     int stream_priority;      /* the engine stream's priority: 0 = default, negative = higher
                                  (clamped to cudaDeviceGetStreamPriorityRange) (0) */
 } cvl_engine_cfg;
@@ -305,6 +305,33 @@ int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, int64_t 
 /* Finishes the requests already admitted, drops the queued ones, stops the
  * workers and releases everything. */
 void cvl_server_destroy(cvl_server *s);
+
+/* ---- tuning and the autotuner -------------------------------------------
+ * No reference counterpart. An engine keeps one tuning per size bucket of the
+ * batch (its total edges); every tuning gives the same results bit for bit,
+ * only the time changes. cvl_engine_autotune searches them on a
+ * device-resident batch by timing the whole path, and installs the best. */
+#define CVL_TUNING_BUCKETS 4          /* batches of <= 64 Ki, <= 512 Ki, <= 4 Mi, and more edges */
+typedef struct cvl_tuning {
+    int cell_size;                    /* spatial-hash block edge in pixel cells: 2, 4 or 8 (4) */
+    int bundle_blocks_per_sm;         /* bundle kernel's register budget: 3 or 4 resident blocks per SM (4) */
+    int growth_blocks_per_sm;         /* growth kernel's register budget: 4 or 6 resident blocks per SM (4) */
+    int seeds_per_group;              /* chain-growth seeds walked together per warp: 4 or 8 (4) */
+    int anchors_per_warp;             /* chain-growth anchors per warp: 1..32 (4) */
+    int64_t chunk_pairs;              /* neighbour pairs whose bundles are held in HBM at once (4 Mi) */
+} cvl_tuning;
+/* The bucket a batch of num_edges edges uses. */
+int cvl_tuning_bucket(int64_t num_edges);
+int cvl_engine_get_tuning(cvl_engine *e, int bucket, cvl_tuning *t);
+/* bucket -1 sets every bucket. CVL_EINVAL for values outside the ranges above. */
+int cvl_engine_set_tuning(cvl_engine *e, int bucket, const cvl_tuning *t);
+/* Coordinate descent over the tuning of the batch's bucket. It runs `passes`
+ * sweeps over the knobs, each candidate timed as the median of 3 runs of the
+ * whole path (device time), and keeps a change only when it is faster by more
+ * than 1%. The best tuning is installed for that bucket and written to *best,
+ * and its time to *best_ms. The batch's results are not kept. */
+int cvl_engine_autotune(cvl_engine *e, const cvl_batch *b, const cvl_params *p, int passes, cvl_tuning *best,
+                        double *best_ms);
 
 /* Writes a buffer larger than the L2 cache on the engine's stream and waits
  * (timing hygiene between benchmark iterations). */

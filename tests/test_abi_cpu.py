@@ -118,3 +118,12 @@ def test_server_without_gpu_fails_loudly():
     with pytest.raises(cvl.CvlError) as ei:
         cvl.Server()
     assert ei.value.code == _abi.CVL_ENODEV
+
+
+def test_tuning_buckets():
+    lib = _abi.load()
+    assert [lib.cvl_tuning_bucket(n) for n in (1, 64 << 10, (64 << 10) + 1, 512 << 10, (512 << 10) + 1,
+                                                 4 << 20, (4 << 20) + 1, 1 << 30)] == [0, 0, 1, 1, 2, 2, 3, 3]
+    t = _abi.CvlTuning()
+    assert lib.cvl_engine_set_tuning(None, 0, C.byref(t)) == _abi.CVL_EINVAL
+    assert lib.cvl_engine_get_tuning(None, 0, C.byref(t)) == _abi.CVL_EINVAL
