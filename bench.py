@@ -44,6 +44,12 @@ sys.path.insert(0, ROOT)
 METRIC = "edges/s"
 # per computed (non-close) pair: 63 cells x 20 FP64 flops, divisions counted as 1
 FLOPS_PER_PAIR_CELL = 20
+# DRAM bytes of k_bundles per computed pair, from one ncu capture of the kernel on
+# the 242k-edge 1920x1080 map: dram__bytes_read.sum 0.338025 GB + dram__bytes_write.sum
+# 2.194154 GB over 2,176,780 non-close pairs (profiles/kernels_plain_hd.md). The
+# traffic is the bundle write (1,008 B per pair) plus the pair/anchor reads, so it
+# scales with the pairs a launch processes.
+BUNDLE_DRAM_BYTES_PER_PAIR = (0.338025e9 + 2.194154e9) / 2_176_780
 
 
 def _args():
@@ -181,21 +187,13 @@ def _dist_init(args):
 
 
 def _max_over_ranks(pg, v: float) -> float:
-    if pg is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    from curvelet_construction_on_gpu_b200.replicas import reduce_max
+    return reduce_max(pg, v)
 
 
 def _sum_over_ranks(pg, v: float) -> float:
-    if pg is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+    from curvelet_construction_on_gpu_b200.replicas import reduce_sum
+    return reduce_sum(pg, v)
 
 
 def _barrier(pg):
@@ -380,7 +378,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
         r.close()
     _barrier(pg)
     _progress("timed steps")
-    step_ms, kern, launches = [], [], 0
+    step_ms, kern, launches, bundle_launches = [], [], 0, 1
     with _Clocks(local) as clk:
         for _ in range(args.steps):
             eng.flush_l2()
@@ -388,7 +386,9 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
             st = r.stats()
             step_ms.append(st["device_ms"])
             launches = int(st["launches"])
-            kern.append(_stage_sums(eng.kernel_times()))
+            kt = eng.kernel_times()
+            bundle_launches = sum(1 for name, _ in kt if name == "bundles")
+            kern.append(_stage_sums(kt))
             r.close()
     _barrier(pg)
     sum_ms = _max_over_ranks(pg, float(np.sum(step_ms)))
@@ -462,6 +462,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     curv_ms = float(np.mean([k.get("bundles", 0.0) for k in kern]))
     flops = FLOPS_PER_PAIR_CELL * 63 * nonclose
     achieved = flops / (curv_ms / 1e3) / 1e12 if curv_ms > 0 else 0.0
+    launches_b = max(1, int(bundle_launches))
     clocks = clk.summary()
     stage_ms = {k: float(np.mean([d.get(k, 0.0) for d in kern])) for k in kern[0]} if kern else {}
     line = {
@@ -476,8 +477,13 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
         "roofline": {"bound": "fp64", "kernel": "k_bundles", "achieved": achieved, "peak": fp64_peak,
                      "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if fp64_peak else None,
                      "peak_source": "measured DFMA loop (cvl_measure_fp64_peak), 2 flops per FMA",
-                     "work": f"{FLOPS_PER_PAIR_CELL} flops x 63 cells x {nonclose} non-close pairs",
-                     "traffic": None},
+                     "work": f"{FLOPS_PER_PAIR_CELL} flops x 63 cells x {nonclose} non-close pairs, "
+                             f"{launches_b} launch(es) per step",
+                     "traffic": BUNDLE_DRAM_BYTES_PER_PAIR * nonclose / launches_b,
+                     "traffic_unit": "bytes per launch",
+                     "traffic_source": "ncu dram bytes of k_bundles on the 242k-edge map, per non-close pair, "
+                                       "times this workload's pairs per launch",
+                     "algorithmic_bytes": 1008.0 * nonclose / launches_b},
         "gpu_launches": launches,
         "clocks": clocks,
         "e2e": e2e,

@@ -252,7 +252,7 @@ cvl_tuning default_tuning(int cell_size, int seeds_per_group) {
     t.bundle_blocks_per_sm = 4;
     t.growth_blocks_per_sm = 4;
     t.seeds_per_group = seeds_per_group;
-    t.anchors_per_warp = 4;
+    t.anchors_per_warp = 2;
     t.chunk_pairs = (int64_t)CHUNK_PAIRS_DEFAULT;
     return t;
 }
@@ -839,8 +839,13 @@ int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out) {
     e->cell_size = c.cell_size > 0 ? c.cell_size : 4;
     e->seeds_per_group = (c.seeds_per_group == 8) ? 8 : 4;
     {
-        const int cs = (e->cell_size == 2 || e->cell_size == 8) ? e->cell_size : 4;
-        for (cvl_tuning &t : e->tune) t = default_tuning(cs, e->seeds_per_group);
+        // measured on B200: 4-pixel blocks for batches up to 512 Ki edges, 8-pixel
+        // blocks above (the spatial hash then touches fewer buckets per window)
+        for (int b = 0; b < CVL_TUNING_BUCKETS; ++b) {
+            const int dflt = b >= 2 ? 8 : 4;
+            const int cs = (c.cell_size == 2 || c.cell_size == 4 || c.cell_size == 8) ? c.cell_size : dflt;
+            e->tune[b] = default_tuning(cs, e->seeds_per_group);
+        }
     }
     e->slots = c.bundle_slots > 0 ? c.bundle_slots : 10;
     cudaError_t ce = cudaSetDevice(e->device);

@@ -353,9 +353,9 @@ __global__ void __launch_bounds__(128, MINB) k_growth(GrowthArgs a) {
             unsigned n_acc = 0;  // curvelets of this run
             unsigned n_fit = 0;  // of those, written to the arena (all, unless it ran out)
             unsigned long long run_base = 0;
-            // With group_max_sz <= 2 a chain stops at length 2 and the len > 2 gate
-            // (:549) never passes.
-            if (!a.count_only && ns > 0 && md.gms > 2) {
+            // A curvelet needs the anchor and at least two more edges (len > 2, :549):
+            // a run with fewer than two seeds, or group_max_sz <= 2, grows none.
+            if (!a.count_only && ns > 1 && md.gms > 2) {
                 auto load_bundle = [&](int s, double *mn, double *mx) {
                     const unsigned sq = seed_q[s];
                     if (sq & CLOSE_BIT) {

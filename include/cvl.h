@@ -67,7 +67,8 @@ typedef struct cvl_engine cvl_engine;
 typedef struct cvl_engine_cfg {
     int device;               /* CUDA device ordinal (0) */
     size_t mem_budget_bytes;  /* device memory the engine may hold; 0 = no limit */
-    int cell_size;            /* initial spatial-hash block edge of every tuning bucket: 2, 4 or 8; 0 = 4 */
+    int cell_size;            /* initial spatial-hash block edge of every tuning bucket: 2, 4 or 8;
+                                 0 = 4 up to 512 Ki edges and 8 above */
     int seeds_per_group;      /* initial seeds per group of every tuning bucket: 4 or 8; 0 = 4 */
     int bundle_slots;         /* reserved, unused (0) */
     int warps_per_block;      /* reserved, unused (0) */
@@ -313,11 +314,11 @@ void cvl_server_destroy(cvl_server *s);
  * device-resident batch by timing the whole path, and installs the best. */
 #define CVL_TUNING_BUCKETS 4          /* batches of <= 64 Ki, <= 512 Ki, <= 4 Mi, and more edges */
 typedef struct cvl_tuning {
-    int cell_size;                    /* spatial-hash block edge in pixel cells: 2, 4 or 8 (4) */
+    int cell_size;                    /* spatial-hash block edge in pixel cells: 2, 4 or 8 (4; 8 above 512 Ki edges) */
     int bundle_blocks_per_sm;         /* bundle kernel's register budget: 3 or 4 resident blocks per SM (4) */
     int growth_blocks_per_sm;         /* growth kernel's register budget: 4 or 6 resident blocks per SM (4) */
     int seeds_per_group;              /* chain-growth seeds walked together per warp: 4 or 8 (4) */
-    int anchors_per_warp;             /* chain-growth anchors per warp: 1..32 (4) */
+    int anchors_per_warp;             /* chain-growth anchors per warp: 1..32 (2) */
     int64_t chunk_pairs;              /* neighbour pairs whose bundles are held in HBM at once (4 Mi) */
 } cvl_tuning;
 /* The bucket a batch of num_edges edges uses. */
