@@ -252,7 +252,7 @@ cvl_tuning default_tuning(int cell_size, int seeds_per_group) {
     t.bundle_blocks_per_sm = 4;
     t.growth_blocks_per_sm = 4;
     t.seeds_per_group = seeds_per_group;
-    t.anchors_per_warp = 2;
+    t.anchors_per_warp = 8;
     t.chunk_pairs = (int64_t)CHUNK_PAIRS_DEFAULT;
     return t;
 }
@@ -423,9 +423,8 @@ int launch_bundles(cvl_engine *e, BundleArgs &a, int blocks) {
 template <int CPL, int K, int MINB>
 int launch_growth(cvl_engine *e, GrowthArgs &a, size_t smem, int blocks) {
     CVL_CUDA(cudaFuncSetAttribute(k_growth<CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    // a warp per anchor, 4 anchors per warp: short blocks (a higher-priority
-    // stream's blocks get SMs as soon as any block ends) with the per-block
-    // set-up spread over 16 anchors
+    // a warp per anchor and anchors_per_warp anchors per warp: short blocks (a
+    // higher-priority stream's blocks get SMs as soon as any block ends)
     const long long per_block = 4LL * a.anchors_per_warp;
     blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + per_block - 1) / per_block,
                                                     0x7fffffffLL));

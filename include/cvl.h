@@ -318,7 +318,7 @@ typedef struct cvl_tuning {
     int bundle_blocks_per_sm;         /* bundle kernel's register budget: 3 or 4 resident blocks per SM (4) */
     int growth_blocks_per_sm;         /* growth kernel's register budget: 4 or 6 resident blocks per SM (4) */
     int seeds_per_group;              /* chain-growth seeds walked together per warp: 4 or 8 (4) */
-    int anchors_per_warp;             /* chain-growth anchors per warp: 1..32 (2) */
+    int anchors_per_warp;             /* chain-growth anchors per warp: 1..32 (8) */
     int64_t chunk_pairs;              /* neighbour pairs whose bundles are held in HBM at once (4 Mi) */
 } cvl_tuning;
 /* The bucket a batch of num_edges edges uses. */
