@@ -425,10 +425,10 @@ int launch_growth(cvl_engine *e, GrowthArgs &a, size_t smem, int blocks) {
     CVL_CUDA(cudaFuncSetAttribute(k_growth<CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // a warp per anchor and anchors_per_warp anchors per warp: short blocks (a
     // higher-priority stream's blocks get SMs as soon as any block ends)
-    const long long per_block = 4LL * a.anchors_per_warp;
+    const long long per_block = (GROWTH_THREADS / 32) * (long long)a.anchors_per_warp;
     blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + per_block - 1) / per_block,
                                                     0x7fffffffLL));
-    k_growth<CPL, K, MINB><<<blocks, 128, smem, e->stream>>>(a);
+    k_growth<CPL, K, MINB><<<blocks, GROWTH_THREADS, smem, e->stream>>>(a);
     return check_launch("k_growth");
 }
 
@@ -615,7 +615,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     bundles_fn bf;
     growth_fn gf;
     pick_kernels(cpl, tn, bf, gf);
-    const size_t gsmem = (size_t)4 * growth_smem_per_warp(md.max_cand, md.gms);
+    const size_t gsmem = (size_t)(GROWTH_THREADS / 32) * growth_smem_per_warp(md.max_cand, md.gms);
     int gbps = 0;
     {
         // occupancy of the chosen growth kernel

@@ -279,10 +279,12 @@ __host__ __device__ inline size_t growth_smem_per_warp(int max_cand, int gms) {
     return (b + 15) & ~(size_t)15;
 }
 
-// K: seeds walked together; MINB: the resident blocks per SM the register
-// allocation is capped for
+// K: seeds walked together; MINB: the register budget, as resident blocks of 4
+// warps per SM. A block is one warp: a block's SM slot frees as soon as its own
+// anchors are done (measured 2% faster than 4-warp blocks).
+constexpr int GROWTH_THREADS = 32;
 template <int CPL, int K, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_growth(GrowthArgs a) {
+__global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs a) {
     extern __shared__ __align__(16) unsigned char gr_smem[];
     const Model &md = a.md;
     const int lane = threadIdx.x & 31;
