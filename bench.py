@@ -50,6 +50,11 @@ FLOPS_PER_PAIR_CELL = 20
 # traffic is the bundle write (1,008 B per pair) plus the pair/anchor reads, so it
 # scales with the pairs a launch processes.
 BUNDLE_DRAM_BYTES_PER_PAIR = (0.338025e9 + 2.194154e9) / 2_176_780
+# FP64-pipe instructions of k_bundles per cell, from the same capture: the pipe was
+# active 45.38% of 1.046336 ms on 148 SMs (each issues 2 FP64 warp-instructions a
+# cycle at 1.965 GHz), 30.65 active lanes per warp-instruction, 2,176,780 x 63 cells.
+# A division costs about 10 of them, which the algorithmic count above takes as 1 flop.
+BUNDLE_FP64_INSTR_PER_CELL = 0.4538 * 1.046336e-3 * 148 * 2 * 1.965e9 * 30.65 / (2_176_780 * 63)
 
 
 def _args():
@@ -483,7 +488,13 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
                      "traffic_unit": "bytes per launch",
                      "traffic_source": "ncu dram bytes of k_bundles on the 242k-edge map, per non-close pair, "
                                        "times this workload's pairs per launch",
-                     "algorithmic_bytes": 1008.0 * nonclose / launches_b},
+                     "algorithmic_bytes": 1008.0 * nonclose / launches_b,
+                     "fp64_pipe": {
+                         "instr_per_cell": BUNDLE_FP64_INSTR_PER_CELL,
+                         "frac": (BUNDLE_FP64_INSTR_PER_CELL * 63 * nonclose / (curv_ms / 1e3)
+                                  / (fp64_peak * 1e12 / 2.0)) if (fp64_peak and curv_ms > 0) else None,
+                         "note": "FP64-pipe instructions per cell from ncu, scaled to this run's k_bundles time, "
+                                 "against the DFMA issue peak (measured TFLOP/s / 2)"}},
         "gpu_launches": launches,
         "clocks": clocks,
         "e2e": e2e,

@@ -67,6 +67,8 @@ inline unsigned next_pow2(unsigned long long v) {
 
 int cvl_fail(int code, const std::string &msg) { return fail(code, msg); }
 
+void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx);
+
 // Results live in page-locked memory (cvl::PinnedArena): device-to-host copies
 // at full PCIe/C2C rate and no per-call pinning. The arena is shared by the
 // engine and its live results, so a result may outlive its engine.
@@ -91,6 +93,9 @@ struct cvl_engine {
     DBuf chains, info, stats, err, work, scratch, scratch_chain, scratch_res, scan_tmp, flush, deg_orig, off_orig,
         gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start, crank;
     cvl_tuning tune[CVL_TUNING_BUCKETS];                   // per size bucket of the batch
+    cvl_yield_fn yield_fn = nullptr;                       // called between chunks (serving)
+    void *yield_ctx = nullptr;
+    cudaEvent_t chunk_done = nullptr;
     std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
     DBuf pairs_in, pb_min, pb_max, pb_valid;
@@ -652,6 +657,14 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
         for (int c = 0; c < nchunks; ++c) {
             const int a0 = cstart[c], a1 = cstart[c + 1];
             if (a1 <= a0) continue;
+            if (e->yield_fn && c > 0) {
+                // let the previous chunk finish, then give the hook the chance to hold
+                // this stream back while others' work goes first
+                if (!e->chunk_done) CVL_CUDA(cudaEventCreateWithFlags(&e->chunk_done, cudaEventDisableTiming));
+                CVL_CUDA(cudaEventRecord(e->chunk_done, s));
+                CVL_CUDA(cudaEventSynchronize(e->chunk_done));
+                e->yield_fn(e->yield_ctx);
+            }
             BundleArgs ba{};
             ba.md = md;
             ba.B = B;
@@ -876,6 +889,7 @@ void cvl_engine_destroy(cvl_engine *e) {
     while (!e->batches.empty()) cvl_batch_free(e->batches.back());
     e->release_all();
     for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
+    if (e->chunk_done) cudaEventDestroy(e->chunk_done);
     cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -1302,6 +1316,16 @@ int cvl_batch_result_stats(const cvl_batch_result *r, cvl_batch_stats *out) {
 void cvl_batch_result_free(cvl_batch_result *r) { delete r; }
 
 int cvl_tuning_bucket(int64_t num_edges) { return bucket_of((long long)num_edges); }
+
+}  // extern "C"
+
+void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx) {
+    if (!e) return;
+    e->yield_fn = fn;
+    e->yield_ctx = ctx;
+}
+
+extern "C" {
 
 int cvl_engine_get_tuning(cvl_engine *e, int bucket, cvl_tuning *t) {
     if (!e || !t || bucket < 0 || bucket >= CVL_TUNING_BUCKETS) return fail(CVL_EINVAL, "invalid tuning arguments");

@@ -6,3 +6,12 @@
 
 // Records msg as the calling thread's cvl_last_error() and returns code.
 int cvl_fail(int code, const std::string &msg);
+
+struct cvl_engine;
+
+// A host hook that the engine calls between the bundle/growth chunks of a run,
+// once the previous chunk's kernels have finished. The hook may block to let
+// other streams' work through first (the server uses it to yield a large map
+// to small ones); nullptr removes it.
+using cvl_yield_fn = void (*)(void *ctx);
+void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx);

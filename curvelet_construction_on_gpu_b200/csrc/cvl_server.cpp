@@ -65,6 +65,8 @@ struct cvl_server {
     std::mutex mu;
     std::condition_variable cv_work;  // workers: requests queued or stop
     std::condition_variable cv_done;  // waiters: a request finished
+    std::condition_variable cv_yield; // large launches waiting for the small lane to drain
+    int small_running = 0;            // small-lane launches on the device
     std::deque<Request *> lanes[2];   // 0 small, 1 large
     std::unordered_map<uint64_t, Request *> reqs;
     std::deque<uint64_t> finished;    // ids in completion order, not handed out yet
@@ -110,6 +112,21 @@ struct cvl_server {
     }
 
     void worker(int w);
+
+    // Engine hook of a worker running a large launch, called between its chunks:
+    // while small-lane work is queued or running, hold back (10 ms at most), so
+    // that a small map does not share the SMs with a large map's chunks. Only
+    // when the server is not backlogged: with requests piling up, the GPU must
+    // not idle and the large launch goes on.
+    static constexpr size_t YIELD_MAX_QUEUED = 4;
+    static void yield_to_small(void *ctx) {
+        cvl_server *s = (cvl_server *)ctx;
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_yield.wait_for(lk, std::chrono::milliseconds(10), [&] {
+            const size_t queued = s->lanes[0].size() + s->lanes[1].size();
+            return s->stop || queued > YIELD_MAX_QUEUED || (s->small_running == 0 && s->lanes[0].empty());
+        });
+    }
 };
 
 void cvl_server::worker(int w) {
@@ -119,6 +136,7 @@ void cvl_server::worker(int w) {
     std::vector<Request *> take;
     std::vector<int32_t> counts;
     std::vector<const double *> parts;
+    int lane_now = 0;
     while (true) {
         take.clear();
         {
@@ -126,6 +144,7 @@ void cvl_server::worker(int w) {
             cv_work.wait(lk, [&] { return stop || lane_to_take(w) >= 0; });
             if (stop) break;
             const int l = lane_to_take(w);
+            lane_now = l;
             int64_t sum = 0;
             while (!lanes[l].empty()) {
                 Request *r = lanes[l].front();
@@ -139,7 +158,11 @@ void cvl_server::worker(int w) {
                 sum += r->n;
             }
             ++launches;
+            if (lane_now == 0) ++small_running;
         }
+        cv_yield.notify_all();
+        // a large launch yields to small ones between its chunks (with another worker to run them)
+        cvl_engine_set_yield(e, (lane_now == 1 && cfg.workers >= 2) ? &cvl_server::yield_to_small : nullptr, this);
         // one edge_data_sz per launch: a request with another width goes alone
         size_t cut = 1;
         while (cut < take.size() && take[cut]->sz == take[0]->sz) ++cut;
@@ -201,9 +224,11 @@ void cvl_server::worker(int w) {
                 take[m]->edges = nullptr;
                 finish(take[m], st[m], errs[m], outs[m]);
             }
+            if (lane_now == 0) --small_running;
         }
         cv_done.notify_all();
         cv_work.notify_all();  // budget freed
+        cv_yield.notify_all();
     }
     if (batch) cvl_batch_free(batch);
 }
@@ -417,6 +442,7 @@ void cvl_server_destroy(cvl_server *s) {
         }
     }
     s->cv_work.notify_all();
+    s->cv_yield.notify_all();
     for (std::thread &t : s->threads) t.join();
     s->cv_done.notify_all();
     for (auto &kv : s->reqs) {
