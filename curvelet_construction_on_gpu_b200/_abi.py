@@ -120,6 +120,9 @@ SIGNATURES = [
     ("cvl_server_stats_get", C.c_int, [_vp, C.POINTER(CvlServerStats)]),
     ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.c_int64]),
     ("cvl_server_destroy", None, [_vp]),
+    ("cvl_read_edges", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_dp), C.POINTER(C.c_int64)]),
+    ("cvl_free_edges", None, [_dp]),
+    ("cvl_write_edges_binary", C.c_int, [C.c_char_p, _dp, C.c_int64, C.c_int32]),
     ("cvl_tuning_bucket", C.c_int, [C.c_int64]),
     ("cvl_engine_get_tuning", C.c_int, [_vp, C.c_int, C.POINTER(CvlTuning)]),
     ("cvl_engine_set_tuning", C.c_int, [_vp, C.c_int, C.POINTER(CvlTuning)]),

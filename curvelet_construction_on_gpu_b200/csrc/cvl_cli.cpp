@@ -136,55 +136,26 @@ bool parse_args(int argc, char **argv, CliParams &cp, bool &use_double, std::str
     return true;
 }
 
-bool blank(const std::string &s) { return s.find_first_not_of(" \t\r\n") == std::string::npos; }
-
-// Edge-file reader with the reference's acceptance rules (data_io.hpp:22-79).
+// Edge-file reader with the reference's acceptance rules and messages
+// (data_io.hpp:22-79), multi-threaded in libcvl (cvl_read_edges); a name ending in
+// ".cvle" is the binary edge format.
 bool read_edges(const std::string &filename, int per_edge, std::vector<double> &out) {
     const std::string path = "../test_files/" + filename;
-    std::ifstream in(path);
-    if (!in) {
+    if (!std::ifstream(path)) {
         std::cerr << "Error: input file does not exist: " << path << std::endl;
         return false;
     }
     std::cout << "reading data from file " << filename << std::endl;
     out.clear();
-    std::string line;
-    int ln = 0, count = 0;
-    while (std::getline(in, line)) {
-        ++ln;
-        if (blank(line)) {
-            std::cerr << "Error: blank line at line " << ln << " in " << path << " (each line must contain exactly "
-                      << per_edge << " numeric values)" << std::endl;
-            out.clear();
-            return false;
-        }
-        std::istringstream iss(line);
-        for (int j = 0; j < per_edge; j++) {
-            double v;
-            if (!(iss >> v)) {
-                std::cerr << "Error: invalid edge file format in " << path << " at line " << ln << ": expected "
-                          << per_edge << " numeric values per line, found " << j << "." << std::endl;
-                out.clear();
-                return false;
-            }
-            out.push_back(v);
-        }
-        std::string rest;
-        std::getline(iss, rest);
-        if (!blank(rest)) {
-            std::cerr << "Error: invalid edge file format in " << path << " at line " << ln << ": expected exactly "
-                      << per_edge << " numeric values per line, found extra data." << std::endl;
-            out.clear();
-            return false;
-        }
-        ++count;
-    }
-    if (count == 0) {
-        std::cerr << "Error: input file contains no valid edges: " << path << std::endl;
-        out.clear();
+    double *buf = nullptr;
+    int64_t n = 0;
+    if (cvl_read_edges(path.c_str(), per_edge, 0, &buf, &n) != CVL_OK) {
+        std::cerr << cvl_last_error() << std::endl;
         return false;
     }
-    std::cout << "read " << count << " edges from " << filename << std::endl;
+    out.assign(buf, buf + (size_t)n * per_edge);
+    cvl_free_edges(buf);
+    std::cout << "read " << n << " edges from " << filename << std::endl;
     return true;
 }
 

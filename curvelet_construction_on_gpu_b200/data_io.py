@@ -74,3 +74,36 @@ def chain_to_info_filename(chain_file: str) -> str:
     if pos >= 0:
         return chain_file[:pos] + "info" + chain_file[pos + 5:]
     return "info_" + chain_file
+
+
+def read_edges(path: str, values_per_edge: int = 4, nthreads: int = 0) -> np.ndarray:
+    """An edge file through cvl_read_edges: the reference's text format read on
+    all cores (same values and error messages as its stream reader), or the
+    binary format for a path ending in ".cvle". nthreads -1: the stream reader
+    alone. Raises ValueError with the reference's message on bad input."""
+    import ctypes as C
+
+    from . import _abi
+    lib = _abi.load()
+    ptr = C.POINTER(C.c_double)()
+    n = C.c_int64(0)
+    rc = lib.cvl_read_edges(path.encode(), values_per_edge, nthreads, C.byref(ptr), C.byref(n))
+    if rc != 0:
+        raise ValueError(lib.cvl_last_error().decode())
+    try:
+        return np.ctypeslib.as_array(ptr, shape=(int(n.value) * values_per_edge,)).reshape(-1, values_per_edge).copy()
+    finally:
+        lib.cvl_free_edges(ptr)
+
+
+def write_edges_binary(path: str, edges: np.ndarray) -> None:
+    """The binary edge format (cvl_write_edges_binary): "CVLEDGE1", uint32
+    values_per_edge, uint32 0, uint64 num_edges, little-endian float64 rows."""
+    import ctypes as C
+
+    from . import _abi
+    e = np.ascontiguousarray(edges, dtype=np.float64)
+    rc = _abi.load().cvl_write_edges_binary(path.encode(), e.ctypes.data_as(C.POINTER(C.c_double)), e.shape[0],
+                                            e.shape[1])
+    if rc != 0:
+        raise ValueError(_abi.load().cvl_last_error().decode())

@@ -307,6 +307,19 @@ int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, int64_t 
  * workers and releases everything. */
 void cvl_server_destroy(cvl_server *s);
 
+/* ---- edge files ----------------------------------------------------------
+ * read_TO_edges_from_file (data_io.hpp:22-79) for any path, multi-threaded:
+ * the same values and the same error messages (in cvl_last_error) as the
+ * reference's stream reader on every input. A path ending in ".cvle" is read as
+ * the binary format of cvl_write_edges_binary instead. *edges is freed with
+ * cvl_free_edges. nthreads 0: all hardware threads; -1: the stream reader
+ * alone, line by line (the reference's loop, for comparisons). */
+int cvl_read_edges(const char *path, int32_t values_per_edge, int32_t nthreads, double **edges, int64_t *num_edges);
+void cvl_free_edges(double *edges);
+/* Binary edge file: "CVLEDGE1", uint32 values_per_edge, uint32 0, uint64
+ * num_edges, then the rows as little-endian doubles (no reference counterpart). */
+int cvl_write_edges_binary(const char *path, const double *edges, int64_t num_edges, int32_t values_per_edge);
+
 /* ---- tuning and the autotuner -------------------------------------------
  * No reference counterpart. An engine keeps one tuning per size bucket of the
  * batch (its total edges); every tuning gives the same results bit for bit,
