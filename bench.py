@@ -15,6 +15,8 @@ one batch of seeded synthetic edges. Workloads:
   plain_hd    one 1920x1080 map, ~242k edges, one map per launch
   plain_small one 480x320 map (~4.5k edges)
   served      only the served stream, at each rate of --rates
+  stress      16 dense 3840x2160 maps interleaved with 1,024 small 640x480 maps,
+              Poisson at 150 maps/s; small-map p99 apart
 
 value: edges/s with the edges already in HBM (CUDA events on the engine's
 stream around each step, L2 flushed between steps). e2e: the same metric
@@ -63,7 +65,8 @@ def _args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="mixed64", choices=["mixed64", "plain_hd", "plain_small", "served"])
+    ap.add_argument("--workload", default="mixed64",
+                    choices=["mixed64", "plain_hd", "plain_small", "served", "stress"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-served", action="store_true")
@@ -72,7 +75,9 @@ def _args():
     ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")
     ap.add_argument("--requests", type=int, default=600, help="served stream: requests per rate")
     ap.add_argument("--workers", type=int, default=2, help="served stream: server workers")
-    return ap.parse_args()
+    args = ap.parse_args()
+    args.rate_given = any(a == "--rate" or a.startswith("--rate=") for a in sys.argv[1:])
+    return args
 
 
 def _workload(name: str, rank: int):
@@ -81,10 +86,14 @@ def _workload(name: str, rank: int):
         return [synth.plain_hd(1000 + rank)], {"image": "1920x1080", "curves": 1500, "clutter": 0.2}
     if name == "plain_small":
         return [synth.plain_small(0 + rank)], {"image": "480x320", "curves": 50, "clutter": 0.1}
+    if name == "stress":
+        maps, kinds = synth.stress_mix(5000 + 10_000 * rank)
+        return maps, {"maps": len(maps), "dense": "16 x 3840x2160 (6,000 curves, half radius 3-15 px, 40% clutter)",
+                      "small": "1024 x 640x480 (config-0 generator)", "_labels": kinds}
     # mixed64 and served share the pool of 64 seeded maps
     maps = synth.mixed64(2000 + 64 * rank, 64)
-    images = [synth.mixed_map_image(2000 + 64 * rank + i) for i in range(64)]
-    return maps, {"maps": 64, "images": "640x480..3840x2160", "clutter": 0.2, "_images": images}
+    images = ["%dx%d" % synth.mixed_map_image(2000 + 64 * rank + i) for i in range(64)]
+    return maps, {"maps": 64, "images": "640x480..3840x2160", "clutter": 0.2, "_labels": images}
 
 
 class _Clocks:
@@ -296,28 +305,38 @@ def _plain_device_ms(eng, maps, steps: int) -> float:
     return total / steps
 
 
-def _served(maps, images, rate: float, n_req: int, workers: int, device: int, seed: int = 7) -> dict:
-    """Open-loop Poisson stream through cvl_server_*: n_req maps drawn (with
-    replacement) from `maps`, arrivals at `rate` maps/s, submitted on schedule
-    by one thread while another collects the results. Latency is the server's
-    own clock from the submit call to the result being ready in host memory."""
+def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, seed: int = 7,
+            sequence=None, warm_all: bool = True) -> dict:
+    """Open-loop Poisson stream through cvl_server_*: arrivals at `rate` maps/s,
+    submitted on schedule by one thread while another takes the results in
+    completion order. The maps are `sequence` (indices into maps) when given,
+    else n_req draws with replacement. Latency is the server's own clock from the
+    submit call to the result being ready in host memory; labels[i] names map
+    i's class, and each class gets its own percentiles."""
     import threading
 
     import curvelet_construction_on_gpu_b200 as cvl
     from curvelet_construction_on_gpu_b200 import _abi
     rng = np.random.default_rng(seed)
-    picks = rng.integers(0, len(maps), n_req)
+    picks = np.asarray(sequence) if sequence is not None else rng.integers(0, len(maps), n_req)
+    n_req = len(picks)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     srv = cvl.Server(device=device, workers=workers)
     try:
         # warm-up (workspace and page-locked arena growth): the largest map once per
-        # worker, then every map of the pool once
+        # worker, then every map of the pool once (or a few of each class)
         order = np.argsort([m.shape[0] for m in maps])
         warm = [srv.submit(maps[int(order[-1])]) for _ in range(workers)]
-        warm += [srv.submit(m) for m in maps]
+        if warm_all:
+            warm += [srv.submit(m) for m in maps]
+        else:
+            seen = {}
+            for i, lab in enumerate(labels):
+                if seen.get(lab, 0) < 4:
+                    seen[lab] = seen.get(lab, 0) + 1
+                    warm.append(srv.submit(maps[i]))
         for _ in warm:
             srv.next()
-        n_warm = len(warm)
         warm_stats = srv.stats()
         ids = [None] * n_req
         t0 = time.perf_counter()
@@ -348,22 +367,26 @@ def _served(maps, images, rate: float, n_req: int, workers: int, device: int, se
         th.join()
         wall = time.perf_counter() - t0
         st = srv.stats()
-        ms, ed = srv.latencies()
+        ms, ed, rid = srv.latencies(with_ids=True)
         st0 = warm_stats
     finally:
         srv.close()
-    ms, ed = ms[n_warm:], ed[n_warm:]
-    hd_edges = {int(maps[i].shape[0]) for i in range(len(maps)) if images[i] == (1920, 1080)}
-    hd = np.array([m for m, e in zip(ms, ed) if int(e) in hd_edges])
+    label_of = {int(ids[k]): labels[int(picks[k])] for k in range(n_req)}
+    keep = np.array([int(r) in label_of for r in rid], bool)
+    ms, ed, rid = ms[keep], ed[keep], rid[keep]
 
     def pct(a, q):
         return float(np.percentile(a, q, method="inverted_cdf")) if len(a) else None
 
+    classes = {}
+    for lab in sorted(set(label_of.values())):
+        sel = np.array([label_of[int(r)] == lab for r in rid], bool)
+        classes[lab] = {"requests": int(sel.sum()), "p50_ms": pct(ms[sel], 50), "p99_ms": pct(ms[sel], 99)}
     edges = float(np.sum(ed))
     return {"rate_maps_per_s": rate, "requests": n_req, "workers": workers, "wall_s": wall,
             "edges_per_s": edges / wall, "maps_per_s": len(ms) / wall,
             "p50_ms": pct(ms, 50), "p95_ms": pct(ms, 95), "p99_ms": pct(ms, 99), "max_ms": float(np.max(ms)),
-            "hd_1920x1080": {"requests": int(len(hd)), "p50_ms": pct(hd, 50), "p99_ms": pct(hd, 99)},
+            "by_class": classes,
             "launches": int(st["launches"] - st0["launches"]), "failed": int(st["failed"]),
             "worker_ms": {k: float(st[k] - st0[k]) for k in ("upload_ms", "run_ms", "device_ms", "result_ms")},
             "queue_ms_mean": float(st["queue_ms"] - st0["queue_ms"]) / max(1, len(ms)),
@@ -456,11 +479,11 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
                         "pinned host edges")}
 
     served = None
-    if len(maps) > 1 and not args.no_served and cfg.get("_images"):
+    if len(maps) > 1 and not args.no_served and cfg.get("_labels"):
         _progress(f"served stream at {args.rate} maps/s")
         batch.close()
         eng.close()
-        served = _served(maps, cfg["_images"], args.rate, args.requests, args.workers, local)
+        served = _served(maps, cfg["_labels"], args.rate, args.requests, args.workers, local)
 
     if rank != 0:
         return
@@ -507,7 +530,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     if world == 1 and not args.no_cpu_baseline:
         _progress("cpu baseline")
         line["cpu_baseline"] = _cpu_baseline(maps)
-    line["config"].pop("_images", None)
+    line["config"].pop("_labels", None)
     print(json.dumps(line))
     eng.close()
 
@@ -515,7 +538,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
 def run_served(args, maps, cfg, world, rank, local, pg):
     """The served stream alone, swept over --rates (one JSON line)."""
     rates = [float(r) for r in args.rates.split(",") if r]
-    sweep = [_served(maps, cfg["_images"], r, args.requests, args.workers, local) for r in rates]
+    sweep = [_served(maps, cfg["_labels"], r, args.requests, args.workers, local) for r in rates]
     if rank != 0:
         return
     best = max(sweep, key=lambda d: d["edges_per_s"])
@@ -528,6 +551,23 @@ def run_served(args, maps, cfg, world, rank, local, pg):
         "served": sweep}))
 
 
+def run_stress(args, maps, cfg, world, rank, local, pg):
+    """The stress stream: every map once, in its seeded
+    interleaved order, Poisson at --rate (150 maps/s unless given); small-map
+    latency reported apart from the dense maps'."""
+    rate = args.rate if args.rate_given else 150.0
+    sv = _served(maps, cfg["_labels"], rate, len(maps), args.workers, local, sequence=list(range(len(maps))),
+                 warm_all=False)
+    if rank != 0:
+        return
+    cfg = {k: v for k, v in cfg.items() if not k.startswith("_")}
+    print(json.dumps({
+        "metric": METRIC, "value": sv["edges_per_s"], "unit": METRIC, "n_gpus": world, "steps": 1, "warmup": 1,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators, curvelet_construction_on_gpu_b200/synth.py)",
+        "config": dict(workload="stress", rate_maps_per_s=rate, **cfg), "served": sv}))
+
+
 def main():
     args = _args()
     world, rank, local, pg = _dist_init(args)
@@ -537,6 +577,8 @@ def main():
             run_reference(args, maps, cfg, world, rank)
         elif args.workload == "served":
             run_served(args, maps, cfg, world, rank, local, pg)
+        elif args.workload == "stress":
+            run_stress(args, maps, cfg, world, rank, local, pg)
         else:
             run_ours(args, maps, cfg, world, rank, local, pg)
     finally:

@@ -60,7 +60,7 @@ class CvlBatchStats(C.Structure):
 class CvlServerCfg(C.Structure):
     _fields_ = [("device", C.c_int), ("workers", C.c_int), ("mem_budget_bytes", C.c_size_t),
                 ("admit_bytes_per_edge", C.c_size_t), ("max_batch_edges", C.c_int64),
-                ("large_map_edges", C.c_int64)]
+                ("large_map_edges", C.c_int64), ("host_reserve_bytes", C.c_size_t)]
 
 
 class CvlServerStats(C.Structure):
@@ -118,7 +118,7 @@ SIGNATURES = [
     ("cvl_server_wait", C.c_int, [_vp, C.c_uint64, C.c_int64, C.POINTER(_vp)]),
     ("cvl_server_next", C.c_int, [_vp, C.c_int64, C.POINTER(C.c_uint64), C.POINTER(_vp)]),
     ("cvl_server_stats_get", C.c_int, [_vp, C.POINTER(CvlServerStats)]),
-    ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.c_int64]),
+    ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), C.c_int64]),
     ("cvl_server_destroy", None, [_vp]),
     ("cvl_read_edges", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_dp), C.POINTER(C.c_int64)]),
     ("cvl_free_edges", None, [_dp]),

@@ -378,7 +378,8 @@ class Server:
 
     def __init__(self, params: CurveletParams | None = None, device: int = 0, workers: int = 2,
                  mem_budget_bytes: int = 40 << 30, admit_bytes_per_edge: int = 2048,
-                 max_batch_edges: int = 4 << 20, large_map_edges: int = 1_000_000):
+                 max_batch_edges: int = 4 << 20, large_map_edges: int = 1_000_000,
+                 host_reserve_bytes: int = 2 << 30):
         lib = _abi.load()
         self._lib = lib
         cfg = _abi.CvlServerCfg()
@@ -386,6 +387,7 @@ class Server:
         cfg.device, cfg.workers, cfg.mem_budget_bytes = device, workers, mem_budget_bytes
         cfg.admit_bytes_per_edge, cfg.max_batch_edges, cfg.large_map_edges = (admit_bytes_per_edge, max_batch_edges,
                                                                               large_map_edges)
+        cfg.host_reserve_bytes = host_reserve_bytes
         self._p = (params or CurveletParams()).to_c()
         h = C.c_void_p()
         check(lib.cvl_server_create(C.byref(cfg), C.byref(self._p), C.byref(h)), "cvl_server_create")
@@ -430,16 +432,18 @@ class Server:
         check(self._lib.cvl_server_stats_get(self._h, C.byref(st)), "cvl_server_stats_get")
         return {name: getattr(st, name) for name, _ in st._fields_}
 
-    def latencies(self) -> tuple[np.ndarray, np.ndarray]:
-        """(ms, edges) of every completed request, in completion order."""
+    def latencies(self, with_ids: bool = False):
+        """(ms, edges[, ids]) of every completed request, in completion order."""
         n = int(self.stats()["completed"])
         ms = np.zeros(max(n, 1))
         ed = np.zeros(max(n, 1), np.int64)
+        ids = np.zeros(max(n, 1), np.uint64)
         k = self._lib.cvl_server_latencies(self._h, ms.ctypes.data_as(_abi._dp),
-                                           ed.ctypes.data_as(C.POINTER(C.c_int64)), n)
+                                           ed.ctypes.data_as(C.POINTER(C.c_int64)),
+                                           ids.ctypes.data_as(C.POINTER(C.c_uint64)), n)
         if k < 0:
             check(int(k), "cvl_server_latencies")
-        return ms[:k], ed[:k]
+        return (ms[:k], ed[:k], ids[:k]) if with_ids else (ms[:k], ed[:k])
 
     def close(self):
         if self._h:

@@ -1325,6 +1325,12 @@ void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx) {
     e->yield_ctx = ctx;
 }
 
+int cvl_engine_reserve_host(cvl_engine *e, size_t bytes) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    if (bytes && !e->pinned->reserve(bytes)) return fail(CVL_ENOMEM, "page-locked host memory could not be reserved");
+    return CVL_OK;
+}
+
 extern "C" {
 
 int cvl_engine_get_tuning(cvl_engine *e, int bucket, cvl_tuning *t) {

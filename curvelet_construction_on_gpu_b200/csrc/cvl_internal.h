@@ -15,3 +15,7 @@ struct cvl_engine;
 // to small ones); nullptr removes it.
 using cvl_yield_fn = void (*)(void *ctx);
 void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx);
+
+// Sets aside `bytes` of page-locked host memory in the engine's result arena
+// (one chunk made ahead of time, so results do not pin memory while serving).
+int cvl_engine_reserve_host(cvl_engine *e, size_t bytes);

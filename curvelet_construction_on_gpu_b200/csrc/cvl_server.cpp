@@ -78,6 +78,7 @@ struct cvl_server {
     double upload_ms = 0, run_ms = 0, device_ms = 0, result_ms = 0, queue_ms = 0;
     std::vector<double> lat_ms;
     std::vector<int64_t> lat_edges;
+    std::vector<uint64_t> lat_ids;
 
     // the lane a worker serves first (the last worker prefers large maps when there are several)
     int preferred_lane(int w) const { return (cfg.workers >= 2 && w == cfg.workers - 1) ? 1 : 0; }
@@ -106,6 +107,7 @@ struct cvl_server {
             edges_completed += (uint64_t)r->n;
             lat_ms.push_back(ms_between(r->t_submit, Clock::now()));
             lat_edges.push_back(r->n);
+            lat_ids.push_back(r->id);
         } else {
             ++failed;
         }
@@ -243,6 +245,7 @@ void cvl_server_cfg_default(cvl_server_cfg *c) {
     c->admit_bytes_per_edge = 2048;
     c->max_batch_edges = 4 << 20;
     c->large_map_edges = 1000000;
+    c->host_reserve_bytes = (size_t)2 << 30;
 }
 
 int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out) {
@@ -273,6 +276,18 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
             return cvl_fail(rc, msg);
         }
         s->engines.push_back(e);
+        const int rr = cvl_engine_reserve_host(e, c.host_reserve_bytes);
+        if (rr != CVL_OK) {
+            const std::string msg = cvl_last_error();
+            for (cvl_engine *x : s->engines) cvl_engine_destroy(x);
+            delete s;
+            return cvl_fail(rr, msg);
+        }
+    }
+    if (c.host_reserve_bytes && !s->host.reserve(c.host_reserve_bytes)) {
+        for (cvl_engine *x : s->engines) cvl_engine_destroy(x);
+        delete s;
+        return cvl_fail(CVL_ENOMEM, "page-locked host memory could not be reserved");
     }
     for (int w = 0; w < c.workers; ++w) s->threads.emplace_back(&cvl_server::worker, s, w);
     *out = s;
@@ -413,13 +428,14 @@ int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out) {
     return CVL_OK;
 }
 
-int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, int64_t cap) {
+int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, uint64_t *ids, int64_t cap) {
     if (!s || cap < 0 || (cap > 0 && (!ms || !edges))) return cvl_fail(CVL_EINVAL, "invalid arguments");
     std::lock_guard<std::mutex> lk(s->mu);
     const int64_t n = std::min<int64_t>(cap, (int64_t)s->lat_ms.size());
     for (int64_t k = 0; k < n; ++k) {
         ms[k] = s->lat_ms[k];
         edges[k] = s->lat_edges[k];
+        if (ids) ids[k] = s->lat_ids[k];
     }
     return n;
 }

@@ -101,11 +101,10 @@ def _hd_curves(rng, n, W, H):
     return _arcs(rng, n_arc, W, H, radius, alen) + _segments(rng, n_seg, W, H, slen)
 
 
-def plain_small(seed: int = 0) -> np.ndarray:
-    """480x320: 40 arcs (radius U[8, 200], length U[20, 300]), 10 segments
-    (length U[20, 200]), 10% clutter; ~6k edges."""
+def plain_small(seed: int = 0, W: int = 480, H: int = 320) -> np.ndarray:
+    """480x320 (or W x H): 40 arcs (radius U[8, 200], length U[20, 300]), 10
+    segments (length U[20, 200]), 10% clutter; ~6k edges."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    W, H = 480, 320
     radius = rng.uniform(8.0, 200.0, 40)
     alen = rng.uniform(20.0, 300.0, 40)
     slen = rng.uniform(20.0, 200.0, 10)
@@ -149,6 +148,16 @@ def dense_4k(seed: int = 4000) -> np.ndarray:
     alen = rng.uniform(10.0, 60.0, 3000)
     curves = _arcs(rng, 3000, W, H, radius, alen) + _hd_curves(rng, 3000, W, H)
     return _assemble(rng, curves, W, H, 0.40)
+
+
+def stress_mix(base_seed: int = 5000, n_dense: int = 16, n_small: int = 1024) -> tuple[list[np.ndarray], list[str]]:
+    """The stress stream's maps: n_dense dense 3840x2160 maps (dense_4k) and
+    n_small config-0 maps at 640x480, interleaved in a seeded random order.
+    Returns (maps, kinds) with kinds "dense" / "small"."""
+    maps = [(dense_4k(base_seed + i), "dense") for i in range(n_dense)]
+    maps += [(plain_small(base_seed + 100 + i, 640, 480), "small") for i in range(n_small)]
+    order = np.random.Generator(np.random.PCG64(base_seed)).permutation(len(maps))
+    return [maps[i][0] for i in order], [maps[i][1] for i in order]
 
 
 def write_edge_file(path: str, edges: np.ndarray) -> None:

@@ -264,6 +264,8 @@ typedef struct cvl_server_cfg {
                                       footprint per edge, edges + hash + neighbour pairs + curvelets) */
     int64_t max_batch_edges;       /* edges folded into one launch at most; a larger map runs alone (4 Mi) */
     int64_t large_map_edges;       /* maps with at least this many edges use the large lane (1,000,000) */
+    size_t host_reserve_bytes;     /* page-locked host memory set aside at creation for each worker's results
+                                      and for the queued requests, so that serving does not pin memory (2 GiB) */
 } cvl_server_cfg;
 
 typedef struct cvl_server_stats {
@@ -300,9 +302,10 @@ int cvl_server_wait(cvl_server *s, uint64_t id, int64_t timeout_us, cvl_result *
  * at once if no request is queued or running. */
 int cvl_server_next(cvl_server *s, int64_t timeout_us, uint64_t *id, cvl_result **out);
 int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out);
-/* Latency (ms, submit -> result ready) and edge count of each completed
- * request, in completion order; returns how many were written (<= cap). */
-int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, int64_t cap);
+/* Latency (ms, submit -> result ready), edge count and id of each completed
+ * request, in completion order; returns how many were written (<= cap). ids
+ * may be NULL. */
+int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, uint64_t *ids, int64_t cap);
 /* Finishes the requests already admitted, drops the queued ones, stops the
  * workers and releases everything. */
 void cvl_server_destroy(cvl_server *s);
