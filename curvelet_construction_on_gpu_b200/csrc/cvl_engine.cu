@@ -77,6 +77,11 @@ using PinnedPool = cvl::PinnedArena;
 struct cvl_engine {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // The workspace comes from the engine's own stream-ordered pool: growing a
+    // buffer frees the old one in stream order (cudaFreeAsync) instead of with
+    // cudaFree, which would wait for every stream of the device (other engines'
+    // work included). The pool keeps what it has (release threshold: no limit).
+    cudaMemPool_t pool = nullptr;
     cudaDeviceProp prop{};
     size_t budget = 0;
     size_t held = 0;
@@ -113,7 +118,7 @@ struct cvl_engine {
         size_t want = std::max(bytes, b.bytes + b.bytes / 2);
         want = (want + 255) & ~(size_t)255;
         if (b.p) {
-            cudaFree(b.p);
+            cudaFreeAsync(b.p, stream);
             held -= b.bytes;
             b.p = nullptr;
             b.bytes = 0;
@@ -124,11 +129,12 @@ struct cvl_engine {
                 return fail(CVL_ENOMEM, "device memory budget exceeded (" + std::to_string(held + want) + " > " +
                                             std::to_string(budget) + " bytes)");
         }
-        cudaError_t e = cudaMalloc(&b.p, want);
+        cudaError_t e = cudaMallocFromPoolAsync(&b.p, want, pool, stream);
         if (e != cudaSuccess) {
             b.p = nullptr;
             cudaGetLastError();
-            return fail(CVL_ENOMEM, std::string("cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e));
+            return fail(CVL_ENOMEM, std::string("device allocation of ") + std::to_string(want) +
+                                        " bytes: " + cudaGetErrorString(e));
         }
         b.bytes = want;
         held += want;
@@ -172,7 +178,7 @@ struct cvl_engine {
                        &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
                        &pb_max, &pb_valid};
         for (DBuf *b : all) {
-            if (b->p) cudaFree(b->p);
+            if (b->p) cudaFreeAsync(b->p, stream);
             b->p = nullptr;
             b->bytes = 0;
         }
@@ -869,11 +875,25 @@ int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out) {
         const int prio = std::min(std::max(c.stream_priority, greatest), least);
         if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, prio);
     }
+    if (ce == cudaSuccess) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = e->device;
+        ce = cudaMemPoolCreate(&e->pool, &props);
+        if (ce == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            ce = cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (ce != cudaSuccess) {
+        if (e->pool) cudaMemPoolDestroy(e->pool);
+        if (e->stream) cudaStreamDestroy(e->stream);
         delete e;
         return fail(CVL_ECUDA, std::string("engine init: ") + cudaGetErrorString(ce));
     }
     if (e->prop.major < 10) {
+        cudaMemPoolDestroy(e->pool);
         cudaStreamDestroy(e->stream);
         delete e;
         return fail(CVL_ENODEV, "device is not sm_100 class (the library is built for sm_100a only)");
@@ -888,9 +908,11 @@ void cvl_engine_destroy(cvl_engine *e) {
     cudaStreamSynchronize(e->stream);
     while (!e->batches.empty()) cvl_batch_free(e->batches.back());
     e->release_all();
+    cudaStreamSynchronize(e->stream);
     for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
     if (e->chunk_done) cudaEventDestroy(e->chunk_done);
     cudaStreamDestroy(e->stream);
+    if (e->pool) cudaMemPoolDestroy(e->pool);
     delete e;
 }
 
@@ -1093,13 +1115,13 @@ int cvl_batch_refill_parts(cvl_batch *b, const double *const *parts, const int32
         // synchronise the whole device)
         const size_t want = std::max(eb, b->edges_cap + b->edges_cap / 4);
         if (b->d_edges) {
-            cudaFree(b->d_edges);
+            cudaFreeAsync(b->d_edges, e->stream);
             e->held -= b->edges_cap;
             b->d_edges = nullptr;
             b->edges_cap = 0;
         }
         if (e->budget && e->held + want > e->budget) return fail(CVL_ENOMEM, "batch exceeds the device memory budget");
-        if (cudaMalloc(&b->d_edges, want) != cudaSuccess) {
+        if (cudaMallocFromPoolAsync(&b->d_edges, want, e->pool, e->stream) != cudaSuccess) {
             cudaGetLastError();
             b->d_edges = nullptr;
             return fail(CVL_ENOMEM, "batch allocation failed");
@@ -1109,10 +1131,10 @@ int cvl_batch_refill_parts(cvl_batch *b, const double *const *parts, const int32
     }
     if ((size_t)mo.size() > b->map_off_cap) {
         const size_t want = std::max(mo.size(), b->map_off_cap * 2);
-        if (b->d_map_off) cudaFree(b->d_map_off);
+        if (b->d_map_off) cudaFreeAsync(b->d_map_off, e->stream);
         b->d_map_off = nullptr;
         b->map_off_cap = 0;
-        if (cudaMalloc(&b->d_map_off, sizeof(int) * want) != cudaSuccess) {
+        if (cudaMallocFromPoolAsync(&b->d_map_off, sizeof(int) * want, e->pool, e->stream) != cudaSuccess) {
             cudaGetLastError();
             b->d_map_off = nullptr;
             return fail(CVL_ENOMEM, "batch allocation failed");
@@ -1175,10 +1197,10 @@ void cvl_batch_free(cvl_batch *b) {
     bs.erase(std::remove(bs.begin(), bs.end(), b), bs.end());
     cudaSetDevice(b->eng->device);
     if (b->d_edges) {
-        cudaFree(b->d_edges);
+        cudaFreeAsync(b->d_edges, b->eng->stream);
         b->eng->held -= b->edges_cap;
     }
-    if (b->d_map_off) cudaFree(b->d_map_off);
+    if (b->d_map_off) cudaFreeAsync(b->d_map_off, b->eng->stream);
     delete b;
 }
 
