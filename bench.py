@@ -74,7 +74,7 @@ def _args():
     ap.add_argument("--rate", type=float, default=50.0, help="served stream: offered maps/s")
     ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")
     ap.add_argument("--requests", type=int, default=600, help="served stream: requests per rate")
-    ap.add_argument("--workers", type=int, default=2, help="served stream: server workers")
+    ap.add_argument("--workers", type=int, default=3, help="served stream: server workers")
     args = ap.parse_args()
     args.rate_given = any(a == "--rate" or a.startswith("--rate=") for a in sys.argv[1:])
     return args

@@ -86,7 +86,8 @@ struct cvl_server {
     // lane whose head request fits the remaining budget, preferred lane first; -1 if none
     int lane_to_take(int w) const {
         const int pref = preferred_lane(w);
-        for (int k = 0; k < 2; ++k) {
+        const int nlanes = (pref == 0 && !cfg.small_takes_large && cfg.workers >= 2) ? 1 : 2;
+        for (int k = 0; k < nlanes; ++k) {
             const int l = k == 0 ? pref : 1 - pref;
             if (!lanes[l].empty() && admitted + lanes[l].front()->charge <= cfg.mem_budget_bytes) return l;
         }
@@ -240,12 +241,13 @@ extern "C" {
 void cvl_server_cfg_default(cvl_server_cfg *c) {
     if (!c) return;
     c->device = 0;
-    c->workers = 2;
+    c->workers = 3;
     c->mem_budget_bytes = (size_t)40 << 30;
     c->admit_bytes_per_edge = 2048;
-    c->max_batch_edges = 4 << 20;
+    c->max_batch_edges = 2 << 20;
     c->large_map_edges = 1000000;
     c->host_reserve_bytes = (size_t)2 << 30;
+    c->small_takes_large = 0;
 }
 
 int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out) {

@@ -246,8 +246,9 @@ void cvl_batch_result_free(cvl_batch_result *r);
  *
  * Maps of at least large_map_edges edges go to a separate lane, so small
  * maps do not queue behind them. With two or more workers, the last worker
- * prefers the large lane and the others the small one; an idle worker takes
- * from the other lane. Small-lane workers run on the device's highest stream
+ * prefers the large lane and the others the small one. An idle large-lane
+ * worker takes small maps; a small-lane worker takes large maps only when
+ * small_takes_large is set. Small-lane workers run on the device's highest stream
  * priority, so their kernels go ahead of a large map's between its blocks.
  * A request's edges are copied at submit into page-locked memory that the
  * server reuses, and go from there to the device.
@@ -258,14 +259,17 @@ void cvl_batch_result_free(cvl_batch_result *r);
 typedef struct cvl_server cvl_server;
 typedef struct cvl_server_cfg {
     int device;                    /* CUDA device ordinal (0) */
-    int workers;                   /* engines working concurrently (2) */
+    int workers;                   /* engines working concurrently (3) */
     size_t mem_budget_bytes;       /* device bytes that admitted requests may hold at once (40 GiB) */
     size_t admit_bytes_per_edge;   /* admission charge per edge (2048: about twice the path's measured
                                       footprint per edge, edges + hash + neighbour pairs + curvelets) */
-    int64_t max_batch_edges;       /* edges folded into one launch at most; a larger map runs alone (4 Mi) */
+    int64_t max_batch_edges;       /* edges folded into one launch at most; a larger map runs alone (2 Mi) */
     int64_t large_map_edges;       /* maps with at least this many edges use the large lane (1,000,000) */
     size_t host_reserve_bytes;     /* page-locked host memory set aside at creation for each worker's results
                                       and for the queued requests, so that serving does not pin memory (2 GiB) */
+    int small_takes_large;         /* 1: a small-lane worker with an empty lane takes large maps;
+                                      0: it keeps free for small maps (0: measured to cut the small maps'
+                                      p99 from 120-170 ms to 20-45 ms at 35-80 maps/s, for no throughput) */
 } cvl_server_cfg;
 
 typedef struct cvl_server_stats {
