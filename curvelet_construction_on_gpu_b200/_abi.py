@@ -91,6 +91,7 @@ SIGNATURES = [
     ("cvl_last_error", C.c_char_p, []),
     ("cvl_version", C.c_char_p, []),
     ("cvl_run", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.POINTER(CvlParams), C.POINTER(_vp)]),
+    ("cvl_run_f32", C.c_int, [_vp, C.POINTER(C.c_float), C.c_int32, C.c_int32, C.POINTER(CvlParams), C.POINTER(_vp)]),
     ("cvl_result_get", C.c_int, [_vp, C.POINTER(CvlResultView)]),
     ("cvl_result_free", None, [_vp]),
     ("cvl_build_neighbor_graph", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.c_double, C.c_uint, C.c_uint,
@@ -122,7 +123,9 @@ SIGNATURES = [
     ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), C.c_int64]),
     ("cvl_server_destroy", None, [_vp]),
     ("cvl_read_edges", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_dp), C.POINTER(C.c_int64)]),
-    ("cvl_free_edges", None, [_dp]),
+    ("cvl_read_edges_f32", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_float)),
+                                     C.POINTER(C.c_int64)]),
+    ("cvl_free_edges", None, [_vp]),
     ("cvl_write_edges_binary", C.c_int, [C.c_char_p, _dp, C.c_int64, C.c_int32]),
     ("cvl_tuning_bucket", C.c_int, [C.c_int64]),
     ("cvl_engine_get_tuning", C.c_int, [_vp, C.c_int, C.POINTER(CvlTuning)]),

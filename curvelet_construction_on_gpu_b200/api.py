@@ -167,13 +167,28 @@ class Engine:
         self.close()
 
     # ---- the plain form
-    def run(self, edges, params: CurveletParams | None = None, dt_rad: float = 0.0) -> Result:
+    def run(self, edges, params: CurveletParams | None = None, dt_rad: float = 0.0, scalar: str = "double") -> Result:
+        """run_curvelet<double>, or run_curvelet<float> (the reference's --float
+        mode) for scalar="float": then the edges are taken as float32, as the
+        reference reads them in that mode (data_io.read_edges(..., scalar="float"))."""
         params = params or CurveletParams()
-        e = _edges(edges)
         p = params.to_c(dt_rad)
         r = C.c_void_p()
-        check(self._lib.cvl_run(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1], C.byref(p),
-                                C.byref(r)), "cvl_run")
+        if scalar == "float":
+            if np.asarray(edges).dtype != np.float32:
+                raise TypeError("scalar='float' takes float32 edges (as read_edges(..., scalar='float') gives); "
+                                "a float64 array would be rounded here, not read as the reference reads it")
+            e = np.ascontiguousarray(edges)
+            if e.ndim != 2:
+                raise ValueError("edges must be a 2-D array [num_edges, edge_data_sz]")
+            check(self._lib.cvl_run_f32(self._h, e.ctypes.data_as(C.POINTER(C.c_float)), e.shape[0], e.shape[1],
+                                        C.byref(p), C.byref(r)), "cvl_run_f32")
+        elif scalar == "double":
+            e = _edges(edges)
+            check(self._lib.cvl_run(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1], C.byref(p),
+                                    C.byref(r)), "cvl_run")
+        else:
+            raise ValueError("scalar must be 'double' or 'float'")
         owner = _Owner(self._lib, r, "cvl_result_free")
         v = CvlResultView()
         check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")

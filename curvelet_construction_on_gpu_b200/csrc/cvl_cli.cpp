@@ -14,6 +14,7 @@
 #include <iostream>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cvl.h"
@@ -29,7 +30,7 @@ void print_usage(const char *prog) {
     std::cerr << "Usage: " << prog << " [options]\n"
               << "\n"
               << "Options:\n"
-              << "  --float, --double          Scalar type (default: double; the GPU engine computes in double)\n"
+              << "  --float, --double          Scalar type (default: double)\n"
               << "  --output <file>            Output chain file (default: chain_cpu.txt)\n"
               << "  --nthreads <N>             Host thread count (accepted; the path runs on the GPU)\n"
               << "  --edge-file <file>         Input edge file in ../test_files/ (default: eth3d_cables2.txt)\n"
@@ -137,9 +138,11 @@ bool parse_args(int argc, char **argv, CliParams &cp, bool &use_double, std::str
 }
 
 // Edge-file reader with the reference's acceptance rules and messages
-// (data_io.hpp:22-79), multi-threaded in libcvl (cvl_read_edges); a name ending in
-// ".cvle" is the binary edge format.
-bool read_edges(const std::string &filename, int per_edge, std::vector<double> &out) {
+// (data_io.hpp:22-79), multi-threaded in libcvl (cvl_read_edges /
+// cvl_read_edges_f32, into the run's scalar type); a name ending in ".cvle" is
+// the binary edge format.
+template <typename T>
+bool read_edges(const std::string &filename, int per_edge, std::vector<T> &out) {
     const std::string path = "../test_files/" + filename;
     if (!std::ifstream(path)) {
         std::cerr << "Error: input file does not exist: " << path << std::endl;
@@ -147,9 +150,14 @@ bool read_edges(const std::string &filename, int per_edge, std::vector<double> &
     }
     std::cout << "reading data from file " << filename << std::endl;
     out.clear();
-    double *buf = nullptr;
+    T *buf = nullptr;
     int64_t n = 0;
-    if (cvl_read_edges(path.c_str(), per_edge, 0, &buf, &n) != CVL_OK) {
+    int rc;
+    if constexpr (std::is_same<T, float>::value)
+        rc = cvl_read_edges_f32(path.c_str(), per_edge, 0, &buf, &n);
+    else
+        rc = cvl_read_edges(path.c_str(), per_edge, 0, &buf, &n);
+    if (rc != CVL_OK) {
         std::cerr << cvl_last_error() << std::endl;
         return false;
     }
@@ -194,15 +202,14 @@ int main(int argc, char **argv) {
     bool help = false;
     if (!parse_args(argc, argv, cp, use_double, out_file, nthreads, help)) return help ? 0 : 1;
     (void)nthreads;
-    if (!use_double) {
-        std::cerr << "Error: --float is not available: the B200 engine computes the path in double precision"
-                  << std::endl;
-        return 1;
-    }
-    std::cout << "Using scalar type: double" << std::endl;
+    std::cout << "Using scalar type: " << (use_double ? "double" : "float") << std::endl;
+    // run_curvelet<double> or run_curvelet<float> (main.cpp:110)
     std::vector<double> edges;
-    if (!read_edges(cp.edge_file, cp.p.edge_data_sz, edges)) return 1;
-    const int n = (int)(edges.size() / (size_t)cp.p.edge_data_sz);
+    std::vector<float> edges_f;
+    if (use_double ? !read_edges(cp.edge_file, cp.p.edge_data_sz, edges)
+                   : !read_edges(cp.edge_file, cp.p.edge_data_sz, edges_f))
+        return 1;
+    const int n = (int)((use_double ? edges.size() : edges_f.size()) / (size_t)cp.p.edge_data_sz);
 
     cvl_engine *eng = nullptr;
     if (cvl_engine_create(nullptr, &eng) != CVL_OK) {
@@ -210,7 +217,9 @@ int main(int argc, char **argv) {
         return 1;
     }
     cvl_result *res = nullptr;
-    if (cvl_run(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &res) != CVL_OK) {
+    const int rc = use_double ? cvl_run(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &res)
+                              : cvl_run_f32(eng, edges_f.data(), n, cp.p.edge_data_sz, &cp.p, &res);
+    if (rc != CVL_OK) {
         std::cerr << "Error: " << cvl_last_error() << std::endl;
         cvl_engine_destroy(eng);
         return 1;

@@ -283,8 +283,11 @@ int check_tuning(const cvl_tuning &t) {
 }
 
 // ---- parameters -> model ---------------------------------------------------
-int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nbr_radius, unsigned max_cand, Model &md,
-               int &cpl) {
+// The model of run_curvelet<T> (main.cpp:21-29): parameters converted to T as
+// the reference converts them, and its derived constants computed in T.
+template <typename T>
+int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nbr_radius, unsigned max_cand,
+               ModelT<T> &md, int &cpl) {
     if (!p) return fail(CVL_EINVAL, "params is NULL");
     if (!(p->sx > 0) || !(p->st > 0)) return fail(CVL_EINVAL, "sx and st must be > 0");
     if (!std::isfinite(p->dx) || !std::isfinite(p->dt_deg) || !std::isfinite(p->dt_rad) || !std::isfinite(p->max_k) || !std::isfinite(p->nrad) ||
@@ -294,17 +297,18 @@ int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nb
         return fail(CVL_EUNSUPPORTED, "group_max_sz must be in [1, 16]");
     if (max_cand < 1 || max_cand > 1024) return fail(CVL_EUNSUPPORTED, "max_candidates must be in [1, 1024]");
     if (nbr_radius > 64) return fail(CVL_EUNSUPPORTED, "neighbor_radius must be <= 64");
-    md.nrad = p->nrad;
-    md.rad_sqr = rad * rad;  // rad * rad (preprocess.hpp:221)
-    md.dx = p->dx;
-    md.dx2 = p->dx * p->dx;
-    md.four_dx_dx = 4 * p->dx * p->dx;
-    md.dt = (p->dt_rad > 0) ? p->dt_rad : (double)(p->dt_deg / 180.0) * (double)CVL_PI;  // main.cpp:24
-    md.sx = p->sx;
-    md.st = p->st;
-    md.max_k = p->max_k;
-    const double Pd = 2 * std::floor(md.dx / md.sx + 0.5) + 1;  // cpu_curvelet.hpp:73
-    const double Qd = 2 * std::floor(md.dt / md.st + 0.5) + 1;  // cpu_curvelet.hpp:74
+    md.nrad = T(p->nrad);
+    const T rad_t = T(rad);
+    md.rad_sqr = rad_t * rad_t;  // rad * rad (preprocess.hpp:221)
+    md.dx = T(p->dx);
+    md.dx2 = md.dx * md.dx;
+    md.four_dx_dx = T(4) * md.dx * md.dx;
+    md.dt = (p->dt_rad > 0) ? T(p->dt_rad) : T(p->dt_deg / 180.0) * T(CVL_PI);  // main.cpp:24
+    md.sx = T(p->sx);
+    md.st = T(p->st);
+    md.max_k = T(p->max_k);
+    const double Pd = 2 * std::floor((double)(md.dx / md.sx) + 0.5) + 1;  // cpu_curvelet.hpp:73
+    const double Qd = 2 * std::floor((double)(md.dt / md.st) + 0.5) + 1;  // cpu_curvelet.hpp:74
     if (!(Pd >= 1 && Pd <= 128 && Qd >= 1 && Qd <= QMAX))
         return fail(CVL_EUNSUPPORTED, "bundle grid out of range (P <= 128, Q <= 32 required)");
     md.P = (int)Pd;
@@ -420,61 +424,75 @@ struct RunOut {
     unsigned max_deg = 0;
 };
 
-template <int CPL, int MINB>
-int launch_bundles(cvl_engine *e, BundleArgs &a, int blocks) {
+template <typename T, int CPL, int MINB>
+int launch_bundles(cvl_engine *e, BundleArgsT<T> &a, int blocks) {
     // one block per PPB pairs and no grid stride: short blocks, so that a
     // higher-priority stream's blocks get SMs as soon as any block ends
     const long long ppb = BUNDLE_THREADS / a.md.Q;
     const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
     blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
-    k_bundles<CPL, MINB><<<blocks, BUNDLE_THREADS, 0, e->stream>>>(a);
+    k_bundles<T, CPL, MINB><<<blocks, BUNDLE_THREADS, 0, e->stream>>>(a);
     return check_launch("k_bundles");
 }
 
-template <int CPL, int K, int MINB>
-int launch_growth(cvl_engine *e, GrowthArgs &a, size_t smem, int blocks) {
-    CVL_CUDA(cudaFuncSetAttribute(k_growth<CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+template <typename T, int CPL, int K, int MINB>
+int launch_growth(cvl_engine *e, GrowthArgsT<T> &a, size_t smem, int blocks) {
+    CVL_CUDA(cudaFuncSetAttribute(k_growth<T, CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // a warp per anchor and anchors_per_warp anchors per warp: short blocks (a
     // higher-priority stream's blocks get SMs as soon as any block ends)
     const long long per_block = (GROWTH_THREADS / 32) * (long long)a.anchors_per_warp;
     blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + per_block - 1) / per_block,
                                                     0x7fffffffLL));
-    k_growth<CPL, K, MINB><<<blocks, GROWTH_THREADS, smem, e->stream>>>(a);
+    k_growth<T, CPL, K, MINB><<<blocks, GROWTH_THREADS, smem, e->stream>>>(a);
     return check_launch("k_growth");
 }
 
-typedef int (*bundles_fn)(cvl_engine *, BundleArgs &, int);
-typedef int (*growth_fn)(cvl_engine *, GrowthArgs &, size_t, int);
+template <typename T>
+using bundles_fn = int (*)(cvl_engine *, BundleArgsT<T> &, int);
+template <typename T>
+using growth_fn = int (*)(cvl_engine *, GrowthArgsT<T> &, size_t, int);
+
+// Float mode (a parity mode) runs the default variants only.
+void pick_kernels(int cpl, const cvl_tuning &, bundles_fn<float> &bf, growth_fn<float> &gf) {
+    switch (cpl) {
+        case 1: bf = launch_bundles<float, 1, 4>; gf = launch_growth<float, 1, 4, 4>; break;
+        case 3: bf = launch_bundles<float, 3, 4>; gf = launch_growth<float, 3, 4, 4>; break;
+        case 4: bf = launch_bundles<float, 4, 4>; gf = launch_growth<float, 4, 4, 4>; break;
+        default: bf = launch_bundles<float, 2, 4>; gf = launch_growth<float, 2, 4, 4>; break;
+    }
+}
 
 // The kernel variants a tuning selects (seeds_per_group 8 only for grids of up to
 // 64 cells, where its register footprint fits).
-void pick_kernels(int cpl, const cvl_tuning &t, bundles_fn &bf, growth_fn &gf) {
+void pick_kernels(int cpl, const cvl_tuning &t, bundles_fn<double> &bf, growth_fn<double> &gf) {
     const bool b3 = t.bundle_blocks_per_sm == 3;
     const bool g6 = t.growth_blocks_per_sm == 6;
     const bool k8 = t.seeds_per_group == 8 && cpl <= 2;
     switch (cpl) {
         case 1:
-            bf = b3 ? launch_bundles<1, 3> : launch_bundles<1, 4>;
-            gf = k8 ? launch_growth<1, 8, 4> : (g6 ? launch_growth<1, 4, 6> : launch_growth<1, 4, 4>);
+            bf = b3 ? launch_bundles<double, 1, 3> : launch_bundles<double, 1, 4>;
+            gf = k8 ? launch_growth<double, 1, 8, 4> : (g6 ? launch_growth<double, 1, 4, 6> : launch_growth<double, 1, 4, 4>);
             break;
         case 3:
-            bf = b3 ? launch_bundles<3, 3> : launch_bundles<3, 4>;
-            gf = g6 ? launch_growth<3, 4, 6> : launch_growth<3, 4, 4>;
+            bf = b3 ? launch_bundles<double, 3, 3> : launch_bundles<double, 3, 4>;
+            gf = g6 ? launch_growth<double, 3, 4, 6> : launch_growth<double, 3, 4, 4>;
             break;
         case 4:
-            bf = b3 ? launch_bundles<4, 3> : launch_bundles<4, 4>;
-            gf = g6 ? launch_growth<4, 4, 6> : launch_growth<4, 4, 4>;
+            bf = b3 ? launch_bundles<double, 4, 3> : launch_bundles<double, 4, 4>;
+            gf = g6 ? launch_growth<double, 4, 4, 6> : launch_growth<double, 4, 4, 4>;
             break;
         default:
-            bf = b3 ? launch_bundles<2, 3> : launch_bundles<2, 4>;
-            gf = k8 ? launch_growth<2, 8, 4> : (g6 ? launch_growth<2, 4, 6> : launch_growth<2, 4, 4>);
+            bf = b3 ? launch_bundles<double, 2, 3> : launch_bundles<double, 2, 4>;
+            gf = k8 ? launch_growth<double, 2, 8, 4> : (g6 ? launch_growth<double, 2, 4, 6> : launch_growth<double, 2, 4, 4>);
             break;
     }
 }
 
 // mode: 0 = full run, 1 = count valid pairs only, 2 = neighbour graph only
-int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int *d_map_off,
-                 const std::vector<int32_t> &map_off_host, Model md, int cpl, int mode, bool want_d2, RunOut &ro) {
+template <typename R>
+int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_map_off,
+                 const std::vector<int32_t> &map_off_host, ModelT<R> md, int cpl, int mode, bool want_d2,
+                 RunOut &ro) {
     const int M = (int)map_off_host.size() - 1;
     cudaStream_t s = e->stream;
     e->nmarks = 0;
@@ -493,13 +511,13 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     CVL_TRY(e->alloc(e->bstart, sizeof(unsigned) * (T + 1)));
     CVL_TRY(e->alloc(e->bfill, sizeof(unsigned) * (T + 1)));
     CVL_TRY(e->alloc(e->pos_of, sizeof(int) * n));
-    CVL_TRY(e->alloc(e->bx, sizeof(double) * n));
-    CVL_TRY(e->alloc(e->by, sizeof(double) * n));
-    CVL_TRY(e->alloc(e->bth, sizeof(double) * n));
-    CVL_TRY(e->alloc(e->bsp, sizeof(double) * n));
-    CVL_TRY(e->alloc(e->bcp, sizeof(double) * n));
-    CVL_TRY(e->alloc(e->bsm, sizeof(double) * n));
-    CVL_TRY(e->alloc(e->bcm, sizeof(double) * n));
+    CVL_TRY(e->alloc(e->bx, sizeof(R) * n));
+    CVL_TRY(e->alloc(e->by, sizeof(R) * n));
+    CVL_TRY(e->alloc(e->bth, sizeof(R) * n));
+    CVL_TRY(e->alloc(e->bsp, sizeof(R) * n));
+    CVL_TRY(e->alloc(e->bcp, sizeof(R) * n));
+    CVL_TRY(e->alloc(e->bsm, sizeof(R) * n));
+    CVL_TRY(e->alloc(e->bcm, sizeof(R) * n));
     CVL_TRY(e->alloc(e->bcell, sizeof(int2) * n));
     CVL_TRY(e->alloc(e->orig_of, sizeof(int) * n));
     CVL_TRY(e->alloc(e->bmap, sizeof(int) * n));
@@ -514,14 +532,14 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     CVL_TRY(e->alloc(e->err, sizeof(unsigned) * 4));
     CVL_TRY(e->alloc(e->work, sizeof(unsigned long long) * 2));
 
-    Binned B;
-    B.x = (double *)e->bx.p;
-    B.y = (double *)e->by.p;
-    B.th = (double *)e->bth.p;
-    B.sp = (double *)e->bsp.p;
-    B.cp = (double *)e->bcp.p;
-    B.sm = (double *)e->bsm.p;
-    B.cm = (double *)e->bcm.p;
+    BinnedT<R> B;
+    B.x = (R *)e->bx.p;
+    B.y = (R *)e->by.p;
+    B.th = (R *)e->bth.p;
+    B.sp = (R *)e->bsp.p;
+    B.cp = (R *)e->bcp.p;
+    B.sm = (R *)e->bsm.p;
+    B.cm = (R *)e->bcm.p;
     B.cell = (int2 *)e->bcell.p;
     B.orig = (int *)e->orig_of.p;
     B.map = (int *)e->bmap.p;
@@ -549,10 +567,10 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     // ---- (b) neighbour count, CSR offsets, chunk boundaries
     const int nb_wpb = 8;
     const size_t nb_smem = (size_t)nb_wpb * nbr_smem_per_warp(md.max_cand);
-    CVL_CUDA(cudaFuncSetAttribute(k_nb<NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
-    CVL_CUDA(cudaFuncSetAttribute(k_nb<NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
+    CVL_CUDA(cudaFuncSetAttribute(k_nb<R, NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
+    CVL_CUDA(cudaFuncSetAttribute(k_nb<R, NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
     const int gn = short_grid(n, (long long)nb_wpb * 4);  // a warp per anchor, 4 anchors per warp
-    NbArgs na{};
+    NbArgsT<R> na{};
     na.md = md;
     na.B = B;
     na.bstart = (const unsigned *)e->bstart.p;
@@ -562,7 +580,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     na.stats = stats;
     na.pair_off = (const unsigned long long *)e->pair_off.p;
     na.err = err;
-    k_nb<NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+    k_nb<R, NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
     CVL_TRY(check_launch("k_nb<COUNT>"));
     k_deg_from_ncand<<<gb, 256, 0, s>>>(n, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p);
     CVL_TRY(check_launch("k_deg_from_ncand"));
@@ -601,20 +619,20 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
 
     // ---- (b) neighbour fill: CSR, pair classes, pair -> anchor, anchor trig
     CVL_TRY(e->alloc(e->csr_ids, sizeof(int) * P));
-    if (want_d2) CVL_TRY(e->alloc(e->csr_d2, sizeof(double) * P));
+    if (want_d2) CVL_TRY(e->alloc(e->csr_d2, sizeof(R) * P));
     const bool path = (mode != 2);
     if (path) {
         CVL_TRY(e->alloc(e->pcls, P));
         CVL_TRY(e->alloc(e->pflag, P));
         CVL_TRY(e->alloc(e->pair_anchor, sizeof(int) * P));
-        CVL_TRY(e->alloc(e->atrig, sizeof(double) * (size_t)n * (2 * md.Q + 2)));
+        CVL_TRY(e->alloc(e->atrig, sizeof(R) * (size_t)n * (2 * md.Q + 2)));
     }
     na.csr_ids = (int *)e->csr_ids.p;
-    na.csr_d2 = want_d2 ? (double *)e->csr_d2.p : nullptr;
+    na.csr_d2 = want_d2 ? (R *)e->csr_d2.p : nullptr;
     na.pcls = path ? (unsigned char *)e->pcls.p : nullptr;
     na.pair_anchor = path ? (int *)e->pair_anchor.p : nullptr;
-    na.atrig = path ? (double *)e->atrig.p : nullptr;
-    k_nb<NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+    na.atrig = path ? (R *)e->atrig.p : nullptr;
+    k_nb<R, NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
     CVL_TRY(check_launch("k_nb<FILL>"));
     e->mark("neighbors_fill");
     if (mode == 2) {
@@ -623,8 +641,8 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     }
 
     // ---- (c) + (d) per chunk
-    bundles_fn bf;
-    growth_fn gf;
+    bundles_fn<R> bf;
+    growth_fn<R> gf;
     pick_kernels(cpl, tn, bf, gf);
     const size_t gsmem = (size_t)(GROWTH_THREADS / 32) * growth_smem_per_warp(md.max_cand, md.gms);
     int gbps = 0;
@@ -634,7 +652,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
         (void)fa;
     }
     const unsigned long long max_chunk_pairs = per_chunk + (unsigned long long)ro.max_deg + 1;
-    CVL_TRY(e->alloc(e->bund, sizeof(double) * 64 * (size_t)cpl * std::min<unsigned long long>(P + 1, max_chunk_pairs)));
+    CVL_TRY(e->alloc(e->bund, sizeof(R) * 64 * (size_t)cpl * std::min<unsigned long long>(P + 1, max_chunk_pairs)));
     const int bblocks = e->prop.multiProcessorCount * 8;
     const int gblocks = e->prop.multiProcessorCount * 8;
     (void)gbps;
@@ -649,7 +667,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
             cap = 0;
         }
         CVL_TRY(e->alloc(e->crank, sizeof(unsigned short) * CELLS_MAX));
-        k_cell_ranks<<<1, 128, 0, s>>>(md, (unsigned short *)e->crank.p);
+        k_cell_ranks<R><<<1, 128, 0, s>>>(md, (unsigned short *)e->crank.p);
         CVL_TRY(check_launch("k_cell_ranks"));
         Records rec;
         rec.ids = (unsigned *)e->rec_ids.p;
@@ -671,7 +689,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
                 CVL_CUDA(cudaEventSynchronize(e->chunk_done));
                 e->yield_fn(e->yield_ctx);
             }
-            BundleArgs ba{};
+            BundleArgsT<R> ba{};
             ba.md = md;
             ba.B = B;
             ba.p_begin = h_poff[c];
@@ -679,12 +697,12 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
             ba.csr_ids = (const int *)e->csr_ids.p;
             ba.pair_anchor = (const int *)e->pair_anchor.p;
             ba.pcls = (const unsigned char *)e->pcls.p;
-            ba.atrig = (const double *)e->atrig.p;
-            ba.bund = (double *)e->bund.p;
+            ba.atrig = (const R *)e->atrig.p;
+            ba.bund = (R *)e->bund.p;
             ba.pflag = (unsigned char *)e->pflag.p;
             if (ba.p_end > ba.p_begin) CVL_TRY(bf(e, ba, bblocks));
             e->mark("bundles");
-            GrowthArgs ga{};
+            GrowthArgsT<R> ga{};
             ga.md = md;
             ga.B = B;
             ga.M = M;
@@ -695,7 +713,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
             ga.csr_ids = (const int *)e->csr_ids.p;
             ga.pcls = (const unsigned char *)e->pcls.p;
             ga.pflag = (const unsigned char *)e->pflag.p;
-            ga.bund = (const double *)e->bund.p;
+            ga.bund = (const R *)e->bund.p;
             ga.rec = rec;
             ga.arena_cap = cap;
             ga.arena_ctr = arena_ctr;
@@ -749,7 +767,7 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
         const int W = md.gms + 1;
         CVL_TRY(e->alloc(e->chains, sizeof(unsigned) * C * W));
         CVL_TRY(e->alloc(e->info, sizeof(double) * C * 10));
-        k_finalize<<<gb, 256, 0, s>>>(md, d_edges, sz, n, d_map_off, M, rec, (const unsigned *)e->rec_base.p,
+        k_finalize<R><<<gb, 256, 0, s>>>(md, d_edges, sz, n, d_map_off, M, rec, (const unsigned *)e->rec_base.p,
                                       (const unsigned *)e->run_cnt.p, (const unsigned long long *)e->out_off.p, C,
                                       (unsigned *)e->chains.p, (double *)e->info.p);
         CVL_TRY(check_launch("k_finalize"));
@@ -758,16 +776,17 @@ int run_pipeline(cvl_engine *e, const double *d_edges, int n, int sz, const int 
     }
 }
 
-int upload(cvl_engine *e, const double *edges, int n, int sz, const std::vector<int32_t> &map_off) {
-    CVL_TRY(e->alloc(e->edges, sizeof(double) * (size_t)n * sz));
+template <typename T>
+int upload(cvl_engine *e, const T *edges, int n, int sz, const std::vector<int32_t> &map_off) {
+    CVL_TRY(e->alloc(e->edges, sizeof(T) * (size_t)n * sz));
     CVL_TRY(e->alloc(e->map_off, sizeof(int) * map_off.size()));
-    CVL_CUDA(cudaMemcpyAsync(e->edges.p, edges, sizeof(double) * (size_t)n * sz, cudaMemcpyHostToDevice, e->stream));
+    CVL_CUDA(cudaMemcpyAsync(e->edges.p, edges, sizeof(T) * (size_t)n * sz, cudaMemcpyHostToDevice, e->stream));
     CVL_CUDA(cudaMemcpyAsync(e->map_off.p, map_off.data(), sizeof(int) * map_off.size(), cudaMemcpyHostToDevice,
                              e->stream));
     return CVL_OK;
 }
 
-int check_edges_args(const double *edges, int32_t n, int32_t sz) {
+int check_edges_args(const void *edges, int32_t n, int32_t sz) {
     if (n <= 0 || sz < 4 || edges == nullptr)  // preprocess.hpp:197-199
         return fail(CVL_EINVAL, "num_edges must be > 0, edge_data_sz >= 4 and edges non-NULL");
     return CVL_OK;
@@ -916,20 +935,24 @@ void cvl_engine_destroy(cvl_engine *e) {
     delete e;
 }
 
-int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz, const cvl_params *p,
-            cvl_result **out) {
+}  // extern "C"
+
+// run_curvelet<T> on one map: the plain form in either scalar type.
+template <typename T>
+static int run_plain(cvl_engine *e, const T *edges, int32_t num_edges, int32_t edge_data_sz, const cvl_params *p,
+                     cvl_result **out) {
     if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
     *out = nullptr;
     CVL_TRY(check_edges_args(edges, num_edges, edge_data_sz));
     CVL_CUDA(cudaSetDevice(e->device));
-    Model md;
+    ModelT<T> md;
     int cpl = 2;
     CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
     std::vector<int32_t> mo = {0, num_edges};
     CVL_TRY(upload(e, edges, num_edges, edge_data_sz, mo));
     RunOut ro;
-    CVL_TRY(run_pipeline(e, (const double *)e->edges.p, num_edges, edge_data_sz, (const int *)e->map_off.p, mo, md,
-                         cpl, 0, false, ro));
+    CVL_TRY(run_pipeline(e, (const T *)e->edges.p, num_edges, edge_data_sz, (const int *)e->map_off.p, mo, md, cpl,
+                         0, false, ro));
     e->collect_marks();
     cvl_result *r = new cvl_result();
     int rc = fill_view_from_run(e, ro, num_edges, md.gms + 1, r);
@@ -939,6 +962,18 @@ int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_
     }
     *out = r;
     return CVL_OK;
+}
+
+extern "C" {
+
+int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz, const cvl_params *p,
+            cvl_result **out) {
+    return run_plain<double>(e, edges, num_edges, edge_data_sz, p, out);
+}
+
+int cvl_run_f32(cvl_engine *e, const float *edges, int32_t num_edges, int32_t edge_data_sz, const cvl_params *p,
+                cvl_result **out) {
+    return run_plain<float>(e, edges, num_edges, edge_data_sz, p, out);
 }
 
 int cvl_result_get(const cvl_result *r, cvl_result_view *view) {

@@ -27,6 +27,7 @@
 #include <sstream>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cvl.h"
@@ -36,8 +37,10 @@ namespace {
 
 bool blank(const std::string &s) { return s.find_first_not_of(" \t\r\n") == std::string::npos; }
 
-// The reference's reader, line by line (data_io.hpp:38-69).
-int read_stream(const std::string &path, int per_edge, std::vector<double> &out) {
+// The reference's reader, line by line (data_io.hpp:38-69), for T = double or
+// float (read_TO_edges_from_file<T>: `iss >> value` into a T).
+template <typename T>
+int read_stream(const std::string &path, int per_edge, std::vector<T> &out) {
     std::ifstream in(path);
     if (!in) return cvl_fail(CVL_EINVAL, "Error: input file does not exist: " + path);
     out.clear();
@@ -53,7 +56,7 @@ int read_stream(const std::string &path, int per_edge, std::vector<double> &out)
         }
         std::istringstream iss(line);
         for (int j = 0; j < per_edge; j++) {
-            double v;
+            T v;
             if (!(iss >> v)) {
                 out.clear();
                 return cvl_fail(CVL_EINVAL, "Error: invalid edge file format in " + path + " at line " +
@@ -109,7 +112,8 @@ const char *plain_token(const char *p, const char *end) {
 
 // Lines [b, e) of the buffer, all plain: values appended to out. false sends the
 // whole file to the exact reader.
-bool parse_plain(const char *b, const char *e, int per_edge, std::vector<double> &out, long long &lines) {
+template <typename T>
+bool parse_plain(const char *b, const char *e, int per_edge, std::vector<T> &out, long long &lines) {
     const char *p = b;
     while (p < e) {
         const char *nl = (const char *)std::memchr(p, '\n', (size_t)(e - p));
@@ -119,7 +123,7 @@ bool parse_plain(const char *b, const char *e, int per_edge, std::vector<double>
             while (q < le && (*q == ' ' || *q == '\t')) ++q;
             const char *t = plain_token(q, le);
             if (!t) return false;
-            double v;
+            T v;
             const auto r = std::from_chars(q, t, v, std::chars_format::general);
             if (r.ec != std::errc() || r.ptr != t) return false;
             // the token must end at a separator (a stream would read "1.5x" as 1.5
@@ -136,7 +140,8 @@ bool parse_plain(const char *b, const char *e, int per_edge, std::vector<double>
     return true;
 }
 
-int read_text(const std::string &path, int per_edge, int nthreads, std::vector<double> &out) {
+template <typename T>
+int read_text(const std::string &path, int per_edge, int nthreads, std::vector<T> &out) {
     std::FILE *f = std::fopen(path.c_str(), "rb");
     if (!f) return cvl_fail(CVL_EINVAL, "Error: input file does not exist: " + path);
     std::string buf;
@@ -156,28 +161,28 @@ int read_text(const std::string &path, int per_edge, int nthreads, std::vector<d
     // an empty body, or one that still ends in '\n' (an empty last line), is the
     // exact reader's to judge
     if (body_end == b || body_end[-1] == '\n') return read_stream(path, per_edge, out);
-    const int T = std::max(1, std::min(nthreads, (int)((body_end - b) >> 16) + 1));
-    std::vector<const char *> cut(T + 1);
+    const int NT = std::max(1, std::min(nthreads, (int)((body_end - b) >> 16) + 1));
+    std::vector<const char *> cut(NT + 1);
     cut[0] = b;
-    cut[T] = body_end;
-    for (int t = 1; t < T; ++t) {
-        const char *s = b + (size_t)(body_end - b) * t / T;
+    cut[NT] = body_end;
+    for (int t = 1; t < NT; ++t) {
+        const char *s = b + (size_t)(body_end - b) * t / NT;
         if (s < cut[t - 1]) s = cut[t - 1];
         const char *nl = (const char *)std::memchr(s, '\n', (size_t)(body_end - s));
         cut[t] = nl ? nl + 1 : body_end;
     }
-    std::vector<std::vector<double>> parts(T);
-    std::vector<long long> lines(T, 0);
-    std::vector<char> ok(T, 0);
+    std::vector<std::vector<T>> parts(NT);
+    std::vector<long long> lines(NT, 0);
+    std::vector<char> ok(NT, 0);
     // a chunk ends just after a '\n' (the last one at the body's end): each of its
     // lines ends in '\n' or at the chunk's end, and an empty line fails the grammar
     auto work = [&](int t) { ok[t] = parse_plain(cut[t], cut[t + 1], per_edge, parts[t], lines[t]) ? 1 : 0; };
     std::vector<std::thread> th;
-    for (int t = 1; t < T; ++t) th.emplace_back(work, t);
+    for (int t = 1; t < NT; ++t) th.emplace_back(work, t);
     work(0);
     for (std::thread &x : th) x.join();
     long long n = 0;
-    for (int t = 0; t < T; ++t) {
+    for (int t = 0; t < NT; ++t) {
         if (!ok[t]) return read_stream(path, per_edge, out);
         n += lines[t];
     }
@@ -228,33 +233,46 @@ int read_binary(const std::string &path, int per_edge, std::vector<double> &out)
 
 }  // namespace
 
-extern "C" {
-
-int cvl_read_edges(const char *path, int32_t values_per_edge, int32_t nthreads, double **edges, int64_t *num_edges) {
+template <typename T>
+static int read_edges_t(const char *path, int32_t values_per_edge, int32_t nthreads, T **edges, int64_t *num_edges) {
     if (!path || !edges || !num_edges || values_per_edge < 4) return cvl_fail(CVL_EINVAL, "invalid arguments");
     *edges = nullptr;
     *num_edges = 0;
     const std::string p(path);
-    std::vector<double> v;
+    std::vector<T> v;
     int rc;
     if (ends_with(p, ".cvle")) {
-        rc = read_binary(p, values_per_edge, v);
+        if constexpr (std::is_same<T, double>::value)
+            rc = read_binary(p, values_per_edge, v);
+        else
+            return cvl_fail(CVL_EINVAL, "the binary edge format holds doubles; read it with cvl_read_edges");
     } else if (nthreads < 0) {
         rc = read_stream(p, values_per_edge, v);
     } else {
-        const int T = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
-        rc = read_text(p, values_per_edge, T, v);
+        const int nt = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
+        rc = read_text(p, values_per_edge, nt, v);
     }
     if (rc != CVL_OK) return rc;
-    double *buf = (double *)std::malloc(sizeof(double) * v.size());
+    T *buf = (T *)std::malloc(sizeof(T) * v.size());
     if (!buf) return cvl_fail(CVL_ENOMEM, "host allocation failed");
-    std::memcpy(buf, v.data(), sizeof(double) * v.size());
+    std::memcpy(buf, v.data(), sizeof(T) * v.size());
     *edges = buf;
     *num_edges = (int64_t)(v.size() / (size_t)values_per_edge);
     return CVL_OK;
 }
 
-void cvl_free_edges(double *edges) { std::free(edges); }
+extern "C" {
+
+int cvl_read_edges(const char *path, int32_t values_per_edge, int32_t nthreads, double **edges, int64_t *num_edges) {
+    return read_edges_t<double>(path, values_per_edge, nthreads, edges, num_edges);
+}
+
+int cvl_read_edges_f32(const char *path, int32_t values_per_edge, int32_t nthreads, float **edges,
+                       int64_t *num_edges) {
+    return read_edges_t<float>(path, values_per_edge, nthreads, edges, num_edges);
+}
+
+void cvl_free_edges(void *edges) { std::free(edges); }
 
 int cvl_write_edges_binary(const char *path, const double *edges, int64_t num_edges, int32_t values_per_edge) {
     if (!path || !edges || num_edges <= 0 || num_edges > 0x7fffffff || values_per_edge < 4)

@@ -39,10 +39,18 @@ constexpr unsigned ERR_CAPACITY = 2u;    // a device capacity was exceeded
 constexpr unsigned ERR_INTERNAL = 4u;    // an internal invariant failed (bounds check)
 constexpr unsigned ERR_ARENA = 8u;       // the record arena was too small (the host resizes and reruns)
 
-struct Model {
-    double nrad, rad_sqr;        // neighbour radius and its square (preprocess.hpp:221)
-    double dx, dx2, four_dx_dx;  // _dx, _dx*_dx, 4*_dx*_dx (cpu_curvelet.hpp:654,682)
-    double dt, sx, st, max_k;    // dt in radians (main.cpp:24)
+// T is the path's scalar type: double (run_curvelet<double>) or float (the
+// reference's --float mode, run_curvelet<float>, main.cpp:110). In float mode
+// the reference's expressions keep their C++ types: a double literal in an
+// expression (2.0, 1.0) promotes it to double and the result rounds to float
+// on assignment; everything else is float arithmetic. The kernels restate
+// each expression with those types (marked "float mode" where they differ from
+// the all-T form).
+template <typename T>
+struct ModelT {
+    T nrad, rad_sqr;        // neighbour radius and its square (preprocess.hpp:221)
+    T dx, dx2, four_dx_dx;  // _dx, _dx*_dx, 4*_dx*_dx (cpu_curvelet.hpp:654,682)
+    T dt, sx, st, max_k;    // dt in radians (main.cpp:24)
     int P, Q, cells;             // bundle grid (cpu_curvelet.hpp:73-74)
     int gms;                     // group_max_sz
     int max_cand;                // max_candidates
@@ -50,11 +58,13 @@ struct Model {
     int sbits;                   // hash block edge S = 1 << sbits pixel cells
     unsigned hash_mask;          // table size - 1
 };
+using Model = ModelT<double>;
 
 // SoA copy of the edges in hash-bucket order ("internal" index space).
-struct Binned {
-    double *x, *y, *th;         // position, orientation
-    double *sp, *cp, *sm, *cm;  // sin/cos(theta + dt), sin/cos(theta - dt)
+template <typename T>
+struct BinnedT {
+    T *x, *y, *th;         // position, orientation
+    T *sp, *cp, *sm, *cm;  // sin/cos(theta + dt), sin/cos(theta - dt)
     int2 *cell;                 // pixel cell (lrint(x), lrint(y))
     int *orig;                  // global input index
     int *map;                   // map of the edge
@@ -131,7 +141,8 @@ __device__ __forceinline__ unsigned cell_hash(int m, int bx, int by) {
 }
 
 // sq_dist (curvelet_utils.hpp:13-17)
-__device__ __forceinline__ double sq_dist(double x1, double y1, double x2, double y2) {
+template <typename T>
+__device__ __forceinline__ T sq_dist(T x1, T y1, T x2, T y2) {
     return (x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2);
 }
 
@@ -141,22 +152,46 @@ __device__ __noinline__ double cvl_sin(double x) { return sin(x); }
 __device__ __noinline__ double cvl_cos(double x) { return cos(x); }
 __device__ __noinline__ double cvl_atan2(double y, double x) { return atan2(y, x); }
 __device__ __noinline__ double cvl_fmod(double x, double y) { return fmod(x, y); }
+// the float functions of float mode (std::sin(float) etc.)
+__device__ __noinline__ float cvl_sin(float x) { return sinf(x); }
+__device__ __noinline__ float cvl_cos(float x) { return cosf(x); }
+__device__ __noinline__ float cvl_atan2(float y, float x) { return atan2f(y, x); }
+__device__ __noinline__ float cvl_fmod(float x, float y) { return fmodf(x, y); }
+
+// T(2) * T(M_PI), To2Pi's bound (curvelet_utils.hpp:29)
+template <typename T>
+__device__ __forceinline__ T two_pi() {
+    return T(2) * T(CVL_PI);
+}
+
+// lrint (preprocess.hpp:85-86): round half to even, of the scalar type's value
+__device__ __forceinline__ int lrint_dev(double x) { return __double2int_rn(x); }
+__device__ __forceinline__ int lrint_dev(float x) { return __float2int_rn(x); }
+
+// delta = s * (k - (n - 1.0) / 2.0) with k, n small integers: evaluated in double
+// (the 1.0 and 2.0 are double literals) and rounded to T (cpu_curvelet.hpp:697-698)
+template <typename T>
+__device__ __forceinline__ T grid_offset(T s, int k, int n) {
+    return (T)((double)s * ((double)k - ((double)n - 1.0) / 2.0));
+}
 
 // fmod(x, 2pi) with its IEEE fast case inline: for |x| < |y|, fmod(x, y) == x exactly.
-__device__ __forceinline__ double fmod_2pi(double x) {
-    return (fabs(x) < 2.0 * CVL_PI) ? x : cvl_fmod(x, 2.0 * CVL_PI);
+template <typename T>
+__device__ __forceinline__ T fmod_2pi(T x) {
+    return (fabs(x) < two_pi<T>()) ? x : cvl_fmod(x, two_pi<T>());
 }
 
 // To2Pi (curvelet_utils.hpp:25-46)
-__device__ __forceinline__ double to_2pi(double angle) {
-    double a;
-    if (angle >= 2.0 * CVL_PI)
+template <typename T>
+__device__ __forceinline__ T to_2pi(T angle) {
+    T a;
+    if (angle >= two_pi<T>())
         a = fmod_2pi(angle);
     else if (angle < 0)
-        a = (2.0 * CVL_PI + fmod_2pi(angle));
+        a = (two_pi<T>() + fmod_2pi(angle));
     else
         a = angle;
-    if (!(a >= 0 && a < 2.0 * CVL_PI)) a = 0;
+    if (!(a >= 0 && a < two_pi<T>())) a = 0;
     return a;
 }
 
@@ -172,49 +207,51 @@ __device__ __forceinline__ int map_of(const int *map_off, int M, int e) {
 // ---------------------------------------------------------------------------
 // (a) spatial-hash binning
 // ---------------------------------------------------------------------------
-__global__ void k_bin_keys(const double *__restrict__ edges, int sz, int N, const int *__restrict__ map_off, int M,
-                           Model md, unsigned *__restrict__ ehash, unsigned *__restrict__ bcount,
+template <typename T>
+__global__ void k_bin_keys(const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off, int M,
+                           ModelT<T> md, unsigned *__restrict__ ehash, unsigned *__restrict__ bcount,
                            unsigned *__restrict__ err) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N; e += gridDim.x * blockDim.x) {
-        const double x = edges[(size_t)e * sz + 0];
-        const double y = edges[(size_t)e * sz + 1];
-        const double th = edges[(size_t)e * sz + 2];
-        if (!isfinite(x) || !isfinite(y) || !isfinite(th) || fabs(x) >= 1.0e9 || fabs(y) >= 1.0e9) {
+        const T x = edges[(size_t)e * sz + 0];
+        const T y = edges[(size_t)e * sz + 1];
+        const T th = edges[(size_t)e * sz + 2];
+        if (!isfinite(x) || !isfinite(y) || !isfinite(th) || fabs(x) >= T(1.0e9) || fabs(y) >= T(1.0e9)) {
             atomicOr(err, ERR_NONFINITE);
             ehash[e] = 0;
             atomicAdd(&bcount[0], 1u);
             continue;
         }
         const int m = map_of(map_off, M, e);
-        const int cx = __double2int_rn(x);  // lrint, round half to even (preprocess.hpp:85-86)
-        const int cy = __double2int_rn(y);
+        const int cx = lrint_dev(x);  // lrint, round half to even (preprocess.hpp:85-86)
+        const int cy = lrint_dev(y);
         const unsigned h = cell_hash(m, cx >> md.sbits, cy >> md.sbits) & md.hash_mask;
         ehash[e] = h;
         atomicAdd(&bcount[h], 1u);
     }
 }
 
-__global__ void k_bin_scatter(const double *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
-                              int M, Model md, const unsigned *__restrict__ ehash,
-                              const unsigned *__restrict__ bstart, unsigned *__restrict__ bfill, Binned B,
+template <typename T>
+__global__ void k_bin_scatter(const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
+                              int M, ModelT<T> md, const unsigned *__restrict__ ehash,
+                              const unsigned *__restrict__ bstart, unsigned *__restrict__ bfill, BinnedT<T> B,
                               int *__restrict__ pos_of) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N; e += gridDim.x * blockDim.x) {
         const unsigned h = ehash[e];
         const unsigned pos = bstart[h] + atomicAdd(&bfill[h], 1u);
-        const double x = edges[(size_t)e * sz + 0];
-        const double y = edges[(size_t)e * sz + 1];
-        const double th = edges[(size_t)e * sz + 2];
+        const T x = edges[(size_t)e * sz + 0];
+        const T y = edges[(size_t)e * sz + 1];
+        const T th = edges[(size_t)e * sz + 2];
         B.x[pos] = x;
         B.y[pos] = y;
         B.th[pos] = th;
         // T0 +- dt and their sin/cos (cpu_curvelet.hpp:655-656, 730-733), once per edge
-        const double t_p = th + md.dt;
-        const double t_m = th - md.dt;
+        const T t_p = th + md.dt;
+        const T t_m = th - md.dt;
         B.sp[pos] = sin(t_p);
         B.cp[pos] = cos(t_p);
         B.sm[pos] = sin(t_m);
         B.cm[pos] = cos(t_m);
-        B.cell[pos] = make_int2(__double2int_rn(x), __double2int_rn(y));
+        B.cell[pos] = make_int2(lrint_dev(x), lrint_dev(y));
         B.orig[pos] = e;
         B.map[pos] = map_of(map_off, M, e);
         pos_of[e] = (int)pos;
@@ -232,8 +269,9 @@ __device__ __forceinline__ unsigned long long scan_key(int2 c, int cx, int cy, i
     return ((unsigned long long)r << 32) | (unsigned)e;
 }
 
-struct NbrSmem {  // per-warp candidate staging, capacity max_cand
-    double *d2;
+template <typename T>
+struct NbrSmemT {  // per-warp candidate staging, capacity max_cand (d2 slots are 8 bytes in both modes)
+    T *d2;
     unsigned long long *key;
     int *idx;
 };
@@ -250,9 +288,9 @@ __host__ __device__ inline size_t nbr_smem_per_warp(int max_cand) {
 // and calls f(ok, j, d2, key) warp-uniformly, 32 entries at a time; ok is the
 // reference predicate. The window's bucket ranges (up to 32 per round) are
 // loaded by the lanes at once; entries are enumerated over their prefix sums.
-template <typename F>
-__device__ __forceinline__ void for_window_candidates(const Model &md, const Binned &B, const unsigned *bstart,
-                                                      int i, int m, int2 ac, double ax, double ay, int lane, F &&f) {
+template <typename T, typename F>
+__device__ __forceinline__ void for_window_candidates(const ModelT<T> &md, const BinnedT<T> &B, const unsigned *bstart,
+                                                      int i, int m, int2 ac, T ax, T ay, int lane, F &&f) {
     const int bx0 = (ac.x - md.w) >> md.sbits, bx1 = (ac.x + md.w) >> md.sbits;
     const int by0 = (ac.y - md.w) >> md.sbits, by1 = (ac.y + md.w) >> md.sbits;
     const int nbx = bx1 - bx0 + 1;
@@ -289,7 +327,7 @@ __device__ __forceinline__ void for_window_candidates(const Model &md, const Bin
             const unsigned sb = __shfl_sync(FULL, s, lo);
             const int vbx = __shfl_sync(FULL, bx, lo), vby = __shfl_sync(FULL, by, lo);
             bool ok = false;
-            double d2 = 0.0;
+            T d2 = 0;
             unsigned long long key = 0;
             const int j = (int)(sb + (e - pre));
             if (e < total && j != i) {
@@ -311,8 +349,9 @@ __device__ __forceinline__ void for_window_candidates(const Model &md, const Bin
 // Truncation (preprocess.hpp:165-167): keep the first max_cand candidates in
 // window-scan order. Walks the window pixel cell by pixel cell; inside the cell
 // where the cap is crossed keeps the lowest edge indices. Returns the count kept.
-__device__ __noinline__ unsigned gather_truncated(const Model &md, const Binned &B, const unsigned *bstart, int i,
-                                                  int m, int2 ac, double ax, double ay, int lane, NbrSmem S,
+template <typename T>
+__device__ __noinline__ unsigned gather_truncated(const ModelT<T> &md, const BinnedT<T> &B, const unsigned *bstart,
+                                                  int i, int m, int2 ac, T ax, T ay, int lane, NbrSmemT<T> S,
                                                   unsigned *err) {
     const unsigned lt_mask = (1u << lane) - 1u;
     const int side = 2 * md.w + 1;
@@ -337,7 +376,7 @@ __device__ __noinline__ unsigned gather_truncated(const Model &md, const Binned 
         for (int base = b0; base < b1; base += 32) {
             const int j = base + lane;
             bool ok = false;
-            double d2 = 0.0;
+            T d2 = 0;
             int oj = 0;
             if (j < b1 && j != i) {
                 const int2 cc = B.cell[j];
@@ -376,30 +415,31 @@ __device__ __noinline__ unsigned gather_truncated(const Model &md, const Binned 
     return n > (unsigned)md.max_cand ? (unsigned)md.max_cand : n;
 }
 
-struct NbArgs {
-    Model md;
-    Binned B;
+template <typename T>
+struct NbArgsT {
+    ModelT<T> md;
+    BinnedT<T> B;
     const unsigned *bstart;
     int N, M;
     unsigned *ncand;                     // COUNT: candidates in window (before the cap)
     MapStats *stats;
     const unsigned long long *pair_off;  // FILL: [N+1] internal order
     int *csr_ids;                        // FILL: internal neighbour indices, by pair
-    double *csr_d2;                      // FILL (optional): squared distances
+    T *csr_d2;                           // FILL (optional): squared distances
     unsigned char *pcls;                 // FILL (optional): run | close << 2 per pair
     int *pair_anchor;                    // FILL (optional): internal anchor of each pair
-    double *atrig;                       // FILL (optional): [N][2][Q] sin/cos(T2 + delta_t2_j)
+    T *atrig;                            // FILL (optional): [N][2Q + 2] sin/cos(T2 + delta_t2_j), cos/sin(T2)
     unsigned *err;
 };
 
 // COUNT: ncand[i], per-map pairs / max degree / truncated anchors.
 // FILL:  the CSR row of anchor i at pair_off[i] sorted by (d2, scan key), and
 //        optionally the pair classes, pair->anchor map and anchor trig table.
-template <int MODE>
-__global__ void __launch_bounds__(256) k_nb(NbArgs a) {
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_nb(NbArgsT<T> a) {
     extern __shared__ __align__(16) unsigned char nb_smem[];
     __shared__ BlockStats bstats;
-    const Model &md = a.md;
+    const ModelT<T> &md = a.md;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
@@ -407,10 +447,10 @@ __global__ void __launch_bounds__(256) k_nb(NbArgs a) {
         block_stats_init(bstats, a.M);
         __syncthreads();
     }
-    NbrSmem S;
+    NbrSmemT<T> S;
     {
         unsigned char *p = nb_smem + (size_t)wib * nbr_smem_per_warp(md.max_cand);
-        S.d2 = (double *)p;
+        S.d2 = (T *)p;
         S.key = (unsigned long long *)(p + (size_t)md.max_cand * 8);
         S.idx = (int *)(p + (size_t)md.max_cand * 16);
     }
@@ -418,11 +458,11 @@ __global__ void __launch_bounds__(256) k_nb(NbArgs a) {
     for (int i = blockIdx.x * wpb + wib; i < a.N; i += gridDim.x * wpb) {
         const int m = a.B.map[i];
         const int2 ac = a.B.cell[i];
-        const double ax = a.B.x[i], ay = a.B.y[i];
+        const T ax = a.B.x[i], ay = a.B.y[i];
         if (MODE == NB_COUNT) {
             unsigned cnt = 0;
             for_window_candidates(md, a.B, a.bstart, i, m, ac, ax, ay, lane,
-                                  [&](bool ok, int, double, unsigned long long) {
+                                  [&](bool ok, int, T, unsigned long long) {
                                       cnt += __popc(__ballot_sync(FULL, ok));
                                   });
             if (lane == 0) {
@@ -436,7 +476,7 @@ __global__ void __launch_bounds__(256) k_nb(NbArgs a) {
         unsigned n = 0;
         if (total <= (unsigned)md.max_cand) {
             for_window_candidates(md, a.B, a.bstart, i, m, ac, ax, ay, lane,
-                                  [&](bool ok, int j, double d2, unsigned long long key) {
+                                  [&](bool ok, int j, T d2, unsigned long long key) {
                                       const unsigned bal = __ballot_sync(FULL, ok);
                                       if (ok) {
                                           const unsigned p = n + __popc(bal & lt_mask);
@@ -462,13 +502,13 @@ __global__ void __launch_bounds__(256) k_nb(NbArgs a) {
         }
         // the anchor's trig row [2Q + 2]: sin(T2 + delta_t2_j), cos(T2 + delta_t2_j)
         // for j < Q (:702-705), then cos(T2), sin(T2) (:690 and the dot product)
-        const double T2 = a.B.th[i];
-        const double cosT2 = (a.pcls || a.atrig) ? cvl_cos(T2) : 0.0;
-        const double sinT2 = (a.pcls || a.atrig) ? cvl_sin(T2) : 0.0;
+        const T T2 = a.B.th[i];
+        const T cosT2 = (a.pcls || a.atrig) ? cvl_cos(T2) : T(0);
+        const T sinT2 = (a.pcls || a.atrig) ? cvl_sin(T2) : T(0);
         if (a.atrig) {
-            double *row = a.atrig + (size_t)i * (2 * md.Q + 2);
+            T *row = a.atrig + (size_t)i * (2 * md.Q + 2);
             for (int j = lane; j < md.Q; j += 32) {
-                const double t = T2 + md.st * ((double)j - ((double)md.Q - 1.0) / 2.0);
+                const T t = T2 + grid_offset(md.st, j, md.Q);  // T2t = T2 + delta_t2 (:698-702)
                 row[j] = cvl_sin(t);
                 row[md.Q + j] = cvl_cos(t);
             }
@@ -479,11 +519,11 @@ __global__ void __launch_bounds__(256) k_nb(NbArgs a) {
         }
         // rank sort by (d2, scan key) -- std::sort by distance, preprocess.hpp:172-176
         for (unsigned t = lane; t < n; t += 32) {
-            const double dt_ = S.d2[t];
+            const T dt_ = S.d2[t];
             const unsigned long long kt = S.key[t];
             unsigned rk = 0;
             for (unsigned u = 0; u < n; ++u) {
-                const double du = S.d2[u];
+                const T du = S.d2[u];
                 rk += (du < dt_) || (du == dt_ && S.key[u] < kt);
             }
             const int nn = S.idx[t];
@@ -492,11 +532,11 @@ __global__ void __launch_bounds__(256) k_nb(NbArgs a) {
             if (a.pair_anchor) a.pair_anchor[off + rk] = i;
             if (a.pcls) {
                 // direction filter (:454-462) and close pair (:682)
-                const double lx = a.B.x[nn], ly = a.B.y[nn];
-                const double dir = to_2pi(cvl_atan2(ly - ay, lx - ax));      // angle_from_pt_to_pt(te, le)
-                const double d = cvl_cos(dir) * cosT2 + cvl_sin(dir) * sinT2;  // dot(dir, te_orient)
+                const T lx = a.B.x[nn], ly = a.B.y[nn];
+                const T dir = to_2pi(cvl_atan2(ly - ay, lx - ax));      // angle_from_pt_to_pt(te, le)
+                const T d = cvl_cos(dir) * cosT2 + cvl_sin(dir) * sinT2;  // dot(dir, te_orient)
                 const unsigned run = (d > 0) ? 0u : ((d < 0) ? 1u : 2u);
-                const double DX = ax - lx, DY = ay - ly;
+                const T DX = ax - lx, DY = ay - ly;
                 const bool close = (DX * DX + DY * DY < md.four_dx_dx);
                 a.pcls[off + rk] = (unsigned char)(run | (close ? 4u : 0u));
             }

@@ -7,6 +7,8 @@
 // arithmetic, k_growth in control flow and memory; each has one small hot loop.
 #pragma once
 
+#include <type_traits>
+
 #include "cvl_kernels.cuh"
 
 namespace cvl {
@@ -15,7 +17,8 @@ constexpr int PASS_MAX = 32;  // pairs per bundle pass at most (32 / Q)
 
 // Compact curvelet records (the record arena):
 //   ids  [slot][gms]  chain as global edge indices (anchor first)
-//   k    [slot][2]    k_max, k_min of the best cell of the final bundle
+//   k    [slot][2]    k_max, k_min of the best cell of the final bundle (a float
+//                     mode value is held exactly in double)
 //   meta [slot]       len | best_cell << 8 | forward << 24
 struct Records {
     unsigned *ids;
@@ -28,16 +31,19 @@ constexpr size_t CELL_TABLE_BYTES = CELLS_MAX * 8 + CELLS_MAX * 1 + CELLS_MAX * 
 // ---------------------------------------------------------------------------
 // Pair geometry and the bundle transport (cpu_curvelet.hpp:637-819)
 // ---------------------------------------------------------------------------
-struct PairGeom {
-    double DX, DY, DX2, DY2;
-    double sin_p_DY, cos_p_DX, sin_m_DY, cos_m_DX;
+template <typename T>
+struct PairGeomT {
+    T DX, DY, DX2, DY2;
+    T sin_p_DY, cos_p_DX, sin_m_DY, cos_m_DX;
     bool close;    // DX2 + DY2 < 4*_dx*_dx (:682)
     bool branch1;  // DX*cos(T2) + DY*sin(T2) < 0 (:690)
 };
+using PairGeom = PairGeomT<double>;
 
-__device__ __forceinline__ PairGeom pair_geom(const Model &md, double te_x, double te_y, double cosT2, double sinT2,
-                                              double le_x, double le_y, double sp, double cp, double sm, double cm) {
-    PairGeom g;
+template <typename T>
+__device__ __forceinline__ PairGeomT<T> pair_geom(const ModelT<T> &md, T te_x, T te_y, T cosT2, T sinT2, T le_x,
+                                                  T le_y, T sp, T cp, T sm, T cm) {
+    PairGeomT<T> g;
     g.DX = te_x - le_x;
     g.DY = te_y - le_y;
     g.DX2 = g.DX * g.DX;
@@ -84,29 +90,37 @@ __device__ __forceinline__ void bundle_cell_tt(const Model &md, double DX2, doub
 // Cell constants: delta_x2 (:697), orientation index j, and the best-cell rank of
 // fill_curvelet_info (:202-219): cells with d < 100 ordered by (d, row-major index);
 // 0xffff = never eligible.
-__device__ __forceinline__ void cell_tables_init(const Model &md, double *dx2, unsigned char *cj,
+// fill_curvelet_info's cell offsets are all-T: _sx * (T(ii) - (T(P) - T(1)) / T(2))
+// (:210-211, :226-227).
+template <typename T>
+__device__ __forceinline__ T info_offset(T s, int k, int n) {
+    return s * (T(k) - (T(n) - T(1)) / T(2));
+}
+
+template <typename T>
+__device__ __forceinline__ void cell_tables_init(const ModelT<T> &md, T *dx2, unsigned char *cj,
                                                  unsigned short *rank) {
     for (int c = threadIdx.x; c < CELLS_MAX; c += blockDim.x) {
         if (c >= md.cells) {
-            dx2[c] = 0.0;
+            dx2[c] = T(0);
             cj[c] = 0;
             rank[c] = 0xffffu;
             continue;
         }
         const int ci = c / md.Q, j = c % md.Q;
-        dx2[c] = md.sx * ((double)ci - ((double)md.P - 1.0) / 2.0);
+        dx2[c] = grid_offset(md.sx, ci, md.P);
         cj[c] = (unsigned char)j;
-        const double ddx = md.sx * ((double)ci - ((double)md.P - 1.0) / 2.0);
-        const double ddt = md.st * ((double)j - ((double)md.Q - 1.0) / 2.0);
-        const double d = ddx * ddx + ddt * ddt;
+        const T ddx = info_offset(md.sx, ci, md.P);
+        const T ddt = info_offset(md.st, j, md.Q);
+        const T d = ddx * ddx + ddt * ddt;
         unsigned rk = 0xffffu;
-        if (d < 100.0) {
+        if (d < T(100)) {
             rk = 0;
             for (int o = 0; o < md.cells; ++o) {
                 const int oi = o / md.Q, oj = o % md.Q;
-                const double ox = md.sx * ((double)oi - ((double)md.P - 1.0) / 2.0);
-                const double ot = md.st * ((double)oj - ((double)md.Q - 1.0) / 2.0);
-                const double od = ox * ox + ot * ot;
+                const T ox = info_offset(md.sx, oi, md.P);
+                const T ot = info_offset(md.st, oj, md.Q);
+                const T od = ox * ox + ot * ot;
                 rk += (od < d) || (od == d && o < c);
             }
         }
@@ -131,31 +145,36 @@ __device__ __forceinline__ void cell_tables_init(const Model &md, double *dx2, u
 //   (ttmdx2 -+ dx) / eq == (2 (ttmdx2 -+ dx)) / e1, branch 1's k_dx (:707-708);
 //   2 (ttmdx2 -+ dx) = (2 tt - 2 dx2) -+ 2 dx exactly.
 // Only the k_dt clamp order differs between the branches.
+//
+// Float mode keeps the reference's two branches as written: there, eq and
+// branch 1's k_dx are double expressions rounded to float, and branch 2's k_dx
+// is a float division, so the identity above does not carry over.
 // ---------------------------------------------------------------------------
-struct BundleArgs {
-    Model md;
-    Binned B;
+template <typename T>
+struct BundleArgsT {
+    ModelT<T> md;
+    BinnedT<T> B;
     unsigned long long p_begin, p_end;  // pair range of this chunk
     const int *csr_ids;
     const int *pair_anchor;
     const unsigned char *pcls;
-    const double *atrig;                // [N][2Q+2]: sin(T2t_j), cos(T2t_j), cos(T2), sin(T2)
-    double *bund;                       // [p_end - p_begin][2][32 * CPL]
+    const T *atrig;                     // [N][2Q+2]: sin(T2t_j), cos(T2t_j), cos(T2), sin(T2)
+    T *bund;                            // [p_end - p_begin][2][32 * CPL]
     unsigned char *pflag;               // [P]: bit 0 valid, bit 1 close
 };
 
 constexpr int BUNDLE_THREADS = 256;
 
 // MINB: the resident blocks per SM the register allocation is capped for (3 or 4)
-template <int CPL, int MINB>
-__global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgs a) {
-    const Model &md = a.md;
-    __shared__ double s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
+template <typename T, int CPL, int MINB>
+__global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgsT<T> a) {
+    const ModelT<T> &md = a.md;
+    __shared__ T s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
     __shared__ unsigned char s_open[2][BUNDLE_THREADS];
     for (int i = threadIdx.x; i < md.P; i += blockDim.x) {
-        const double d = md.sx * ((double)i - ((double)md.P - 1.0) / 2.0);  // delta_x2 (:697)
+        const T d = grid_offset(md.sx, i, md.P);  // delta_x2 (:697)
         s_dx2[i] = d;
-        s_dx2_2[i] = 2.0 * d;
+        s_dx2_2[i] = T(2) * d;
         s_dx2sq[i] = d * d;
     }
     for (int t = threadIdx.x; t < 2 * BUNDLE_THREADS; t += blockDim.x) (&s_open[0][0])[t] = 0;
@@ -165,8 +184,8 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgs a) 
     const int PPB = BUNDLE_THREADS / md.Q;
     const int pl = t / md.Q, jl = t - pl * md.Q;
     const bool lane_on = pl < PPB;
-    const double delta_t2 = md.st * ((double)jl - ((double)md.Q - 1.0) / 2.0);  // :698
-    const double dx_2 = 2.0 * md.dx;
+    const T delta_t2 = grid_offset(md.st, jl, md.Q);  // :698
+    const T dx_2 = T(2) * md.dx;
     const int A2 = 2 * md.Q + 2;
     const unsigned long long np = a.p_end - a.p_begin;
     int it = 0;
@@ -179,19 +198,51 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgs a) 
             if (!(a.pcls[p] & 4u)) {
                 const int ia = a.pair_anchor[p];
                 const int nn = a.csr_ids[p];
-                const double *at = a.atrig + (size_t)ia * A2;
-                const double ax = a.B.x[ia], ay = a.B.y[ia], T2 = a.B.th[ia];
-                const double sTj = at[jl], cTj = at[md.Q + jl];
-                const PairGeom g2 = pair_geom(md, ax, ay, at[2 * md.Q], at[2 * md.Q + 1], a.B.x[nn], a.B.y[nn],
-                                              a.B.sp[nn], a.B.cp[nn], a.B.sm[nn], a.B.cm[nn]);
-                const double T0 = a.B.th[nn];
-                const double T2t = T2 + delta_t2;                 // :702
-                const double s_m = cvl_sin(T2t - (T0 - md.dt));   // :728
-                const double s_p = cvl_sin(T2t - (T0 + md.dt));   // :729
-                const double tt = sTj * g2.DX - cTj * g2.DY;     // :705
-                const double tt2 = 2.0 * tt;
-                double *dst = a.bund + q * BW;
+                const T *at = a.atrig + (size_t)ia * A2;
+                const T ax = a.B.x[ia], ay = a.B.y[ia], T2 = a.B.th[ia];
+                const T sTj = at[jl], cTj = at[md.Q + jl];
+                const PairGeomT<T> g2 = pair_geom(md, ax, ay, at[2 * md.Q], at[2 * md.Q + 1], a.B.x[nn], a.B.y[nn],
+                                                  a.B.sp[nn], a.B.cp[nn], a.B.sm[nn], a.B.cm[nn]);
+                const T T0 = a.B.th[nn];
+                const T T2t = T2 + delta_t2;                 // :702
+                const T s_m = cvl_sin(T2t - (T0 - md.dt));   // :728
+                const T s_p = cvl_sin(T2t - (T0 + md.dt));   // :729
+                const T tt = sTj * g2.DX - cTj * g2.DY;     // :705
+                T *dst = a.bund + q * BW;
                 bool open = false;
+                if constexpr (!std::is_same<T, double>::value) {
+                    // float mode: :693-809 with their C++ types
+                    for (int i = 0; i < md.P; ++i) {
+                        const T delta_x2 = s_dx2[i];
+                        const T ttmdx2 = tt - delta_x2;
+                        const T sq = s_dx2sq[i];  // delta_x2 * delta_x2, a T product
+                        T k_dx_min, k_dx_max;
+                        if (g2.branch1) {
+                            const T eq = (T)(((((-2.0 * (double)delta_x2) * (double)tt + (double)g2.DX2) +
+                                               (double)g2.DY2) - (double)md.dx2) + (double)sq);       // :711
+                            k_dx_min = (T)((2.0 * (double)(ttmdx2 - md.dx)) / (double)eq);           // :714
+                            k_dx_max = (T)((2.0 * (double)(ttmdx2 + md.dx)) / (double)eq);           // :715
+                        } else {
+                            const T eq = (T)(-(((((2.0 * (double)delta_x2) * (double)tt - (double)g2.DX2) -
+                                                 (double)g2.DY2) + (double)md.dx2) - (double)sq) / 2.0);  // :774
+                            k_dx_min = (ttmdx2 - md.dx) / eq;                                        // :777
+                            k_dx_max = (ttmdx2 + md.dx) / eq;                                        // :778
+                        }
+                        const T km = s_m / (-s_m * delta_x2 + g2.cos_m_DX + g2.sin_m_DY);
+                        const T kp = s_p / (-s_p * delta_x2 + g2.cos_p_DX + g2.sin_p_DY);
+                        T bmin = -md.max_k, bmax = md.max_k;
+                        if (bmin < k_dx_min) bmin = k_dx_min;
+                        if (bmax > k_dx_max) bmax = k_dx_max;
+                        const T k2min = g2.branch1 ? km : kp;
+                        const T k2max = g2.branch1 ? kp : km;
+                        if (bmin < k2min) bmin = k2min;
+                        if (bmax > k2max) bmax = k2max;
+                        open = open || (bmax > bmin);
+                        dst[i * md.Q + jl] = bmin;
+                        dst[32 * CPL + i * md.Q + jl] = bmax;
+                    }
+                } else {
+                const double tt2 = 2.0 * tt;
 #pragma unroll 1  // (measured: unrolling by 2 spills under the 64-register cap and is 2.6% slower)
                 for (int i = 0; i < md.P; ++i) {
                     const double delta_x2 = s_dx2[i], dx2_2 = s_dx2_2[i];
@@ -212,6 +263,7 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgs a) 
                     open = open || (bmax > bmin);
                     dst[i * md.Q + jl] = bmin;
                     dst[32 * CPL + i * md.Q + jl] = bmax;
+                }
                 }
                 if (open) s_open[buf][pl] = 1;
             }
@@ -237,9 +289,10 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgs a) 
 // __reduce_or_sync vote; first-wins dedup (:876-916); each run's accepted chains
 // go as compact records to one exactly sized reservation in the record arena.
 // ---------------------------------------------------------------------------
-struct GrowthArgs {
-    Model md;
-    Binned B;
+template <typename T>
+struct GrowthArgsT {
+    ModelT<T> md;
+    BinnedT<T> B;
     int M;
     int a_begin, a_end;                 // anchors (internal order) of this chunk
     unsigned long long p_begin;         // first pair of the chunk
@@ -247,7 +300,7 @@ struct GrowthArgs {
     const int *csr_ids;
     const unsigned char *pcls;
     const unsigned char *pflag;
-    const double *bund;
+    const T *bund;
     Records rec;                        // record arena
     unsigned long long arena_cap;
     unsigned long long *arena_ctr;
@@ -262,8 +315,9 @@ struct GrowthArgs {
 };
 
 // The best-cell ranks of fill_curvelet_info (:202-219), once per run.
-__global__ void k_cell_ranks(Model md, unsigned short *__restrict__ out) {
-    __shared__ double dx2[CELLS_MAX];
+template <typename T>
+__global__ void k_cell_ranks(ModelT<T> md, unsigned short *__restrict__ out) {
+    __shared__ T dx2[CELLS_MAX];
     __shared__ unsigned char cj[CELLS_MAX];
     __shared__ unsigned short rank[CELLS_MAX];
     cell_tables_init(md, dx2, cj, rank);
@@ -283,10 +337,10 @@ __host__ __device__ inline size_t growth_smem_per_warp(int max_cand, int gms) {
 // warps per SM. A block is one warp: a block's SM slot frees as soon as its own
 // anchors are done (measured 2% faster than 4-warp blocks).
 constexpr int GROWTH_THREADS = 32;
-template <int CPL, int K, int MINB>
-__global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs a) {
+template <typename T, int CPL, int K, int MINB>
+__global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT<T> a) {
     extern __shared__ __align__(16) unsigned char gr_smem[];
-    const Model &md = a.md;
+    const ModelT<T> &md = a.md;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
@@ -357,7 +411,7 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
             // A curvelet needs the anchor and at least two more edges (len > 2, :549):
             // a run with fewer than two seeds, or group_max_sz <= 2, grows none.
             if (!a.count_only && ns > 1 && md.gms > 2) {
-                auto load_bundle = [&](int s, double *mn, double *mx) {
+                auto load_bundle = [&](int s, T *mn, T *mx) {
                     const unsigned sq = seed_q[s];
                     if (sq & CLOSE_BIT) {
 #pragma unroll
@@ -366,7 +420,7 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
                             mx[u] = md.max_k;
                         }
                     } else {
-                        const double *src = a.bund + (size_t)sq * BW;
+                        const T *src = a.bund + (size_t)sq * BW;
 #pragma unroll
                         for (int u = 0; u < CPL; ++u) {
                             mn[u] = src[lane + 32 * u];
@@ -375,7 +429,7 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
                     }
                 };
                 for (int g0 = 0; g0 < ns; g0 += K) {
-                    double cmin[K][CPL], cmax[K][CPL];
+                    T cmin[K][CPL], cmax[K][CPL];
                     unsigned len[K];
                     unsigned done = 0;
 #pragma unroll
@@ -389,14 +443,14 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
                             len[q] = 0;
                             done |= 1u << q;
 #pragma unroll
-                            for (int u = 0; u < CPL; ++u) cmin[q][u] = cmax[q][u] = 0.0;
+                            for (int u = 0; u < CPL; ++u) cmin[q][u] = cmax[q][u] = T(0);
                         }
                     }
                     // the walk's bundles, one ahead: r + 1 loads while r is intersected
-                    double nmin[CPL], nmax[CPL];
+                    T nmin[CPL], nmax[CPL];
                     load_bundle(0, nmin, nmax);
                     for (int r = 0; r < ns && done != (1u << K) - 1u; ++r) {
-                        double rmin[CPL], rmax[CPL];
+                        T rmin[CPL], rmax[CPL];
 #pragma unroll
                         for (int u = 0; u < CPL; ++u) {
                             rmin[u] = nmin[u];
@@ -410,8 +464,8 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
 #pragma unroll
                             for (int u = 0; u < CPL; ++u) {
                                 // bundle_intersection (:832-843)
-                                const double lo = (cmin[q][u] < rmin[u]) ? rmin[u] : cmin[q][u];
-                                const double hi = (cmax[q][u] > rmax[u]) ? rmax[u] : cmax[q][u];
+                                const T lo = (cmin[q][u] < rmin[u]) ? rmin[u] : cmin[q][u];
+                                const T hi = (cmax[q][u] > rmax[u]) ? rmax[u] : cmax[q][u];
                                 lv = lv || (on_l[u] && hi > lo);
                             }
                             bits |= lv ? (1u << q) : 0u;
@@ -455,7 +509,7 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
                             if (on_l[u] && cmax[q][u] > cmin[q][u] && rank_l[u] < best) best = rank_l[u];
                         best = __reduce_min_sync(FULL, best);
                         int mycell = -1;
-                        double mymax = 0.0, mymin = 0.0;
+                        T mymax = T(0), mymin = T(0);
 #pragma unroll
                         for (int u = 0; u < CPL; ++u) {
                             const bool hit = (best != 0xffffu)
@@ -470,8 +524,8 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
                         const unsigned who = __ballot_sync(FULL, mycell >= 0);
                         const int srcl = who ? (__ffs(who) - 1) : 0;
                         const int bcell = __shfl_sync(FULL, mycell, srcl);
-                        const double kmax = __shfl_sync(FULL, mymax, srcl);
-                        const double kmin = __shfl_sync(FULL, mymin, srcl);
+                        const T kmax = __shfl_sync(FULL, mymax, srcl);
+                        const T kmin = __shfl_sync(FULL, mymin, srcl);
                         if (lane == 0) {
                             double *rs = res + (size_t)s * 3;
                             rs[0] = kmax;
@@ -569,7 +623,8 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgs 
 
 // (e) finalize: records -> chain rows + info rows at anchor-major positions
 // ---------------------------------------------------------------------------
-__global__ void k_finalize(Model md, const double *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
+template <typename T>
+__global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
                            int M, Records rec, const unsigned *__restrict__ rec_base,
                            const unsigned *__restrict__ run_cnt, const unsigned long long *__restrict__ out_off,
                            unsigned long long out_cap, unsigned *__restrict__ chains, double *__restrict__ info) {
@@ -580,9 +635,9 @@ __global__ void k_finalize(Model md, const double *__restrict__ edges, int sz, i
         const int m = map_of(map_off, M, a);
         const int moff = map_off[m];
         const unsigned long long dst = out_off[a];
-        const double ref_x = edges[(size_t)a * sz + 0];
-        const double ref_y = edges[(size_t)a * sz + 1];
-        const double ref_theta = edges[(size_t)a * sz + 2];
+        const T ref_x = edges[(size_t)a * sz + 0];
+        const T ref_y = edges[(size_t)a * sz + 1];
+        const T ref_theta = edges[(size_t)a * sz + 2];
         for (unsigned r = 0; r < c0 + c1; ++r) {
             const unsigned long long s =
                 (r < c0) ? (unsigned long long)rec_base[2 * a] + r : (unsigned long long)rec_base[2 * a + 1] + (r - c0);
@@ -598,33 +653,33 @@ __global__ void k_finalize(Model md, const double *__restrict__ edges, int sz, i
             for (int z = 0; z + 1 < W; ++z) row[z + 1] = (z < (int)len) ? (ids[z] - (unsigned)moff) + 1u : 0u;
             // fill_curvelet_info (:221-255)
             const int mini = (int)bcell / md.Q, minj = (int)bcell % md.Q;
-            const double k_max = rec.k[s * 2 + 0];
-            const double k_min = rec.k[s * 2 + 1];
-            const double k = (k_max + k_min) / 2.0;
-            const double dx = md.sx * ((double)mini - ((double)md.P - 1.0) / 2.0);
-            const double dt = md.st * ((double)minj - ((double)md.Q - 1.0) / 2.0);
-            const double theta = to_2pi(ref_theta + dt);
-            const double pt_x = ref_x - dx * sin(theta);
-            const double pt_y = ref_y + dx * cos(theta);
-            double length = 0.0;
+            const T k_max = (T)rec.k[s * 2 + 0];
+            const T k_min = (T)rec.k[s * 2 + 1];
+            const T k = (k_max + k_min) / T(2);
+            const T dx = info_offset(md.sx, mini, md.P);
+            const T dt = info_offset(md.st, minj, md.Q);
+            const T theta = to_2pi(ref_theta + dt);
+            const T pt_x = ref_x - dx * sin(theta);
+            const T pt_y = ref_y + dx * cos(theta);
+            T length = T(0);
             for (unsigned z = 0; z + 1 < len; ++z) {
                 const unsigned e1 = ids[z], e2 = ids[z + 1];
                 length += sqrt(sq_dist(edges[(size_t)e1 * sz + 0], edges[(size_t)e1 * sz + 1],
                                        edges[(size_t)e2 * sz + 0], edges[(size_t)e2 * sz + 1]));
             }
-            const double quality =
-                (length > 0.0 && len > 0) ? 2.0 / (1.0 * md.nrad / length + 1.0 * length / (double)len) : 0.0;
+            const T quality =
+                (length > T(0) && len > 0) ? T(2) / (T(1) * md.nrad / length + T(1) * length / T(len)) : T(0);
             double *inf = info + d * 10ull;
             inf[0] = forward ? 1.0 : 0.0;
-            inf[1] = k_max;
-            inf[2] = k_min;
-            inf[3] = ref_theta;
-            inf[4] = pt_x;
-            inf[5] = pt_y;
-            inf[6] = theta;
-            inf[7] = k;
-            inf[8] = length;
-            inf[9] = quality;
+            inf[1] = (double)k_max;
+            inf[2] = (double)k_min;
+            inf[3] = (double)ref_theta;
+            inf[4] = (double)pt_x;
+            inf[5] = (double)pt_y;
+            inf[6] = (double)theta;
+            inf[7] = (double)k;
+            inf[8] = (double)length;
+            inf[9] = (double)quality;
         }
     }
 }

@@ -76,18 +76,21 @@ def chain_to_info_filename(chain_file: str) -> str:
     return "info_" + chain_file
 
 
-def read_edges(path: str, values_per_edge: int = 4, nthreads: int = 0) -> np.ndarray:
+def read_edges(path: str, values_per_edge: int = 4, nthreads: int = 0, scalar: str = "double") -> np.ndarray:
     """An edge file through cvl_read_edges: the reference's text format read on
     all cores (same values and error messages as its stream reader), or the
     binary format for a path ending in ".cvle". nthreads -1: the stream reader
-    alone. Raises ValueError with the reference's message on bad input."""
+    alone. scalar="float" reads as read_TO_edges_from_file<float> (each number
+    straight to float32). Raises ValueError with the reference's message on bad
+    input."""
     import ctypes as C
 
     from . import _abi
     lib = _abi.load()
-    ptr = C.POINTER(C.c_double)()
+    ctype, fn = (C.c_float, lib.cvl_read_edges_f32) if scalar == "float" else (C.c_double, lib.cvl_read_edges)
+    ptr = C.POINTER(ctype)()
     n = C.c_int64(0)
-    rc = lib.cvl_read_edges(path.encode(), values_per_edge, nthreads, C.byref(ptr), C.byref(n))
+    rc = fn(path.encode(), values_per_edge, nthreads, C.byref(ptr), C.byref(n))
     if rc != 0:
         raise ValueError(lib.cvl_last_error().decode())
     try:

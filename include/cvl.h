@@ -116,6 +116,13 @@ typedef struct cvl_result_view {
 int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
             const cvl_params *p, cvl_result **out);
 
+/* The same in the reference's --float mode (run_curvelet<float>, main.cpp:110):
+ * edges as float, the path computed with the reference's float-mode types (its
+ * float arithmetic, and the double expressions it rounds to float). The result
+ * has the same layout (info holds the float values as doubles). */
+int cvl_run_f32(cvl_engine *e, const float *edges, int32_t num_edges, int32_t edge_data_sz,
+                const cvl_params *p, cvl_result **out);
+
 /* Views a result. chains/info point into page-locked host memory owned by the
  * result; they stay valid until cvl_result_free, which may also be called after
  * the engine was destroyed. */
@@ -322,7 +329,12 @@ void cvl_server_destroy(cvl_server *s);
  * cvl_free_edges. nthreads 0: all hardware threads; -1: the stream reader
  * alone, line by line (the reference's loop, for comparisons). */
 int cvl_read_edges(const char *path, int32_t values_per_edge, int32_t nthreads, double **edges, int64_t *num_edges);
-void cvl_free_edges(double *edges);
+/* The same into float, as read_TO_edges_from_file<float> reads (each number
+ * converted straight to float, not through double); text files only. */
+int cvl_read_edges_f32(const char *path, int32_t values_per_edge, int32_t nthreads, float **edges,
+                       int64_t *num_edges);
+/* Frees the rows of cvl_read_edges or cvl_read_edges_f32. */
+void cvl_free_edges(void *edges);
 /* Binary edge file: "CVLEDGE1", uint32 values_per_edge, uint32 0, uint64
  * num_edges, then the rows as little-endian doubles (no reference counterpart). */
 int cvl_write_edges_binary(const char *path, const double *edges, int64_t num_edges, int32_t values_per_edge);

@@ -133,6 +133,7 @@ def ref_lib():
         L.cvlref_run.argtypes = [dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_int, C.c_int, C.c_int,
                                  C.POINTER(_RefOut)]
+        L.cvlref_run_f32.argtypes = [C.POINTER(C.c_float)] + L.cvlref_run.argtypes[1:]
         L.cvlref_free.argtypes = [C.POINTER(_RefOut)]
         L.cvlref_pair_bundle.argtypes = [C.c_double] * 12 + [dp, dp, C.POINTER(C.c_int)]
         _ref = L
@@ -181,14 +182,25 @@ def run(edges, nthreads=1, **params) -> Result:
         lib().orc_result_free(C.byref(r))
 
 
-def ref_run(edges, nthreads=1, want_outputs=True, **params) -> Result:
-    """The reference's own cpu_curvelet code over one edge map."""
+def ref_run(edges, nthreads=1, want_outputs=True, scalar="double", **params) -> Result:
+    """The reference's own cpu_curvelet code over one edge map: run_curvelet<double>,
+    or run_curvelet<float> (its --float mode) for scalar="float", which takes the
+    edges as float32 (convert them the way the reference reads them: float32
+    values, as from parse_edges_f32)."""
     p = dict(DEFAULTS, **params)
-    e, ptr, n, sz = _edges_arg(edges)
     r = _RefOut()
-    rc = ref_lib().cvlref_run(ptr, n, sz, p["nrad"], p["dx"], p["dt_deg"], p["max_k"], p["sx"], p["st"],
-                              p["group_max_sz"], p["max_candidates"], nthreads, 1, int(want_outputs),
-                              C.byref(r))
+    if scalar == "float":
+        e = np.ascontiguousarray(edges, dtype=np.float32)
+        assert e.ndim == 2 and e.shape[1] >= 4
+        n, sz = e.shape
+        rc = ref_lib().cvlref_run_f32(e.ctypes.data_as(C.POINTER(C.c_float)), n, sz, p["nrad"], p["dx"],
+                                      p["dt_deg"], p["max_k"], p["sx"], p["st"], p["group_max_sz"],
+                                      p["max_candidates"], nthreads, 1, int(want_outputs), C.byref(r))
+    else:
+        e, ptr, n, sz = _edges_arg(edges)
+        rc = ref_lib().cvlref_run(ptr, n, sz, p["nrad"], p["dx"], p["dt_deg"], p["max_k"], p["sx"], p["st"],
+                                  p["group_max_sz"], p["max_candidates"], nthreads, 1, int(want_outputs),
+                                  C.byref(r))
     if rc != 0:
         raise ValueError(f"cvlref_run failed ({rc})")
     try:
@@ -231,3 +243,21 @@ def read_edge_file(path: str, values_per_edge: int = 4) -> np.ndarray:
     if not rows:
         raise ValueError(f"{path}: no edges")
     return np.asarray(rows, dtype=np.float64)
+
+
+def parse_edges_f32(path: str, values_per_edge: int = 4) -> np.ndarray:
+    """An edge file read into float32 the way `std::istream >> float` reads it
+    (read_TO_edges_from_file<float>, data_io.hpp:22-79): each token converted
+    straight to float by the C library's strtof (correctly rounded), not through
+    double. Plain files only (the rows of read_edge_file)."""
+    libc = C.CDLL(None)
+    libc.strtof.restype = C.c_float
+    libc.strtof.argtypes = [C.c_char_p, C.c_void_p]
+    rows = []
+    with open(path) as fh:
+        for line in fh:
+            toks = line.split()
+            if len(toks) != values_per_edge:
+                raise ValueError(f"{path}: expected {values_per_edge} values, found {len(toks)}")
+            rows.append([libc.strtof(t.encode(), None) for t in toks])
+    return np.asarray(rows, dtype=np.float32)

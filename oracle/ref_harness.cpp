@@ -16,12 +16,20 @@
 //
 // Nothing in the product (libcvl) links or loads this file.
 
+// The headers come in main.cpp's order (main.cpp:1-11): <math.h> before the
+// reference headers puts the float overloads of sin/cos in the global namespace,
+// so that an unqualified sin(float) inside the templates resolves to the float
+// function there, as it does in the reference program (T = float).
+#include <iostream>
+#include <cmath>
+#include <math.h>
+#include <string>
+#include <vector>
+
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
-#include <iostream>
 #include <sstream>
-#include <vector>
 
 #include "preprocess.hpp"
 #include "cpu_curvelet.hpp"
@@ -65,36 +73,39 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-int cvlref_run(const double *edges, int num_edges, int edge_data_sz,
-               double nrad, double dx, double dt_deg, double max_k,
-               double sx, double st, unsigned group_max_sz, unsigned max_candidates,
-               int nthreads, int quiet, int want_outputs, cvlref_out *out)
+}  // extern "C"
+
+// run_curvelet<T> without the file I/O (main.cpp:20-96), for T = double and float.
+template <typename T>
+static int run_impl(const T *edges, int num_edges, int edge_data_sz, double nrad, double dx, double dt_deg,
+                    double max_k, double sx, double st, unsigned group_max_sz, unsigned max_candidates, int nthreads,
+                    int quiet, int want_outputs, cvlref_out *out)
 {
     std::memset(out, 0, sizeof(*out));
     quiet_scope q(quiet != 0);
 
-    // main.cpp:21-29 parameter conversions (T = double).
-    const double t_nrad = nrad;
-    const double t_dx = dx;
-    const double t_dt = double(dt_deg / 180.0) * double(M_PI);
-    const double t_max_k = max_k;
-    const double t_sx = sx;
-    const double t_st = st;
+    // main.cpp:21-29 parameter conversions
+    const T t_nrad = T(nrad);
+    const T t_dx = T(dx);
+    const T t_dt = T(dt_deg / 180.0) * T(M_PI);
+    const T t_max_k = T(max_k);
+    const T t_sx = T(sx);
+    const T t_st = T(st);
 
-    std::vector<double> toed(edges, edges + (size_t)num_edges * (size_t)edge_data_sz);
+    std::vector<T> toed(edges, edges + (size_t)num_edges * (size_t)edge_data_sz);
     int edge_num = num_edges;
     int sz = edge_data_sz;
 
     auto t0 = std::chrono::steady_clock::now();
-    CPUNeighborGraph<double> csr;
+    CPUNeighborGraph<T> csr;
     if (!build_neighbor_csr_graph(edge_num, sz, toed.data(), t_nrad, 3u, max_candidates, nthreads, csr)) {
         return -1;
     }
     out->ms_csr = ms_since(t0);
 
     t0 = std::chrono::steady_clock::now();
-    CurveletCPU<double> obj(edge_num, sz, csr, t_dx, t_dt, t_sx, t_st, t_max_k, group_max_sz, nthreads,
-                            toed.data(), t_nrad);
+    CurveletCPU<T> obj(edge_num, sz, csr, t_dx, t_dt, t_sx, t_st, t_max_k, group_max_sz, nthreads, toed.data(),
+                       t_nrad);
     CPUCurveletFormationResult br;
     if (!obj.form_pairwise_bundles(br)) {
         return -2;
@@ -122,7 +133,7 @@ int cvlref_run(const double *edges, int num_edges, int edge_data_sz,
     std::memcpy(out->neighbor_offsets, csr.neighbor_offsets.data(), sizeof(int) * ((size_t)num_edges + 1));
     if (np) {
         std::memcpy(out->neighbor_ids, csr.neighbor_ids.data(), sizeof(int) * np);
-        std::memcpy(out->neighbor_dist2, csr.neighbor_dist2.data(), sizeof(double) * np);
+        for (size_t k = 0; k < np; ++k) out->neighbor_dist2[k] = (double)csr.neighbor_dist2[k];
     }
 
     const size_t nc = out->num_curvelets;
@@ -135,6 +146,27 @@ int cvlref_run(const double *edges, int num_edges, int edge_data_sz,
         for (size_t col = 0; col < 10; ++col)
             out->info[row * 10 + col] = obj._curvelet_info[col * stride + row];
     return 0;
+}
+
+extern "C" {
+
+int cvlref_run(const double *edges, int num_edges, int edge_data_sz,
+               double nrad, double dx, double dt_deg, double max_k,
+               double sx, double st, unsigned group_max_sz, unsigned max_candidates,
+               int nthreads, int quiet, int want_outputs, cvlref_out *out)
+{
+    return run_impl<double>(edges, num_edges, edge_data_sz, nrad, dx, dt_deg, max_k, sx, st, group_max_sz,
+                            max_candidates, nthreads, quiet, want_outputs, out);
+}
+
+// run_curvelet<float> (the --float mode, main.cpp:110), on edges already in float.
+int cvlref_run_f32(const float *edges, int num_edges, int edge_data_sz,
+                   double nrad, double dx, double dt_deg, double max_k,
+                   double sx, double st, unsigned group_max_sz, unsigned max_candidates,
+                   int nthreads, int quiet, int want_outputs, cvlref_out *out)
+{
+    return run_impl<float>(edges, num_edges, edge_data_sz, nrad, dx, dt_deg, max_k, sx, st, group_max_sz,
+                           max_candidates, nthreads, quiet, want_outputs, out);
 }
 
 void cvlref_free(cvlref_out *out)

@@ -81,8 +81,6 @@ def test_cli_flags_without_gpu(tmp_path):
     assert r.returncode == 0 and "--max-candidates" in r.stderr
     r = subprocess.run([cli, "--bogus"], capture_output=True, text=True)
     assert r.returncode == 1 and "Unknown argument: --bogus" in r.stderr
-    r = subprocess.run([cli, "--float"], capture_output=True, text=True)
-    assert r.returncode == 1
     r = subprocess.run([cli, "--nrad", "abc"], capture_output=True, text=True)
     assert r.returncode == 1 and "invalid value for --nrad" in r.stderr
     # missing input file is reported before any device work (data_io.hpp:27-31)

@@ -114,3 +114,58 @@ def test_binary_round_trip_and_checks(tmp_path):
     with pytest.raises(ValueError) as ei:
         data_io.read_edges(str(tmp_path / "x.cvle"), 6)
     assert "not a binary edge file" in str(ei.value)
+
+
+# ---- --float mode: read_TO_edges_from_file<float> reads each number straight to float ----
+def _both_f32(path, vpe=4):
+    out = []
+    for nt in (8, -1):
+        try:
+            out.append(("ok", data_io.read_edges(str(path), vpe, nt, scalar="float")))
+        except ValueError as e:
+            out.append(("err", str(e)))
+    (k1, v1), (k2, v2) = out
+    assert k1 == k2, (v1, v2)
+    if k1 == "ok":
+        assert v1.dtype == np.float32 and v1.shape == v2.shape
+        assert np.array_equal(v1.view(np.uint32), v2.view(np.uint32))
+    else:
+        assert v1 == v2
+    return k1, v1
+
+
+def test_float_reader_matches_strtof(tmp_path):
+    """Each token rounded once, to nearest float (strtof), on all threads and in
+    the stream reader; 17-digit tokens include values between two floats that a
+    read through double would round twice."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(12)
+    e = np.column_stack([rng.uniform(-5000, 5000, 20000), rng.uniform(0, 3000, 20000),
+                         rng.uniform(-np.pi, np.pi, 20000), rng.uniform(0, 1e-3, 20000)])
+    # midpoints between adjacent floats, nudged by one double ulp either way
+    f = rng.uniform(1, 2000, 4000).astype(np.float32)
+    mid = (f.astype(np.float64) + np.nextafter(f, np.float32(np.inf)).astype(np.float64)) / 2
+    e[:4000, 0] = np.nextafter(mid, np.inf)
+    e[4000:8000, 1] = np.nextafter(mid, -np.inf)
+    for fmt in ("%.17g", "%.6f", "%g"):
+        p = tmp_path / "f.txt"
+        np.savetxt(p, e, fmt=fmt, delimiter="\t")
+        kind, v = _both_f32(p)
+        assert kind == "ok"
+        assert np.array_equal(v.view(np.uint32), O.parse_edges_f32(str(p)).view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["plus_sign", "inf", "nan", "overflow", "underflow", "negative_zero",
+                                  "leading_point", "missing_value", "text", "trailing_empty_line",
+                                  "blank_line_inside", "crlf"])
+def test_float_reader_unusual_input(tmp_path, name):
+    p = tmp_path / f"{name}.txt"
+    p.write_bytes(UNUSUAL[name].encode())
+    _both_f32(p)
+
+
+def test_float_reader_rejects_binary(tmp_path):
+    p = tmp_path / "m.cvle"
+    data_io.write_edges_binary(str(p), np.zeros((3, 4)))
+    with pytest.raises(ValueError):
+        data_io.read_edges(str(p), 4, scalar="float")

@@ -87,3 +87,20 @@ def test_restatement_matches_live_reference_nondefault_params(oracle):
     o = oracle.run(e, nthreads=4, **kw)
     assert np.array_equal(r.chains, o.chains)
     assert np.array_equal(r.info.view(np.uint64), o.info.view(np.uint64))
+
+
+def test_float_fixtures_reproduce_with_live_reference(oracle):
+    """The --float fixtures are the reference's run_curvelet<float>: where the
+    harness is built, running it again gives the same bits (KATs, digit1)."""
+    import os
+    if not oracle.ref_available():
+        pytest.skip("reference harness not built here")
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_files_f32.npz"))
+    for name in sorted({k.split("/")[1] for k in z.files if k.startswith("kat/")}):
+        gms, mc = z[f"kat/{name}/params"].tolist()
+        r = oracle.ref_run(z[f"kat/{name}/edges"], scalar="float", group_max_sz=gms, max_candidates=mc)
+        assert np.array_equal(r.chains, z[f"kat/{name}/chains"]), name
+        assert np.array_equal(r.info.view(np.uint64), z[f"kat/{name}/info"].view(np.uint64)), name
+    r = oracle.ref_run(z["TO_edges_digit1/edges"], scalar="float")
+    assert np.array_equal(r.chains, z["TO_edges_digit1/chains"])
+    assert np.array_equal(r.info.view(np.uint64), z["TO_edges_digit1/info"].view(np.uint64))
