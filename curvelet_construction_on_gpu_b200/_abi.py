@@ -80,6 +80,18 @@ class CvlTuning(C.Structure):
 
 CVL_TUNING_BUCKETS = 4
 
+
+class CvlContourParams(C.Structure):
+    _fields_ = [("min_group_size", C.c_uint32), ("gap", C.c_double)]
+
+
+class CvlContoursView(C.Structure):
+    _fields_ = [("num_links", C.c_int64), ("link_parent", C.POINTER(C.c_int32)),
+                ("link_child", C.POINTER(C.c_int32)), ("link_votes", C.POINTER(C.c_int32)),
+                ("num_fragments", C.c_int64), ("fragment_offsets", C.POINTER(C.c_int64)),
+                ("fragment_ids", C.POINTER(C.c_int32)), ("max_fragment_length", C.c_int32),
+                ("num_edges", C.c_int32), ("device_ms", C.c_float)]
+
 # (name, restype, argtypes) of every entry point declared in include/cvl.h
 _vp = C.c_void_p
 _dp = C.POINTER(C.c_double)
@@ -135,6 +147,13 @@ SIGNATURES = [
     ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),
     ("cvl_engine_last_launch_count", C.c_int, [_vp]),
     ("cvl_measure_fp64_peak", C.c_int, [_vp, _dp]),
+    ("cvl_contour_params_default", None, [C.POINTER(CvlContourParams)]),
+    ("cvl_link_contours", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.c_int64, C.c_int32,
+                                    C.POINTER(CvlContourParams), C.POINTER(_vp)]),
+    ("cvl_run_contours", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.POINTER(CvlParams),
+                                   C.POINTER(CvlContourParams), C.POINTER(_vp), C.POINTER(_vp)]),
+    ("cvl_contours_get", C.c_int, [_vp, C.POINTER(CvlContoursView)]),
+    ("cvl_contours_free", None, [_vp]),
 ]
 
 _lib = None

@@ -107,6 +107,68 @@ def _view_to_result(v: CvlResultView, owner: "_Owner | None" = None) -> Result:
                   int(v.truncated_anchors), int(v.num_edges), float(v.device_ms))
 
 
+@dataclass
+class ContourParams:
+    """construct_the_link_graph's min_group_size (4 in form_curvelet_process::execute,
+    original_code/form_curvelet_process.cpp:79) and the gap between consecutive
+    edges of a fragment (1.5 in original_code/main.cpp:146)."""
+    min_group_size: int = 4
+    gap: float = 1.5
+
+    def to_c(self) -> _abi.CvlContourParams:
+        return _abi.CvlContourParams(int(self.min_group_size), float(self.gap))
+
+
+@dataclass
+class Contours:
+    """The edgel link graph and its contour fragments (one-chains) of one map.
+    links: [L, 3] int32 (parent id, child id, votes), 0-based, in _cLinks order
+    (parent ascending, then creation order); fragments in start-edge order as
+    CSR: frag_offsets [F + 1] int64, frag_ids int32 (0-based)."""
+    links: np.ndarray
+    frag_offsets: np.ndarray
+    frag_ids: np.ndarray
+    num_edges: int
+    device_ms: float = 0.0
+
+    @property
+    def num_frags(self) -> int:
+        return int(self.frag_offsets.shape[0] - 1)
+
+    def fragments(self) -> list:
+        return [self.frag_ids[self.frag_offsets[i]:self.frag_offsets[i + 1]] for i in range(self.num_frags)]
+
+    def as_array(self) -> np.ndarray:
+        """curve_fragment_graph::get_output_array: one row per fragment, 1-based
+        edge ids, width = the longest fragment, zero-padded (the reference leaves
+        the padding unset)."""
+        lens = np.diff(self.frag_offsets)
+        w = int(lens.max()) if lens.size else 0
+        out = np.zeros((self.num_frags, w), np.int32)
+        for i in range(self.num_frags):
+            out[i, :lens[i]] = self.frag_ids[self.frag_offsets[i]:self.frag_offsets[i + 1]] + 1
+        return out
+
+
+def _contours_from_handle(lib, h) -> Contours:
+    try:
+        v = _abi.CvlContoursView()
+        check(lib.cvl_contours_get(h, C.byref(v)), "cvl_contours_get")
+        L, F = int(v.num_links), int(v.num_fragments)
+        if L:
+            links = np.column_stack([np.ctypeslib.as_array(v.link_parent, shape=(L,)),
+                                     np.ctypeslib.as_array(v.link_child, shape=(L,)),
+                                     np.ctypeslib.as_array(v.link_votes, shape=(L,))]).astype(np.int32)
+        else:
+            links = np.zeros((0, 3), np.int32)
+        offs = np.ctypeslib.as_array(v.fragment_offsets, shape=(F + 1,)).copy()
+        nid = int(offs[-1])
+        ids = np.ctypeslib.as_array(v.fragment_ids, shape=(nid,)).copy() if nid else np.zeros(0, np.int32)
+        return Contours(links, offs, ids, int(v.num_edges), float(v.device_ms))
+    finally:
+        lib.cvl_contours_free(h)
+
+
 def _result_from_handle(lib, r) -> Result:
     owner = _Owner(lib, r, "cvl_result_free")
     v = CvlResultView()
@@ -193,6 +255,39 @@ class Engine:
         v = CvlResultView()
         check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
         return _view_to_result(v, owner)
+
+    # ---- downstream: link graph and contour fragments
+    def link_contours(self, edges, chains, contour_params: ContourParams | None = None) -> Contours:
+        """construct_the_link_graph + extract_regular_contours_from_the_link_graph
+        (original_code/form_curvelet_process.cpp:453-654) on curvelets the caller
+        holds (chains as Result.chains gives them)."""
+        cp = (contour_params or ContourParams()).to_c()
+        e = _edges(edges)
+        ch = np.ascontiguousarray(chains, dtype=np.uint32)
+        if ch.ndim != 2:
+            raise ValueError("chains must be a 2-D array [num_curvelets, chain_width]")
+        h = C.c_void_p()
+        check(self._lib.cvl_link_contours(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1],
+                                          ch.ctypes.data_as(C.POINTER(C.c_uint32)), ch.shape[0], ch.shape[1],
+                                          C.byref(cp), C.byref(h)), "cvl_link_contours")
+        return _contours_from_handle(self._lib, h)
+
+    def run_contours(self, edges, params: CurveletParams | None = None,
+                     contour_params: ContourParams | None = None, dt_rad: float = 0.0,
+                     want_curvelets: bool = True):
+        """Edges -> curvelets -> link graph -> fragments in one device pass.
+        Returns (Result or None, Contours)."""
+        params = params or CurveletParams()
+        cp = (contour_params or ContourParams(gap=params.gap)).to_c()
+        e = _edges(edges)
+        p = params.to_c(dt_rad)
+        r = C.c_void_p()
+        h = C.c_void_p()
+        check(self._lib.cvl_run_contours(self._h, e.ctypes.data_as(_abi._dp), e.shape[0], e.shape[1], C.byref(p),
+                                         C.byref(cp), C.byref(r) if want_curvelets else None, C.byref(h)),
+              "cvl_run_contours")
+        res = _result_from_handle(self._lib, r) if want_curvelets else None
+        return res, _contours_from_handle(self._lib, h)
 
     # ---- staged API
     def build_neighbor_graph(self, edges, rad: float = 3.5, neighbor_radius: int = 3,

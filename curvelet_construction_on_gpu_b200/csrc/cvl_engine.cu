@@ -20,6 +20,7 @@
 #include "../../include/cvl.h"
 #include "cvl_internal.h"
 #include "cvl_pinned.h"
+#include "cvl_contours.cuh"
 #include "cvl_path.cuh"
 #include "cvl_scan.cuh"
 
@@ -104,6 +105,17 @@ struct cvl_engine {
     std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
     DBuf pairs_in, pb_min, pb_max, pb_valid;
+    // downstream stage (link graph, contour fragments)
+    struct ContourBufs {
+        DBuf chains_in, cnt, off, cursor, bucket, outdeg, indeg, child, parent, succ, pred, flags, linked, firsts,
+            region, ctr, fsrc, fnf, fnb, isfrag, flen, fidx, idoff, loff, lpe, lce, lvotes, fragoff, fragids, err;
+        DBuf *all(int i) {
+            DBuf *b[] = {&chains_in, &cnt, &off, &cursor, &bucket, &outdeg, &indeg, &child, &parent, &succ,
+                         &pred, &flags, &linked, &firsts, &region, &ctr, &fsrc, &fnf, &fnb, &isfrag,
+                         &flen, &fidx, &idoff, &loff, &lpe, &lce, &lvotes, &fragoff, &fragids, &err};
+            return i < (int)(sizeof(b) / sizeof(b[0])) ? b[i] : nullptr;
+        }
+    } cw;
 
     // per-kernel timing of the last run
     std::vector<const char *> mark_names;
@@ -178,6 +190,11 @@ struct cvl_engine {
                        &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
                        &pb_max, &pb_valid};
         for (DBuf *b : all) {
+            if (b->p) cudaFreeAsync(b->p, stream);
+            b->p = nullptr;
+            b->bytes = 0;
+        }
+        for (int i = 0; DBuf *b = cw.all(i); ++i) {
             if (b->p) cudaFreeAsync(b->p, stream);
             b->p = nullptr;
             b->bytes = 0;
@@ -1669,5 +1686,301 @@ int cvl_pair_bundles_noalloc(const double *pairs, int32_t n, const cvl_params *p
     CVL_CUDA(cudaStreamSynchronize(s));
     return CVL_OK;
 }
+
+}  // extern "C"
+
+
+// =============================================================================
+// Downstream: curvelets -> edgel link graph -> contour fragments (cvl_contours.cuh)
+// =============================================================================
+struct cvl_contours {
+    std::shared_ptr<PinnedPool> pool;
+    void *links_p = nullptr;  // pe, ce, votes: 3 x num_links int32
+    void *offs_p = nullptr;
+    void *ids_p = nullptr;
+    cvl_contours_view v{};
+    ~cvl_contours() {
+        if (pool) {
+            pool->put(links_p);
+            pool->put(offs_p);
+            pool->put(ids_p);
+        }
+    }
+};
+
+namespace {
+
+// The stage on device-resident edges (double AoS) and chains, on the engine's
+// stream; copies the link list and the fragments into *c.
+int contours_on_device(cvl_engine *e, const double *d_edges, int n, int sz, const unsigned *d_chains, long long C,
+                       int W, const cvl_contour_params &cp, cvl_contours *c) {
+    using namespace cvlc;
+    if (W < 2 || W > 64) return fail(CVL_EINVAL, "chain_width must be in [2, 64]");
+    if (n >= (1 << 30)) return fail(CVL_EOVERFLOW, "the link graph takes fewer than 2^30 edges");
+    if ((unsigned long long)C * (unsigned long long)(W - 1) >= (1ull << 32))
+        return fail(CVL_EOVERFLOW, "too many curvelets for the link graph (rows x (width - 1) >= 2^32)");
+    if (!(cp.gap >= 0.0) || !std::isfinite(cp.gap)) return fail(CVL_EINVAL, "gap must be finite and >= 0");
+    cudaStream_t s = e->stream;
+    auto &w = e->cw;
+    const size_t N = (size_t)n;
+    const unsigned long long occ_cap = 2ull * (unsigned long long)C * (unsigned long long)std::max(W - 2, 1);
+    CVL_TRY(e->alloc(w.cnt, sizeof(unsigned) * N));
+    CVL_TRY(e->alloc(w.cursor, sizeof(unsigned) * N));
+    CVL_TRY(e->alloc(w.off, sizeof(unsigned long long) * (N + 1)));
+    CVL_TRY(e->alloc(w.bucket, sizeof(uint2) * std::max<unsigned long long>(occ_cap, 1)));
+    CVL_TRY(e->alloc(w.outdeg, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.indeg, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.child, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.parent, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.succ, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.pred, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.flags, N));
+    CVL_TRY(e->alloc(w.linked, N));
+    CVL_TRY(e->alloc(w.loff, sizeof(unsigned long long) * (N + 1)));
+    CVL_TRY(e->alloc(w.lpe, sizeof(int) * std::max<unsigned long long>(occ_cap / 2, 1)));
+    CVL_TRY(e->alloc(w.lce, sizeof(int) * std::max<unsigned long long>(occ_cap / 2, 1)));
+    CVL_TRY(e->alloc(w.lvotes, sizeof(int) * std::max<unsigned long long>(occ_cap / 2, 1)));
+    CVL_TRY(e->alloc(w.firsts, sizeof(unsigned) * N));
+    const unsigned long long region_cap = 3ull * N + 16;
+    CVL_TRY(e->alloc(w.region, sizeof(int) * region_cap));
+    CVL_TRY(e->alloc(w.ctr, sizeof(unsigned long long) * 2));
+    CVL_TRY(e->alloc(w.fsrc, sizeof(unsigned long long) * N));
+    CVL_TRY(e->alloc(w.fnf, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.fnb, sizeof(int) * N));
+    CVL_TRY(e->alloc(w.isfrag, sizeof(unsigned) * N));
+    CVL_TRY(e->alloc(w.flen, sizeof(unsigned long long) * N));
+    CVL_TRY(e->alloc(w.fidx, sizeof(unsigned) * (N + 1)));
+    CVL_TRY(e->alloc(w.idoff, sizeof(unsigned long long) * (N + 1)));
+    CVL_TRY(e->alloc(w.fragoff, sizeof(long long) * (N + 1)));
+    CVL_TRY(e->alloc(w.fragids, sizeof(int) * region_cap));
+    CVL_TRY(e->alloc(w.err, sizeof(unsigned) * 4));
+
+    CVL_CUDA(cudaMemsetAsync(w.cnt.p, 0, sizeof(unsigned) * N, s));
+    CVL_CUDA(cudaMemsetAsync(w.cursor.p, 0, sizeof(unsigned) * N, s));
+    CVL_CUDA(cudaMemsetAsync(w.ctr.p, 0, sizeof(unsigned long long) * 2, s));
+    CVL_CUDA(cudaMemsetAsync(w.fnf.p, 0xff, sizeof(int) * N, s));  // -1: no fragment starts here
+    CVL_CUDA(cudaMemsetAsync(w.err.p, 0, sizeof(unsigned) * 4, s));
+    unsigned *err = (unsigned *)w.err.p;
+
+    const int rb = (int)std::max(1LL, (C + 255) / 256);
+    const int nb = (int)((N + 255) / 256);
+    if (C > 0) {
+        k_link_count<<<rb, 256, 0, s>>>(d_chains, C, W, cp.min_group_size, n, (unsigned *)w.cnt.p, err);
+        CVL_TRY(check_launch("k_link_count"));
+    }
+    CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)w.cnt.p, N, (unsigned long long *)w.off.p)));
+    if (C > 0) {
+        k_link_fill<<<rb, 256, 0, s>>>(d_chains, C, W, cp.min_group_size, n, (const unsigned long long *)w.off.p,
+                                       (unsigned *)w.cursor.p, (uint2 *)w.bucket.p);
+        CVL_TRY(check_launch("k_link_fill"));
+    }
+    Graph g;
+    g.n = n;
+    g.occ_off = (const unsigned long long *)w.off.p;
+    g.bucket = (uint2 *)w.bucket.p;
+    g.outdeg = (int *)w.outdeg.p;
+    g.indeg = (int *)w.indeg.p;
+    g.child = (int *)w.child.p;
+    g.parent = (int *)w.parent.p;
+    g.succ = (int *)w.succ.p;
+    g.pred = (int *)w.pred.p;
+    g.flags = (unsigned char *)w.flags.p;
+    g.linked = (unsigned char *)w.linked.p;
+    k_link_degrees<<<nb, 256, 0, s>>>(g);
+    CVL_TRY(check_launch("k_link_degrees"));
+    CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)w.outdeg.p, N, (unsigned long long *)w.loff.p)));
+    k_link_list<<<nb, 256, 0, s>>>(g, (const unsigned long long *)w.loff.p, (int *)w.lpe.p, (int *)w.lce.p,
+                                   (int *)w.lvotes.p);
+    CVL_TRY(check_launch("k_link_list"));
+    k_link_paths<<<nb, 256, 0, s>>>(g);
+    CVL_TRY(check_launch("k_link_paths"));
+    FragOut o;
+    o.edges = d_edges;
+    o.sz = sz;
+    o.thres = cp.gap * cp.gap;
+    o.first_ids = (unsigned *)w.firsts.p;
+    o.first_ctr = (unsigned long long *)w.ctr.p;
+    o.region = (int *)w.region.p;
+    o.region_ctr = (unsigned long long *)w.ctr.p + 1;
+    o.region_cap = region_cap;
+    o.first_cap = N;
+    o.frag_src = (unsigned long long *)w.fsrc.p;
+    o.frag_nf = (int *)w.fnf.p;
+    o.frag_nb = (int *)w.fnb.p;
+    o.err = err;
+    // one thread per edge; short blocks, since a few threads trace long components
+    const int nb128 = (int)((N + 127) / 128);
+    k_trace_paths<<<nb128, 128, 0, s>>>(g, o);
+    CVL_TRY(check_launch("k_trace_paths"));
+    k_trace_cycles<<<nb128, 128, 0, s>>>(g, o);
+    CVL_TRY(check_launch("k_trace_cycles"));
+    k_frag_sizes<<<nb, 256, 0, s>>>(n, (const int *)w.fnf.p, (const int *)w.fnb.p, (unsigned *)w.isfrag.p,
+                                    (unsigned long long *)w.flen.p);
+    CVL_TRY(check_launch("k_frag_sizes"));
+    CVL_TRY((scan<unsigned, unsigned>(e, (const unsigned *)w.isfrag.p, N, (unsigned *)w.fidx.p)));
+    CVL_TRY((scan<unsigned long long, unsigned long long>(e, (const unsigned long long *)w.flen.p, N,
+                                                           (unsigned long long *)w.idoff.p)));
+    k_frag_write<<<nb, 256, 0, s>>>(n, (const int *)w.fnf.p, (const int *)w.fnb.p,
+                                    (const unsigned long long *)w.fsrc.p, (const int *)w.region.p,
+                                    (const unsigned *)w.fidx.p, (const unsigned long long *)w.idoff.p,
+                                    (long long *)w.fragoff.p, (int *)w.fragids.p);
+    CVL_TRY(check_launch("k_frag_write"));
+    e->mark("contours");
+
+    unsigned long long h_links = 0, h_ids = 0;
+    unsigned h_frags = 0, h_err = 0;
+    CVL_CUDA(cudaMemcpyAsync(&h_links, (unsigned long long *)w.loff.p + N, sizeof(h_links), cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(&h_ids, (unsigned long long *)w.idoff.p + N, sizeof(h_ids), cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(&h_frags, (unsigned *)w.fidx.p + N, sizeof(h_frags), cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaStreamSynchronize(s));
+    if (h_err & ERR_ID) return fail(CVL_EINVAL, "a curvelet chain holds an edge id outside the map");
+    if (h_err) return fail(CVL_EOVERFLOW, "contour kernels reported error bits " + std::to_string(h_err));
+
+    c->pool = e->pinned;
+    c->links_p = e->pinned->get(sizeof(int) * 3 * (h_links ? h_links : 1));
+    c->offs_p = e->pinned->get(sizeof(long long) * (h_frags + 1));
+    c->ids_p = e->pinned->get(sizeof(int) * (h_ids ? h_ids : 1));
+    if (!c->links_p || !c->offs_p || !c->ids_p)
+        return fail(CVL_ENOMEM, "page-locked result buffers could not be allocated");
+    int *lp = (int *)c->links_p;
+    if (h_links) {
+        CVL_CUDA(cudaMemcpyAsync(lp, w.lpe.p, sizeof(int) * h_links, cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaMemcpyAsync(lp + h_links, w.lce.p, sizeof(int) * h_links, cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaMemcpyAsync(lp + 2 * h_links, w.lvotes.p, sizeof(int) * h_links, cudaMemcpyDeviceToHost, s));
+    }
+    CVL_CUDA(cudaMemcpyAsync(c->offs_p, w.fragoff.p, sizeof(long long) * (h_frags + 1), cudaMemcpyDeviceToHost, s));
+    if (h_ids) CVL_CUDA(cudaMemcpyAsync(c->ids_p, w.fragids.p, sizeof(int) * h_ids, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaStreamSynchronize(s));
+    if (h_frags == 0) ((long long *)c->offs_p)[0] = 0;
+    cvl_contours_view &v = c->v;
+    v.num_links = (int64_t)h_links;
+    v.link_parent = lp;
+    v.link_child = lp + h_links;
+    v.link_votes = lp + 2 * h_links;
+    v.num_fragments = (int64_t)h_frags;
+    v.fragment_offsets = (const int64_t *)c->offs_p;
+    v.fragment_ids = (const int32_t *)c->ids_p;
+    int32_t mx = 0;
+    for (unsigned f = 0; f < h_frags; ++f)
+        mx = std::max<int32_t>(mx, (int32_t)(v.fragment_offsets[f + 1] - v.fragment_offsets[f]));
+    v.max_fragment_length = mx;
+    v.num_edges = n;
+    return CVL_OK;
+}
+
+// the caller's parameters, or the defaults with `gap` (CurveletParams::gap, the
+// downstream stages' parameter, param_settings.hpp) when cp is NULL
+int contour_params_of(const cvl_contour_params *cp, double gap, cvl_contour_params &out) {
+    cvl_contour_params_default(&out);
+    if (cp)
+        out = *cp;
+    else
+        out.gap = gap;
+    if (!(out.gap >= 0.0) || !std::isfinite(out.gap)) return fail(CVL_EINVAL, "gap must be finite and >= 0");
+    return CVL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cvl_contour_params_default(cvl_contour_params *p) {
+    if (!p) return;
+    p->min_group_size = 4;
+    p->gap = 1.5;
+}
+
+int cvl_link_contours(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
+                      const uint32_t *chains, int64_t num_curvelets, int32_t chain_width,
+                      const cvl_contour_params *cp, cvl_contours **out) {
+    if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
+    *out = nullptr;
+    CVL_TRY(check_edges_args(edges, num_edges, edge_data_sz));
+    if (num_curvelets < 0 || (num_curvelets > 0 && !chains)) return fail(CVL_EINVAL, "chains is NULL");
+    if (chain_width < 2 || chain_width > 64) return fail(CVL_EINVAL, "chain_width must be in [2, 64]");
+    cvl_contour_params p;
+    CVL_TRY(contour_params_of(cp, 1.5, p));
+    // the link graph visits anchors in ascending order (form_curvelet_process.cpp:479-491)
+    for (int64_t r = 0; r < num_curvelets; ++r) {
+        const uint32_t a = chains[(size_t)r * chain_width];
+        if (a == 0 || a > (uint32_t)num_edges)
+            return fail(CVL_EINVAL, "curvelet row " + std::to_string(r) + ": anchor id outside the map");
+        if (r > 0 && a < chains[(size_t)(r - 1) * chain_width])
+            return fail(CVL_EINVAL, "curvelet rows must be grouped by anchor in ascending order");
+    }
+    CVL_CUDA(cudaSetDevice(e->device));
+    e->nmarks = 0;
+    g_launches = 0;
+    e->mark("start");
+    std::vector<int32_t> mo = {0, num_edges};
+    CVL_TRY(upload(e, edges, num_edges, edge_data_sz, mo));
+    const size_t cbytes = sizeof(uint32_t) * (size_t)std::max<int64_t>(num_curvelets, 1) * chain_width;
+    CVL_TRY(e->alloc(e->cw.chains_in, cbytes));
+    if (num_curvelets > 0)
+        CVL_CUDA(cudaMemcpyAsync(e->cw.chains_in.p, chains, sizeof(uint32_t) * (size_t)num_curvelets * chain_width,
+                                 cudaMemcpyHostToDevice, e->stream));
+    e->mark("upload");
+    cvl_contours *c = new cvl_contours();
+    int rc = contours_on_device(e, (const double *)e->edges.p, num_edges, edge_data_sz,
+                                (const unsigned *)e->cw.chains_in.p, num_curvelets, chain_width, p, c);
+    if (rc != CVL_OK) {
+        delete c;
+        return rc;
+    }
+    e->collect_marks();
+    c->v.device_ms = (float)e->last_device_ms;
+    *out = c;
+    return CVL_OK;
+}
+
+int cvl_run_contours(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
+                     const cvl_params *p, const cvl_contour_params *cp, cvl_result **curvelets_out,
+                     cvl_contours **out) {
+    if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
+    *out = nullptr;
+    if (curvelets_out) *curvelets_out = nullptr;
+    CVL_TRY(check_edges_args(edges, num_edges, edge_data_sz));
+    cvl_contour_params q;
+    CVL_TRY(contour_params_of(cp, p ? p->gap : 1.5, q));
+    CVL_CUDA(cudaSetDevice(e->device));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
+    std::vector<int32_t> mo = {0, num_edges};
+    CVL_TRY(upload(e, edges, num_edges, edge_data_sz, mo));
+    RunOut ro;
+    CVL_TRY(run_pipeline(e, (const double *)e->edges.p, num_edges, edge_data_sz, (const int *)e->map_off.p, mo, md,
+                         cpl, 0, false, ro));
+    cvl_contours *c = new cvl_contours();
+    int rc = contours_on_device(e, (const double *)e->edges.p, num_edges, edge_data_sz, (const unsigned *)e->chains.p,
+                                (long long)ro.total_curvelets, md.gms + 1, q, c);
+    if (rc != CVL_OK) {
+        delete c;
+        return rc;
+    }
+    e->collect_marks();
+    c->v.device_ms = (float)e->last_device_ms;
+    if (curvelets_out) {
+        cvl_result *r = new cvl_result();
+        rc = fill_view_from_run(e, ro, num_edges, md.gms + 1, r);
+        if (rc != CVL_OK) {
+            delete r;
+            delete c;
+            return rc;
+        }
+        *curvelets_out = r;
+    }
+    *out = c;
+    return CVL_OK;
+}
+
+int cvl_contours_get(const cvl_contours *c, cvl_contours_view *view) {
+    if (!c || !view) return fail(CVL_EINVAL, "contours/view is NULL");
+    *view = c->v;
+    return CVL_OK;
+}
+
+void cvl_contours_free(cvl_contours *c) { delete c; }
 
 }  // extern "C"

@@ -163,3 +163,101 @@ def stress_mix(base_seed: int = 5000, n_dense: int = 16, n_small: int = 1024) ->
 def write_edge_file(path: str, edges: np.ndarray) -> None:
     """Writes rows in the reference edge-file format with round-trip precision."""
     np.savetxt(path, edges, fmt="%.17g", delimiter="\t")
+
+
+# ---- curvelet sets for the link-graph / contour stage -----------------------------
+def contour_fuzz(seed: int = 0, n_edges: int = 3000, width: int = 5, size: float = 120.0,
+                 max_per_anchor: int = 4) -> tuple[np.ndarray, np.ndarray]:
+    """Edges on random polylines (about 1 px apart, some 2-3 px gaps) and random
+    curvelet chains over them: for each anchor in ascending order, up to
+    max_per_anchor rows [anchor + 1, anchor + 1, then a random walk through
+    nearby edges], width - 1 edges at most, zero-padded. The walks cross each
+    other and run both ways, so the link graph has junctions, reversed links,
+    gaps and cycles. Returns (edges [n, 4], chains [C, width] uint32)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pts = []
+    while sum(len(p) for p in pts) < n_edges:
+        k = int(rng.integers(5, 60))
+        step = rng.choice([0.9, 1.0, 1.2, 2.6], size=k, p=[0.4, 0.35, 0.2, 0.05])
+        ang = rng.uniform(0, 2 * np.pi) + np.cumsum(rng.normal(0, 0.25, k))
+        xy = rng.uniform(0, size, 2) + np.cumsum(np.column_stack([np.cos(ang), np.sin(ang)]) * step[:, None], 0)
+        pts.append(xy)
+    xy = np.concatenate(pts)[:n_edges]
+    order = rng.permutation(n_edges)  # ids are not in curve order
+    xy = xy[order]
+    edges = np.column_stack([xy, rng.uniform(-np.pi, np.pi, n_edges), rng.uniform(1, 10, n_edges)])
+    # neighbours within 3 px through a coarse grid
+    cell = np.floor(xy / 3.0).astype(np.int64)
+    key = cell[:, 0] * 100003 + cell[:, 1]
+    buckets: dict = {}
+    for i, k in enumerate(key.tolist()):
+        buckets.setdefault(k, []).append(i)
+
+    def near(i):
+        cx, cy = cell[i]
+        out = []
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                out += buckets.get(int((cx + dx) * 100003 + cy + dy), [])
+        return [j for j in out if j != i and np.hypot(*(xy[j] - xy[i])) < 3.0]
+
+    rows = []
+    for a in range(n_edges):
+        for _ in range(int(rng.integers(0, max_per_anchor + 1))):
+            L = int(rng.integers(2, width))
+            chain = [a]
+            while len(chain) < L:
+                cand = [j for j in near(chain[-1]) if j not in chain]
+                if not cand:
+                    break
+                chain.append(int(rng.choice(cand)))
+            if len(chain) < 2:
+                continue
+            row = np.zeros(width, np.uint32)
+            row[0] = a + 1
+            row[1:1 + len(chain)] = np.asarray(chain) + 1
+            rows.append(row)
+    chains = np.asarray(rows, np.uint32).reshape(-1, width)
+    return edges, chains
+
+
+def contour_rings(seed: int = 0, n_rings: int = 6, width: int = 5) -> tuple[np.ndarray, np.ndarray]:
+    """Closed contours: rings of 8 to 200 edges about 1 px apart, ids shuffled
+    across rings, each edge the anchor of one chain running along its ring (so
+    every link points the same way round and each ring is a cycle); one ring
+    has a 3 px gap and one runs the other way. Returns (edges, chains)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ring_pts, ring_ids = [], []
+    base = 0
+    for r in range(n_rings):
+        k = int(rng.integers(8, 200)) if r else 8
+        rad = k / (2 * np.pi)
+        t = np.arange(k) * 2 * np.pi / k
+        if r == 1:  # a gap: the last step is about 3 px
+            t = np.arange(k) * (2 * np.pi - 3.0 / rad) / (k - 1)
+        c = rng.uniform(0, 400, 2)
+        ring_pts.append(c + rad * np.column_stack([np.cos(t), np.sin(t)]))
+        seq = list(range(base, base + k))
+        if r == 2:
+            seq = seq[::-1]
+        ring_ids.append(seq)
+        base += k
+    n = base
+    perm = rng.permutation(n)  # position in ring order -> edge id
+    xy = np.zeros((n, 2))
+    for pts, seq in zip(ring_pts, ring_ids):
+        for p, s in zip(pts, seq):
+            xy[perm[s]] = p
+    edges = np.column_stack([xy, rng.uniform(-np.pi, np.pi, n), rng.uniform(1, 10, n)])
+    rows = []
+    for seq in ring_ids:
+        k = len(seq)
+        for i in range(k):
+            chain = [perm[seq[(i + j) % k]] for j in range(width - 1)]
+            row = np.zeros(width, np.uint32)
+            row[0] = chain[0] + 1
+            row[1:] = np.asarray(chain) + 1
+            rows.append(row)
+    chains = np.asarray(rows, np.uint32)
+    chains = chains[np.argsort(chains[:, 0], kind="stable")]
+    return edges, chains

@@ -43,7 +43,7 @@ extern "C" {
  * and ignored exactly as the reference ignores them (main.cpp:29,32,94-95). */
 typedef struct cvl_params {
     double nrad;             /* neighbour radius, px (3.5) */
-    double gap;              /* unused by the path (1.5) */
+    double gap;              /* unused by the curvelet path; the contour gap of cvl_run_contours (1.5) */
     double dx;               /* edge position uncertainty, px (0.4) */
     double dt_deg;           /* edge orientation uncertainty, degrees (15) */
     double dt_rad;           /* the same in radians, as CurveletCPU's ctor takes it (cpu_curvelet.hpp:82-83);
@@ -381,6 +381,60 @@ int cvl_engine_last_launch_count(cvl_engine *e);
  * register-resident dependent-chain loop; the roofline denominator for the
  * FP64-bound bundle kernel. */
 int cvl_measure_fp64_peak(cvl_engine *e, double *tflops);
+
+/* ---- Downstream: curvelets -> edgel link graph -> contour fragments ----------
+ * The reference's original_code stage after curvelet formation:
+ *   form_curvelet_process::construct_the_link_graph   (form_curvelet_process.cpp:453-520)
+ *   form_curvelet_process::extract_regular_contours_from_the_link_graph and
+ *   extract_one_chains_from_the_link_graph            (form_curvelet_process.cpp:529-654)
+ *   edgel_link_graph, curve_fragment_graph            (edgel_link_graph.hpp, curve_fragment_graph.hpp)
+ * Every curvelet with at least min_group_size edges links its consecutive edges
+ * (a link joins two edges in either direction; its direction is that of its first
+ * occurrence, anchors ascending); one-chains are then traced from each legal
+ * start edge in ascending id order, a step taken only while the two edges are
+ * closer than gap, and chains of more than 2 edges are kept. */
+typedef struct cvl_contour_params {
+    uint32_t min_group_size; /* construct_the_link_graph(4, ...), form_curvelet_process.cpp:79 */
+    double gap;              /* 1.5, original_code/main.cpp:146 */
+} cvl_contour_params;
+
+void cvl_contour_params_default(cvl_contour_params *p);
+
+typedef struct cvl_contours cvl_contours;
+
+/* Links in _cLinks order (parent id ascending, then creation order) and fragments
+ * in the order of their start edge (curve_fragment_graph::_frags). All ids are
+ * 0-based edge indices. Arrays live in page-locked memory owned by the result. */
+typedef struct cvl_contours_view {
+    int64_t num_links;
+    const int32_t *link_parent; /* edgel_link::_pe */
+    const int32_t *link_child;  /* edgel_link::_ce */
+    const int32_t *link_votes;  /* edgel_link::_vote */
+    int64_t num_fragments;
+    const int64_t *fragment_offsets; /* [num_fragments + 1] */
+    const int32_t *fragment_ids;
+    int32_t max_fragment_length; /* curve_fragment_graph::edgel_chain_max_length */
+    int32_t num_edges;
+    float device_ms; /* the stage's device time (cvl_run_contours: the whole path) */
+} cvl_contours_view;
+
+/* The stage on curvelets the caller holds: chains as cvl_result_view gives them
+ * ([num_curvelets][chain_width], column 0 = anchor + 1, then the chain, 1-based,
+ * zero-padded), rows grouped by anchor in ascending order. CVL_EINVAL for ids
+ * outside the map, rows out of anchor order, or chain_width outside [2, 64]. */
+int cvl_link_contours(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
+                      const uint32_t *chains, int64_t num_curvelets, int32_t chain_width,
+                      const cvl_contour_params *cp, cvl_contours **out);
+
+/* Edges -> curvelets -> link graph -> fragments in one pass on the device (the
+ * curvelets never leave it). curvelets_out may be NULL; otherwise it receives
+ * the curvelets as cvl_run returns them. cp NULL: the defaults, with p->gap. */
+int cvl_run_contours(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,
+                     const cvl_params *p, const cvl_contour_params *cp, cvl_result **curvelets_out,
+                     cvl_contours **out);
+
+int cvl_contours_get(const cvl_contours *c, cvl_contours_view *view);
+void cvl_contours_free(cvl_contours *c);
 
 #ifdef __cplusplus
 }

@@ -607,3 +607,198 @@ int orc_run(const double *edges, int num_edges, int sz, double nrad, double dx, 
     orc_csr_free(&g);
     return 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Downstream: curvelets -> edgel link graph -> contour fragments           */
+/* (original_code/form_curvelet_process.cpp:453-654, edgel_link_graph.hpp,  */
+/*  curve_fragment_graph.hpp)                                                */
+/* ---------------------------------------------------------------------- */
+
+typedef struct {
+    int pe, ce, votes;
+} orc_link;
+
+typedef struct {
+    int *v;
+    int n, cap;
+} orc_ivec;
+
+static void orc_ivec_push(orc_ivec *a, int x)
+{
+    if (a->n == a->cap) {
+        a->cap = a->cap ? 2 * a->cap : 4;
+        a->v = (int *)realloc(a->v, sizeof(int) * (size_t)a->cap);
+    }
+    a->v[a->n++] = x;
+}
+
+typedef struct {
+    int num_links;
+    int *link_pe, *link_ce, *link_votes; /* _cLinks order: parent id ascending, creation order */
+    int num_frags;
+    int64_t *frag_offsets;               /* [num_frags + 1] */
+    int *frag_ids;                       /* 0-based edge ids, fragment order */
+} orc_contours;
+
+void orc_contours_free(orc_contours *c)
+{
+    free(c->link_pe);
+    free(c->link_ce);
+    free(c->link_votes);
+    free(c->frag_offsets);
+    free(c->frag_ids);
+    memset(c, 0, sizeof(*c));
+}
+
+/* sq_distance of two edgel points, original_code/curvelet_utils.hpp:17-20 */
+static double orc_pt_sqd(const double *edges, int sz, int a, int b)
+{
+    const double *A = edges + (size_t)a * sz, *B = edges + (size_t)b * sz;
+    return (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]);
+}
+
+/* chains: row-major [num_curvelets][W] as the curvelet path writes them (column 0 =
+ * anchor + 1, then the ordered chain, 1-based, zero-padded), rows grouped by anchor
+ * in ascending anchor order. Returns 0, -1 on bad input. */
+int orc_link_contours(const double *edges, int num_edges, int sz, const unsigned *chains, int num_curvelets,
+                      int W, unsigned min_group_size, double gap, orc_contours *out)
+{
+    memset(out, 0, sizeof(*out));
+    if (num_edges <= 0 || sz < 4 || W < 2) return -1;
+    orc_ivec *clinks = (orc_ivec *)calloc((size_t)num_edges, sizeof(orc_ivec)); /* link indices */
+    orc_ivec *plinks = (orc_ivec *)calloc((size_t)num_edges, sizeof(orc_ivec));
+    orc_link *links = NULL;
+    int nl = 0, capl = 0;
+    /* construct_the_link_graph (form_curvelet_process.cpp:453-506): every curvelet
+     * of order >= min_group_size, anchors ascending, links each consecutive pair of
+     * its chain (form_links_from_a_curvelet, :509-520) */
+    int prev_anchor = -1;
+    for (int r = 0; r < num_curvelets; ++r) {
+        const unsigned *row = chains + (size_t)r * W;
+        const int a = (int)row[0] - 1;
+        if (a < 0 || a >= num_edges || a < prev_anchor) goto bad;
+        prev_anchor = a;
+        int len = 0;
+        while (len < W - 1 && row[1 + len]) {
+            if ((int)row[1 + len] > num_edges) goto bad;
+            ++len;
+        }
+        if ((unsigned)len < min_group_size) continue;
+        for (int k = 0; k + 1 < len; ++k) {
+            const int e1 = (int)row[1 + k] - 1, e2 = (int)row[2 + k] - 1;
+            /* link_edgels / are_linked (edgel_link_graph.hpp:228-265): a link between
+             * the two edgels in either direction takes the vote */
+            int found = -1;
+            for (int q = 0; q < clinks[e1].n && found < 0; ++q)
+                if (links[clinks[e1].v[q]].ce == e2) found = clinks[e1].v[q];
+            for (int q = 0; q < clinks[e2].n && found < 0; ++q)
+                if (links[clinks[e2].v[q]].ce == e1) found = clinks[e2].v[q];
+            if (found >= 0) {
+                links[found].votes += 1;
+                continue;
+            }
+            if (nl == capl) {
+                capl = capl ? 2 * capl : 1024;
+                links = (orc_link *)realloc(links, sizeof(orc_link) * (size_t)capl);
+            }
+            links[nl].pe = e1;
+            links[nl].ce = e2;
+            links[nl].votes = 1;
+            orc_ivec_push(&clinks[e1], nl);
+            orc_ivec_push(&plinks[e2], nl);
+            ++nl;
+        }
+    }
+    {
+        /* extract_one_chains_from_the_link_graph (form_curvelet_process.cpp:563-654) */
+        const double thres = gap * gap;
+        unsigned char *linked = (unsigned char *)calloc((size_t)num_edges, 1);
+        int *fwd = (int *)malloc(sizeof(int) * ((size_t)num_edges + 2));
+        int *bwd = (int *)malloc(sizeof(int) * ((size_t)num_edges + 2));
+        orc_ivec ids = {0};
+        int64_t total = 0;
+        out->frag_offsets = (int64_t *)malloc(sizeof(int64_t) * ((size_t)num_edges + 1));
+        out->frag_offsets[0] = 0;
+#define ORC_LEGAL(e) (!linked[e] && plinks[e].n <= 1 && clinks[e].n <= 1) /* edgel_link_graph.hpp:218-224 */
+        for (int i = 0; i < num_edges; ++i) {
+            if (linked[i]) continue;
+            /* edgel_is_legal_first_edgel, edgel_link_graph.hpp:208-215 */
+            if (!(plinks[i].n == 1 && clinks[i].n == 1 &&
+                  links[plinks[i].v[0]].pe != links[clinks[i].v[0]].ce))
+                continue;
+            int nf = 0, nb = 0;
+            linked[i] = 1;
+            int eA = links[clinks[i].v[0]].ce, eB;
+            if (orc_pt_sqd(edges, sz, i, eA) < thres) fwd[nf++] = eA;
+            while (ORC_LEGAL(eA)) {
+                linked[eA] = 1;
+                if (clinks[eA].n == 0) break;
+                eB = eA;
+                eA = links[clinks[eA].v[0]].ce;
+                if (orc_pt_sqd(edges, sz, eB, eA) < thres)
+                    fwd[nf++] = eA;
+                else
+                    break;
+            }
+            if (eA != i) {
+                eA = links[plinks[i].v[0]].pe;
+                if (orc_pt_sqd(edges, sz, i, eA) < thres) bwd[nb++] = eA;
+            }
+            while (ORC_LEGAL(eA)) {
+                linked[eA] = 1;
+                if (plinks[eA].n == 0) break;
+                eB = eA;
+                eA = links[plinks[eA].v[0]].pe;
+                if (orc_pt_sqd(edges, sz, eB, eA) < thres)
+                    bwd[nb++] = eA;
+                else
+                    break;
+            }
+            if (nb + 1 + nf > 2) { /* prune the short ones, :648-651 */
+                for (int q = nb - 1; q >= 0; --q) orc_ivec_push(&ids, bwd[q]);
+                orc_ivec_push(&ids, i);
+                for (int q = 0; q < nf; ++q) orc_ivec_push(&ids, fwd[q]);
+                total += nb + 1 + nf;
+                out->frag_offsets[++out->num_frags] = total;
+            }
+        }
+#undef ORC_LEGAL
+        out->frag_ids = ids.v ? ids.v : (int *)malloc(sizeof(int));
+        free(linked);
+        free(fwd);
+        free(bwd);
+    }
+    /* the link list in _cLinks order (parent ascending, creation order) */
+    out->num_links = nl;
+    out->link_pe = (int *)malloc(sizeof(int) * ((size_t)nl + 1));
+    out->link_ce = (int *)malloc(sizeof(int) * ((size_t)nl + 1));
+    out->link_votes = (int *)malloc(sizeof(int) * ((size_t)nl + 1));
+    {
+        int k = 0;
+        for (int e = 0; e < num_edges; ++e)
+            for (int q = 0; q < clinks[e].n; ++q) {
+                const orc_link *l = &links[clinks[e].v[q]];
+                out->link_pe[k] = l->pe;
+                out->link_ce[k] = l->ce;
+                out->link_votes[k] = l->votes;
+                ++k;
+            }
+    }
+    for (int e = 0; e < num_edges; ++e) {
+        free(clinks[e].v);
+        free(plinks[e].v);
+    }
+    free(clinks);
+    free(plinks);
+    free(links);
+    return 0;
+bad:
+    for (int e = 0; e < num_edges; ++e) {
+        free(clinks[e].v);
+        free(plinks[e].v);
+    }
+    free(clinks);
+    free(plinks);
+    free(links);
+    return -1;
+}

@@ -19,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libcvl_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcvlref.so")
 REF_CLI = os.path.join(HERE, "_ref", "CURVELET")
+ORIG_SO = os.path.join(HERE, "_ref", "liborigref.so")
 
 # reference defaults, cpu_curvelet/param_settings.hpp:9-24
 DEFAULTS = dict(nrad=3.5, dx=0.4, dt_deg=15.0, max_k=0.3, sx=0.1, st=0.08,
@@ -261,3 +262,106 @@ def parse_edges_f32(path: str, values_per_edge: int = 4) -> np.ndarray:
                 raise ValueError(f"{path}: expected {values_per_edge} values, found {len(toks)}")
             rows.append([libc.strtof(t.encode(), None) for t in toks])
     return np.asarray(rows, dtype=np.float32)
+
+
+# ---- downstream: curvelets -> edgel link graph -> contour fragments ----------------
+class _OrcContours(C.Structure):
+    _fields_ = [("num_links", C.c_int), ("link_pe", C.POINTER(C.c_int)), ("link_ce", C.POINTER(C.c_int)),
+                ("link_votes", C.POINTER(C.c_int)), ("num_frags", C.c_int),
+                ("frag_offsets", C.POINTER(C.c_int64)), ("frag_ids", C.POINTER(C.c_int))]
+
+
+class _OrigContours(C.Structure):
+    _fields_ = [("num_links", C.c_int32), ("link_pe", C.POINTER(C.c_int32)), ("link_ce", C.POINTER(C.c_int32)),
+                ("link_votes", C.POINTER(C.c_int32)), ("num_frags", C.c_int32),
+                ("frag_offsets", C.POINTER(C.c_int64)), ("frag_ids", C.POINTER(C.c_int32)),
+                ("seconds", C.c_double)]
+
+
+@dataclass
+class Contours:
+    """links: [L, 3] (parent id, child id, votes), 0-based, in _cLinks order (parent
+    ascending, creation order); fragments: CSR (offsets [F+1], ids 0-based)."""
+    links: np.ndarray
+    frag_offsets: np.ndarray
+    frag_ids: np.ndarray
+    seconds: float = 0.0
+
+    @property
+    def num_frags(self) -> int:
+        return int(self.frag_offsets.shape[0] - 1)
+
+    def fragments(self):
+        return [self.frag_ids[self.frag_offsets[i]:self.frag_offsets[i + 1]] for i in range(self.num_frags)]
+
+
+def _contours_from(o, seconds=0.0) -> Contours:
+    L = o.num_links
+    links = np.column_stack([_arr(o.link_pe, L, np.int32), _arr(o.link_ce, L, np.int32),
+                             _arr(o.link_votes, L, np.int32)]) if L else np.zeros((0, 3), np.int32)
+    offs = _arr(o.frag_offsets, o.num_frags + 1, np.int64)
+    ids = _arr(o.frag_ids, int(offs[-1]), np.int32) if offs[-1] else np.zeros(0, np.int32)
+    return Contours(links.astype(np.int32), offs, ids, seconds)
+
+
+def _contour_args(edges, chains, forward=None):
+    e, ep, n, sz = _edges_arg(edges)
+    ch = np.ascontiguousarray(chains, dtype=np.uint32)
+    assert ch.ndim == 2
+    return e, ep, n, sz, ch
+
+
+def link_contours(edges, chains, min_group_size=4, gap=1.5) -> Contours:
+    """The C restatement (oracle/cvl_oracle.c: orc_link_contours)."""
+    L = lib()
+    if not hasattr(L, "_contours_set"):
+        L.orc_link_contours.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_uint), C.c_int,
+                                        C.c_int, C.c_uint, C.c_double, C.POINTER(_OrcContours)]
+        L.orc_contours_free.argtypes = [C.POINTER(_OrcContours)]
+        L._contours_set = True
+    e, ep, n, sz, ch = _contour_args(edges, chains)
+    o = _OrcContours()
+    rc = L.orc_link_contours(ep, n, sz, ch.ctypes.data_as(C.POINTER(C.c_uint)), ch.shape[0], ch.shape[1],
+                             min_group_size, gap, C.byref(o))
+    if rc != 0:
+        raise ValueError(f"orc_link_contours: {rc}")
+    try:
+        return _contours_from(o)
+    finally:
+        L.orc_contours_free(C.byref(o))
+
+
+_orig = None
+
+
+def orig_available() -> bool:
+    return os.path.exists(ORIG_SO)
+
+
+def ref_link_contours(edges, chains, forward=None, min_group_size=4, gap=1.5) -> Contours:
+    """The reference's own original_code link graph + one-chain extraction
+    (oracle/orig_harness.cpp, built into oracle/_ref/liborigref.so)."""
+    global _orig
+    if _orig is None:
+        if not os.path.exists(ORIG_SO):
+            raise FileNotFoundError("original_code harness not built: " + ORIG_SO)
+        L = C.CDLL(ORIG_SO)
+        L.origref_link_contours.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_uint32),
+                                            C.c_int, C.c_int, C.POINTER(C.c_uint8), C.c_uint, C.c_double,
+                                            C.POINTER(_OrigContours)]
+        L.origref_contours_free.argtypes = [C.POINTER(_OrigContours)]
+        _orig = L
+    e, ep, n, sz, ch = _contour_args(edges, chains)
+    fw = None
+    if forward is not None:
+        fw = np.ascontiguousarray(forward, dtype=np.uint8)
+    o = _OrigContours()
+    rc = _orig.origref_link_contours(ep, n, sz, ch.ctypes.data_as(C.POINTER(C.c_uint32)), ch.shape[0],
+                                     ch.shape[1], fw.ctypes.data_as(C.POINTER(C.c_uint8)) if fw is not None
+                                     else None, min_group_size, gap, C.byref(o))
+    if rc != 0:
+        raise ValueError(f"origref_link_contours: {rc}")
+    try:
+        return _contours_from(o, o.seconds)
+    finally:
+        _orig.origref_contours_free(C.byref(o))

@@ -1,0 +1,110 @@
+"""The downstream stage on the GPU (cvl_link_contours / cvl_run_contours): the
+edgel link graph (links, votes, _cLinks order) and the contour fragments equal
+the reference's original_code output (tests/golden/contours.npz) and the pinned
+C restatement, bit for bit: on the sample files' curvelets, on fuzzed curvelet
+sets with junctions, reversed links, gaps and cycles, on rings, and at full
+size on the 1920x1080 map through the fused edges -> contours pass."""
+import os
+
+import numpy as np
+import pytest
+
+import curvelet_construction_on_gpu_b200 as cvl
+from curvelet_construction_on_gpu_b200 import synth
+from tests.test_contours_cpu import _params, assert_same_contours
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def gc():
+    return np.load(os.path.join(GOLDEN, "contours.npz"))
+
+
+def _cp(p):
+    mg, gap = p.split("_")
+    return cvl.ContourParams(int(mg), float(gap))
+
+
+def _same(a, b):
+    return (np.array_equal(a.links, b.links) and np.array_equal(a.frag_offsets, b.frag_offsets)
+            and np.array_equal(a.frag_ids, b.frag_ids))
+
+
+@pytest.mark.parametrize("name", ["TO_edges_digit1", "TO_edges_ABC_0006_thresh1"])
+def test_reference_curvelets(engine, gc, golden_files, name):
+    e, ch = golden_files[f"{name}/edges"], golden_files[f"{name}/chains"]
+    for p in _params(gc, f"file/{name}"):
+        assert_same_contours(engine.link_contours(e, ch, _cp(p)), gc, f"file/{name}/{p}")
+
+
+def test_to_edges_fused_and_staged(engine, gc, golden_files):
+    e = golden_files["TO_edges/edges"]
+    for p in _params(gc, "file/TO_edges"):
+        res, c = engine.run_contours(e, contour_params=_cp(p))
+        assert res.num_curvelets == 67735
+        assert_same_contours(c, gc, f"file/TO_edges/{p}")
+        assert_same_contours(engine.link_contours(e, res.chains, _cp(p)), gc, f"file/TO_edges/{p}")
+
+
+@pytest.mark.parametrize("case", ["fuzz0", "fuzz1", "rings0", "rings1"])
+def test_fuzz_and_rings(engine, gc, case):
+    e, ch = gc[f"{case}/edges"], gc[f"{case}/chains"]
+    for p in _params(gc, case):
+        c = engine.link_contours(e, ch, _cp(p))
+        assert_same_contours(c, gc, f"{case}/{p}")
+    print(f"[contours] {case}: {c.links.shape[0]} links, {c.num_frags} fragments, {c.device_ms:.3f} ms")
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13])
+def test_fuzz_vs_restatement(engine, oracle, seed):
+    e, ch = synth.contour_fuzz(seed, n_edges=4000, width=int(4 + seed % 3 * 2), max_per_anchor=6)
+    for mg, gap in ((2, 1.5), (4, 2.5), (0, 1.0), (3, 0.0)):
+        a = engine.link_contours(e, ch, cvl.ContourParams(mg, gap))
+        b = oracle.link_contours(e, ch, mg, gap)
+        assert _same(a, b), (seed, mg, gap)
+
+
+def test_plain_hd_full_size(engine, oracle):
+    """The 1920x1080 map (about 250k edges, 500k curvelets): fused on the device."""
+    e = synth.plain_hd(1000)
+    for cp in (cvl.ContourParams(), cvl.ContourParams(2, 1.5)):
+        res, c = engine.run_contours(e, contour_params=cp)
+        b = oracle.link_contours(e, res.chains, cp.min_group_size, cp.gap)
+        assert _same(c, b)
+        print(f"[contours plain_hd] mg={cp.min_group_size}: {c.links.shape[0]} links, {c.num_frags} fragments, "
+              f"longest {int(np.diff(c.frag_offsets).max())}, whole path {c.device_ms:.2f} ms")
+    # gap comes from CurveletParams.gap when no contour parameters are given
+    _, c1 = engine.run_contours(e, cvl.CurveletParams(gap=2.0), want_curvelets=False)
+    _, c2 = engine.run_contours(e, contour_params=cvl.ContourParams(4, 2.0), want_curvelets=False)
+    assert _same(c1, c2)
+
+
+def test_dense_map_vs_restatement(engine, oracle):
+    e = synth.dense_4k(4000)[:400000]
+    res, c = engine.run_contours(e, contour_params=cvl.ContourParams(2, 1.5))
+    assert _same(c, oracle.link_contours(e, res.chains, 2, 1.5))
+
+
+def test_edge_cases(engine):
+    e, ch = synth.contour_fuzz(3, n_edges=500)
+    c = engine.link_contours(e, ch[:0])  # no curvelets
+    assert c.links.shape == (0, 3) and c.num_frags == 0
+    c = engine.link_contours(e, ch, cvl.ContourParams(2, 0.0))  # nothing is close enough
+    assert c.num_frags == 0 and c.links.shape[0] > 0
+    c = engine.link_contours(e, ch, cvl.ContourParams(99, 1.5))  # no curvelet is long enough
+    assert c.links.shape[0] == 0 and c.num_frags == 0
+    bad = ch.copy()
+    bad[5, 2] = 501  # an id past the map
+    with pytest.raises(cvl.CvlError):
+        engine.link_contours(e, bad)
+    with pytest.raises(cvl.CvlError):
+        engine.link_contours(e, ch[::-1])  # anchors out of order
+    with pytest.raises(cvl.CvlError):
+        engine.link_contours(e, np.zeros((3, 65), np.uint32) + 1)
+    with pytest.raises(cvl.CvlError):
+        engine.link_contours(e, ch, cvl.ContourParams(4, -1.0))
+    # the engine stays usable after the errors
+    assert engine.link_contours(e, ch).links.shape[0] > 0
