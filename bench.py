@@ -17,6 +17,11 @@ one batch of seeded synthetic edges. Workloads:
   served      only the served stream, at each rate of --rates
   stress      16 dense 3840x2160 maps interleaved with 1,024 small 640x480 maps,
               Poisson at 150 maps/s; small-map p99 apart
+  contours    the downstream stage fused behind the path: one 1920x1080 map,
+              edges -> curvelets -> edgel link graph -> contour fragments
+              (cvl_run_contours), the stage's own time and roofline apart; the
+              CPU baseline adds the reference's original_code link graph and
+              one-chain extraction to its cpu_curvelet time
 
 value: edges/s with the edges already in HBM (CUDA events on the engine's
 stream around each step, L2 flushed between steps). e2e: the same metric
@@ -66,7 +71,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="mixed64",
-                    choices=["mixed64", "plain_hd", "plain_small", "served", "stress"])
+                    choices=["mixed64", "plain_hd", "plain_small", "served", "stress", "contours"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-served", action="store_true")
@@ -84,6 +89,9 @@ def _workload(name: str, rank: int):
     from curvelet_construction_on_gpu_b200 import synth
     if name == "plain_hd":
         return [synth.plain_hd(1000 + rank)], {"image": "1920x1080", "curves": 1500, "clutter": 0.2}
+    if name == "contours":
+        return [synth.plain_hd(1000 + rank)], {"image": "1920x1080", "curves": 1500, "clutter": 0.2,
+                                               "min_group_size": 4, "gap": 1.5}
     if name == "plain_small":
         return [synth.plain_small(0 + rank)], {"image": "480x320", "curves": 50, "clutter": 0.1}
     if name == "stress":
@@ -535,6 +543,143 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     eng.close()
 
 
+def _contour_algorithmic_bytes(n_curv: int, width: int, c) -> int:
+    """The stage's minimal DRAM traffic: the chains read once (4 B per entry),
+    the links written (3 x 4 B), the fragments written (4 B per id, 8 B per
+    offset), and two edge positions (2 x 16 B) read per fragment step."""
+    return int(4 * n_curv * width + 12 * c.links.shape[0] + 4 * c.frag_ids.shape[0]
+               + 8 * (c.num_frags + 1) + 32 * c.frag_ids.shape[0])
+
+
+def run_contours(args, maps, cfg, world, rank, local, pg):
+    import curvelet_construction_on_gpu_b200 as cvl
+    eng = cvl.Engine(device=local)
+    e = maps[0]
+    cp = cvl.ContourParams(cfg["min_group_size"], cfg["gap"])
+    n_edges = int(e.shape[0])
+    pinned = _pinned(e)
+    for _ in range(args.warmup):
+        eng.run_contours(pinned, contour_params=cp, want_curvelets=False)
+    _barrier(pg)
+    step_ms, stage_ms, launches = [], [], 0
+    with _Clocks(local) as clk:
+        for _ in range(args.steps):
+            eng.flush_l2()
+            _, c = eng.run_contours(pinned, contour_params=cp, want_curvelets=False)
+            step_ms.append(c.device_ms)
+            kt = _stage_sums(eng.kernel_times())
+            stage_ms.append(kt)
+            launches = eng.launch_count()
+    _barrier(pg)
+    sum_ms = _max_over_ranks(pg, float(np.sum(step_ms)))
+    value = _sum_over_ranks(pg, float(n_edges)) * args.steps / (sum_ms / 1e3)
+    res, c = eng.run_contours(pinned, contour_params=cp)
+    n_curv, width = res.num_curvelets, res.chains.shape[1]
+    e2e = None
+    if not args.no_e2e:
+        _barrier(pg)
+        t0 = time.perf_counter()
+        bo = 0
+        for _ in range(args.steps):
+            r2, c2 = eng.run_contours(pinned, contour_params=cp)
+            bo += r2.chains.nbytes + r2.info.nbytes + c2.links.nbytes + c2.frag_offsets.nbytes + c2.frag_ids.nbytes
+            del r2, c2
+        wall = _max_over_ranks(pg, time.perf_counter() - t0)
+        e2e = {"value": _sum_over_ranks(pg, float(n_edges)) * args.steps / wall, "unit": METRIC,
+               "h2d_bytes_per_step": int(e.nbytes), "d2h_bytes_per_step": int(bo // args.steps),
+               "path": "cvl_run_contours (C ABI): pinned host edges in; curvelets, links and fragments out"}
+    if rank != 0:
+        eng.close()
+        return
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    cms = float(np.mean([k.get("contours", 0.0) for k in stage_ms]))
+    alg = _contour_algorithmic_bytes(n_curv, width, c)
+    achieved = alg / (cms / 1e3) / 1e9 if cms > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sum_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators, curvelet_construction_on_gpu_b200/synth.py)",
+        "config": dict(workload="contours", edges_per_gpu=n_edges, curvelets_per_gpu=n_curv,
+                       links=int(c.links.shape[0]), fragments=int(c.num_frags), fragment_ids=int(c.frag_ids.shape[0]),
+                       l2="flushed between steps", parallelism=f"replicas x{world}", **cfg),
+        "stage_ms": {k: float(np.mean([d.get(k, 0.0) for d in stage_ms])) for k in stage_ms[0]},
+        "contour_stage": {"ms": cms, "edges_per_s": n_edges / (cms / 1e3) if cms > 0 else None,
+                          "links_per_s": c.links.shape[0] / (cms / 1e3) if cms > 0 else None},
+        "roofline": {"bound": "hbm", "kernel": "contour stage (k_link_* + k_trace_* + k_frag_*)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                     "algorithmic_bytes": alg, "traffic": None,
+                     "note": "the stage walks contours edge by edge (one thread per component): latency-bound, "
+                             "so the HBM fraction is low by nature"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        if O.ref_available() and O.orig_available():
+            r = O.ref_run(e, nthreads=threads)
+            ref_s = (r.ms["csr"] + r.ms["pairwise"] + r.ms["greedy"]) / 1e3
+            fw = (r.info[:, 0] > 0).astype(np.uint8)
+            rc = O.ref_link_contours(e, r.chains, fw, cp.min_group_size, cp.gap)
+            line["cpu_baseline"] = {
+                "value": n_edges / (ref_s + rc.seconds), "unit": METRIC, "cores": threads, "kind": "reference",
+                "sample": f"the whole map ({n_edges} edges): cpu_curvelet CSR + pairwise + greedy on {threads} "
+                          f"threads ({ref_s * 1e3:.1f} ms) + original_code construct_the_link_graph + "
+                          f"extract_regular_contours_from_the_link_graph, single-threaded as written "
+                          f"({rc.seconds * 1e3:.1f} ms)",
+                "contour_stage_ms": rc.seconds * 1e3,
+                "same_result": bool(np.array_equal(rc.links, c.links) and np.array_equal(rc.frag_ids, c.frag_ids)
+                                    and np.array_equal(rc.frag_offsets, c.frag_offsets))}
+        else:
+            t0 = time.perf_counter()
+            r = O.run(e, nthreads=threads)
+            oc = O.link_contours(e, r.chains, cp.min_group_size, cp.gap)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": n_edges / dt, "unit": METRIC, "cores": threads, "kind": "port",
+                                    "sample": f"the whole map ({n_edges} edges), oracle restatement"}
+    print(json.dumps(line))
+    eng.close()
+
+
+def run_reference_contours(args, maps, cfg, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not (O.ref_available() and O.orig_available()):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref harnesses were not built "
+                          "(the reference sources were absent at build time)"}))
+        return
+    threads = os.cpu_count() or 1
+    e = maps[0]
+    r = O.ref_run(e, nthreads=threads)
+    fw = (r.info[:, 0] > 0).astype(np.uint8)
+    for _ in range(max(1, args.warmup)):
+        O.ref_link_contours(e, r.chains, fw, cfg["min_group_size"], cfg["gap"])
+    step_s = []
+    for _ in range(args.steps):
+        r = O.ref_run(e, nthreads=threads)
+        rc = O.ref_link_contours(e, r.chains, fw, cfg["min_group_size"], cfg["gap"])
+        step_s.append((r.ms["csr"] + r.ms["pairwise"] + r.ms["greedy"]) / 1e3 + rc.seconds)
+    ms = 1e3 * float(np.mean(step_s))
+    value = e.shape[0] / (ms / 1e3)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": dict(workload="contours", edges=int(e.shape[0]), **cfg),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+                         "sample": "the whole map per step: cpu_curvelet phases + original_code link graph "
+                                   "and one-chain extraction"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
 def run_served(args, maps, cfg, world, rank, local, pg):
     """The served stream alone, swept over --rates (one JSON line)."""
     rates = [float(r) for r in args.rates.split(",") if r]
@@ -573,8 +718,12 @@ def main():
     world, rank, local, pg = _dist_init(args)
     maps, cfg = _workload(args.workload, rank)
     try:
-        if args.impl == "reference":
+        if args.impl == "reference" and args.workload == "contours":
+            run_reference_contours(args, maps, cfg, world, rank)
+        elif args.impl == "reference":
             run_reference(args, maps, cfg, world, rank)
+        elif args.workload == "contours":
+            run_contours(args, maps, cfg, world, rank, local, pg)
         elif args.workload == "served":
             run_served(args, maps, cfg, world, rank, local, pg)
         elif args.workload == "stress":

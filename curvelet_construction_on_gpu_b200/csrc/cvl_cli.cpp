@@ -45,6 +45,10 @@ void print_usage(const char *prog) {
               << "  --st <val>                 Angle sampling step in radians (default: 0.08)\n"
               << "  --edge-data-sz <N>         Values per edge in input file (default: 4)\n"
               << "  --max-candidates <N>       Max neighbors per anchor in CSR build (default: 128)\n"
+              << "  --fragments <file>         Also write the contour fragments (edgel link graph one-chains)\n"
+              << "                             to ../outputs/<file>, one fragment per row, 1-based ids\n"
+              << "  --gap <val>                Fragment gap: consecutive edges closer than this (default: 1.5)\n"
+              << "  --link-min-group <N>       Curvelets with at least N edges form links (default: 4)\n"
               << "  --help                     Show this help message\n";
 }
 
@@ -83,7 +87,7 @@ bool parse_int(const char *arg, const char *name, int &v) {
 
 // Flag table of param_settings.hpp:86-155.
 bool parse_args(int argc, char **argv, CliParams &cp, bool &use_double, std::string &out_file, int &nthreads,
-                bool &show_help) {
+                bool &show_help, std::string &frag_file, cvl_contour_params &lp) {
     show_help = false;
     for (int i = 1; i < argc; i++) {
         const char *a = argv[i];
@@ -128,6 +132,13 @@ bool parse_args(int argc, char **argv, CliParams &cp, bool &use_double, std::str
             if (!parse_int(next(), "--edge-data-sz", cp.p.edge_data_sz)) return false;
         } else if (!std::strcmp(a, "--max-candidates") && has) {
             if (!parse_uns(next(), "--max-candidates", cp.p.max_candidates)) return false;
+        } else if (!std::strcmp(a, "--fragments") && has) {  // the downstream stage, not in cpu_curvelet
+            frag_file = next();
+        } else if (!std::strcmp(a, "--gap") && has) {
+            if (!parse_num(next(), "--gap", cp.p.gap)) return false;
+            lp.gap = cp.p.gap;
+        } else if (!std::strcmp(a, "--link-min-group") && has) {
+            if (!parse_uns(next(), "--link-min-group", lp.min_group_size)) return false;
         } else {
             std::cerr << "Unknown argument: " << a << std::endl;
             print_usage(argv[0]);
@@ -200,7 +211,14 @@ int main(int argc, char **argv) {
     CliParams cp;
     cvl_params_default(&cp.p);
     bool help = false;
-    if (!parse_args(argc, argv, cp, use_double, out_file, nthreads, help)) return help ? 0 : 1;
+    std::string frag_file;
+    cvl_contour_params lp;
+    cvl_contour_params_default(&lp);
+    if (!parse_args(argc, argv, cp, use_double, out_file, nthreads, help, frag_file, lp)) return help ? 0 : 1;
+    if (!frag_file.empty() && !use_double) {
+        std::cerr << "Error: --fragments runs in double only" << std::endl;
+        return 1;
+    }
     (void)nthreads;
     std::cout << "Using scalar type: " << (use_double ? "double" : "float") << std::endl;
     // run_curvelet<double> or run_curvelet<float> (main.cpp:110)
@@ -217,8 +235,11 @@ int main(int argc, char **argv) {
         return 1;
     }
     cvl_result *res = nullptr;
-    const int rc = use_double ? cvl_run(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &res)
-                              : cvl_run_f32(eng, edges_f.data(), n, cp.p.edge_data_sz, &cp.p, &res);
+    cvl_contours *frags = nullptr;
+    const int rc = !frag_file.empty()
+                       ? cvl_run_contours(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &lp, &res, &frags)
+                   : use_double ? cvl_run(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &res)
+                                : cvl_run_f32(eng, edges_f.data(), n, cp.p.edge_data_sz, &cp.p, &res);
     if (rc != CVL_OK) {
         std::cerr << "Error: " << cvl_last_error() << std::endl;
         cvl_engine_destroy(eng);
@@ -254,6 +275,24 @@ int main(int argc, char **argv) {
                 f << "\n";
             }
         }
+    }
+    if (frags) {
+        // curve_fragment_graph::get_output_array (output type 1 of original_code/main.cpp): one
+        // fragment per row, 1-based ids, as wide as the longest fragment, zero-padded
+        cvl_contours_view cv;
+        cvl_contours_get(frags, &cv);
+        std::cout << "Link graph: " << cv.num_links << " links; contour fragments: " << cv.num_fragments
+                  << " (longest " << cv.max_fragment_length << ")" << std::endl;
+        std::ofstream f;
+        if (open_out(frag_file, f)) {
+            for (int64_t i = 0; i < cv.num_fragments; i++) {
+                const int64_t b = cv.fragment_offsets[i], e = cv.fragment_offsets[i + 1];
+                for (int64_t j = 0; j < cv.max_fragment_length; j++)
+                    f << (b + j < e ? cv.fragment_ids[b + j] + 1 : 0) << "\t";
+                f << "\n";
+            }
+        }
+        cvl_contours_free(frags);
     }
     cvl_result_free(res);
     cvl_engine_destroy(eng);

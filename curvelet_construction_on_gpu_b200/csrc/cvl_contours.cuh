@@ -213,6 +213,10 @@ __device__ void heap_sort(unsigned *a, long long n) {
 
 // Replays extract_one_chains_from_the_link_graph over one component (entered at
 // `start`: a path's head, or a cycle's smallest id), start edges ascending.
+// Region bound: a trace pushes, on each side, at most one edge it does not mark
+// (the step that ends it) besides the edges it marks; every edge of the component
+// is marked at most once and the start edge is not stored. So a component of m
+// edges and f start edges stores at most m + f ids; m + 2f are reserved.
 __device__ void trace_component(const Graph &g, const FragOut &o, int start) {
     long long m = 0, f = 0;
     int v = start;

@@ -108,3 +108,26 @@ def test_edge_cases(engine):
         engine.link_contours(e, ch, cvl.ContourParams(4, -1.0))
     # the engine stays usable after the errors
     assert engine.link_contours(e, ch).links.shape[0] > 0
+
+
+@pytest.mark.parametrize("key", ["TO_edges_digit1", "TO_edges_ABC_0006_thresh1"])
+def test_cli_fragments_file(tmp_path, gc, golden_files, key):
+    """CURVELET --fragments writes the fragment map (output type 1 layout) next to
+    the usual outputs, which stay byte-identical to the reference program's."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cli_bin = os.path.join(root, "curvelet_construction_on_gpu_b200", "bin", "CURVELET")
+    for d in ("bin", "test_files", "outputs"):
+        (tmp_path / d).mkdir(exist_ok=True)
+    synth.write_edge_file(str(tmp_path / "test_files" / f"{key}.txt"), golden_files[f"{key}/edges"])
+    r = subprocess.run([cli_bin, "--double", "--edge-file", f"{key}.txt", "--output", f"chain_{key}.txt",
+                        "--fragments", f"frag_{key}.txt", "--link-min-group", "3", "--gap", "2.0"],
+                       cwd=tmp_path / "bin", capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    cli = np.load(os.path.join(GOLDEN, "cli_outputs.npz"))
+    assert (tmp_path / "outputs" / f"chain_{key}.txt").read_bytes() == cli[f"{key}/chain"].tobytes()
+    assert (tmp_path / "outputs" / f"info_{key}.txt").read_bytes() == cli[f"{key}/info"].tobytes()
+    want = cvl.Contours(gc[f"file/{key}/3_2.0/links"], gc[f"file/{key}/3_2.0/frag_offsets"],
+                        gc[f"file/{key}/3_2.0/frag_ids"], 0).as_array()
+    got = (tmp_path / "outputs" / f"frag_{key}.txt").read_text()
+    assert got == "".join("".join(f"{v}\t" for v in row) + "\n" for row in want.tolist())
