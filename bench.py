@@ -25,8 +25,8 @@ one batch of seeded synthetic edges. Workloads:
 
 value: edges/s with the edges already in HBM (CUDA events on the engine's
 stream around each step, L2 flushed between steps). e2e: the same metric
-through the C ABI call a user makes (cvl_run: pinned host edges in, chains and
-info out, copies inside the timed region). With N GPUs (torchrun) every rank
+through the C ABI call a user makes (cvl_run for one map, cvl_run_maps for many:
+pinned host edges in, chains and info out, copies inside the timed region). With N GPUs (torchrun) every rank
 processes its own instance of the workload (replicas, weak scaling) and the
 step time is the max over ranks; there is no data-path collective.
 
@@ -456,12 +456,8 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
             pinned = _pinned(np.concatenate(maps, axis=0))
             counts = np.array([m.shape[0] for m in maps], np.int32)
             # untimed pass: the result pool's page-locked blocks are allocated once
-            b = eng.upload_ragged(pinned, counts)
-            br = eng.run_batch(b)
-            held = [br.take_map(mi) for mi in range(len(maps))]
+            held = eng.run_maps(pinned, counts=counts)
             del held
-            br.close()
-            b.close()
         _barrier(pg)
         t0 = time.perf_counter()
         bo = 0
@@ -470,21 +466,16 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
                 res = eng.run(pinned)
                 bo += res.chains.nbytes + res.info.nbytes
             else:
-                b = eng.upload_ragged(pinned, counts)
-                br = eng.run_batch(b)
-                for mi in range(len(maps)):
-                    res = br.take_map(mi)
+                for res in eng.run_maps(pinned, counts=counts):
                     bo += res.chains.nbytes + res.info.nbytes
                     del res
-                br.close()
-                b.close()
         wall = time.perf_counter() - t0
         wall = _max_over_ranks(pg, wall)
         e2e = {"value": _sum_over_ranks(pg, float(n_edges)) * args.steps / wall, "unit": METRIC,
                "h2d_bytes_per_step": int(sum(m.nbytes for m in maps)), "d2h_bytes_per_step": int(bo // args.steps),
                "path": ("cvl_run (C ABI), pinned host edges" if len(maps) == 1 else
-                        "cvl_batch_upload + cvl_batch_run + cvl_batch_result_take_map per map (C ABI), "
-                        "pinned host edges")}
+                        "cvl_run_maps (C ABI): pinned host edges in, one result per map out; groups of maps "
+                        "pipelined, result copies overlapping the next group's compute")}
 
     served = None
     if len(maps) > 1 and not args.no_served and cfg.get("_labels"):

@@ -147,6 +147,8 @@ SIGNATURES = [
     ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),
     ("cvl_engine_last_launch_count", C.c_int, [_vp]),
     ("cvl_measure_fp64_peak", C.c_int, [_vp, _dp]),
+    ("cvl_run_maps", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(CvlParams),
+                               C.c_int64, C.POINTER(_vp)]),
     ("cvl_contour_params_default", None, [C.POINTER(CvlContourParams)]),
     ("cvl_link_contours", C.c_int, [_vp, _dp, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.c_int64, C.c_int32,
                                     C.POINTER(CvlContourParams), C.POINTER(_vp)]),

@@ -256,6 +256,26 @@ class Engine:
         check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
         return _view_to_result(v, owner)
 
+    def run_maps(self, maps, params: CurveletParams | None = None, dt_rad: float = 0.0,
+                 group_edges: int = 0, counts=None) -> list:
+        """Many maps, host to host (cvl_run_maps): one Result per map, as run()
+        would give it; the result copies of one group of maps overlap the compute
+        of the next. maps: a list of [n_i, sz] arrays, or one array of all rows
+        back to back with counts."""
+        params = params or CurveletParams()
+        if counts is None:
+            cnt = np.array([np.asarray(m).shape[0] for m in maps], np.int32)
+            e = maps[0] if len(maps) == 1 else np.concatenate([np.asarray(m, np.float64) for m in maps])
+        else:
+            cnt = np.ascontiguousarray(counts, dtype=np.int32)
+            e = maps
+        e = _edges(e)
+        p = params.to_c(dt_rad)
+        hs = (C.c_void_p * len(cnt))()
+        check(self._lib.cvl_run_maps(self._h, e.ctypes.data_as(_abi._dp), cnt.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     len(cnt), e.shape[1], C.byref(p), int(group_edges), hs), "cvl_run_maps")
+        return [_result_from_handle(self._lib, C.c_void_p(h)) for h in hs]
+
     # ---- downstream: link graph and contour fragments
     def link_contours(self, edges, chains, contour_params: ContourParams | None = None) -> Contours:
         """construct_the_link_graph + extract_regular_contours_from_the_link_graph

@@ -105,6 +105,11 @@ struct cvl_engine {
     std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
     DBuf pairs_in, pb_min, pb_max, pb_valid;
+    // cvl_run_maps: the other group's outputs, a copy stream and its events
+    DBuf chains_alt, info_alt;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t computed[2] = {nullptr, nullptr};
+    cudaEvent_t copied[2] = {nullptr, nullptr};
     // downstream stage (link graph, contour fragments)
     struct ContourBufs {
         DBuf chains_in, cnt, off, cursor, bucket, outdeg, indeg, child, parent, succ, pred, flags, linked, firsts,
@@ -188,7 +193,7 @@ struct cvl_engine {
                        &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
                        &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
                        &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
-                       &pb_max, &pb_valid};
+                       &pb_max, &pb_valid, &chains_alt, &info_alt};
         for (DBuf *b : all) {
             if (b->p) cudaFreeAsync(b->p, stream);
             b->p = nullptr;
@@ -947,6 +952,14 @@ void cvl_engine_destroy(cvl_engine *e) {
     cudaStreamSynchronize(e->stream);
     for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
     if (e->chunk_done) cudaEventDestroy(e->chunk_done);
+    if (e->copy_stream) {
+        cudaStreamSynchronize(e->copy_stream);
+        for (int k = 0; k < 2; ++k) {
+            cudaEventDestroy(e->computed[k]);
+            cudaEventDestroy(e->copied[k]);
+        }
+        cudaStreamDestroy(e->copy_stream);
+    }
     cudaStreamDestroy(e->stream);
     if (e->pool) cudaMemPoolDestroy(e->pool);
     delete e;
@@ -1984,3 +1997,115 @@ int cvl_contours_get(const cvl_contours *c, cvl_contours_view *view) {
 void cvl_contours_free(cvl_contours *c) { delete c; }
 
 }  // extern "C"
+
+
+// =============================================================================
+// Many maps, host to host, with the result copies behind the compute
+// =============================================================================
+extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps,
+                            int32_t edge_data_sz, const cvl_params *p, int64_t group_edges, cvl_result **out) {
+    if (!e || !edges || !counts || !out || num_maps <= 0 || edge_data_sz < 4)
+        return fail(CVL_EINVAL, "invalid arguments");
+    for (int32_t m = 0; m < num_maps; ++m) out[m] = nullptr;
+    std::vector<long long> off(num_maps + 1, 0);
+    for (int32_t m = 0; m < num_maps; ++m) {
+        if (counts[m] <= 0) return fail(CVL_EINVAL, "map " + std::to_string(m) + ": num_edges must be > 0");
+        off[m + 1] = off[m] + counts[m];
+    }
+    if (off[num_maps] > 0x7fffffffLL) return fail(CVL_EOVERFLOW, "more than 2^31 - 1 edges in one call");
+    CVL_CUDA(cudaSetDevice(e->device));
+    if (!e->copy_stream) {
+        CVL_CUDA(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CVL_CUDA(cudaEventCreateWithFlags(&e->computed[k], cudaEventDisableTiming));
+            CVL_CUDA(cudaEventCreateWithFlags(&e->copied[k], cudaEventDisableTiming));
+        }
+    }
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
+    const int W = md.gms + 1;
+    const long long total = off[num_maps];
+    if (group_edges <= 0) group_edges = std::min<long long>(std::max<long long>(total / 6, 1LL << 20), 8LL << 20);
+
+    // groups of whole maps, about group_edges edges each
+    std::vector<int32_t> gstart = {0};
+    for (int32_t m = 0; m < num_maps; ++m)
+        if (m + 1 < num_maps && off[m + 1] - off[gstart.back()] >= group_edges) gstart.push_back(m + 1);
+    gstart.push_back(num_maps);
+    const int G = (int)gstart.size() - 1;
+
+    std::vector<cvl_result *> res(num_maps, nullptr);
+    auto cleanup = [&](int rc) {
+        cudaStreamSynchronize(e->copy_stream);
+        for (cvl_result *r : res) delete r;
+        return rc;
+    };
+    double device_ms = 0.0;
+    bool copy_pending[2] = {false, false};
+    for (int g = 0; g < G; ++g) {
+        const int m0 = gstart[g], m1 = gstart[g + 1], M = m1 - m0;
+        const int buf = g & 1;
+        // this group's outputs go to the buffer pair the group before last used:
+        // its copies must be done before run_pipeline may overwrite or regrow it
+        if (g > 0) {
+            std::swap(e->chains, e->chains_alt);
+            std::swap(e->info, e->info_alt);
+        }
+        if (copy_pending[buf]) CVL_CUDA(cudaStreamWaitEvent(e->stream, e->copied[buf], 0));
+        std::vector<int32_t> mo(M + 1, 0);
+        for (int k = 0; k < M; ++k) mo[k + 1] = mo[k] + counts[m0 + k];
+        const int n = mo[M];
+        int rc = upload(e, edges + (size_t)off[m0] * edge_data_sz, n, edge_data_sz, mo);
+        if (rc != CVL_OK) return cleanup(rc);
+        RunOut ro;
+        rc = run_pipeline(e, (const double *)e->edges.p, n, edge_data_sz, (const int *)e->map_off.p, mo, md, cpl, 0,
+                          false, ro);
+        if (rc != CVL_OK) return cleanup(rc);
+        e->collect_marks();
+        device_ms += e->last_device_ms;
+        if (cudaEventRecord(e->computed[buf], e->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(e->copy_stream, e->computed[buf], 0) != cudaSuccess)
+            return cleanup(fail(CVL_ECUDA, "event record/wait failed"));
+        for (int k = 0; k < M; ++k) {
+            const unsigned long long c0 = ro.cv_off[k], C = ro.cv_off[k + 1] - c0;
+            cvl_result *r = new cvl_result();
+            res[m0 + k] = r;
+            r->pool = e->pinned;
+            r->chains_p = e->pinned->get(sizeof(unsigned) * (C ? C : 1) * W);
+            r->info_p = e->pinned->get(sizeof(double) * (C ? C : 1) * 10);
+            if (!r->chains_p || !r->info_p)
+                return cleanup(fail(CVL_ENOMEM, "page-locked result buffers could not be allocated"));
+            if (C) {
+                cudaError_t ce = copy_pieces(r->chains_p, (const unsigned *)e->chains.p + c0 * W,
+                                             sizeof(unsigned) * C * W, cudaMemcpyDeviceToHost, e->copy_stream);
+                if (ce == cudaSuccess)
+                    ce = copy_pieces(r->info_p, (const double *)e->info.p + c0 * 10, sizeof(double) * C * 10,
+                                     cudaMemcpyDeviceToHost, e->copy_stream);
+                if (ce != cudaSuccess) return cleanup(fail(CVL_ECUDA, std::string("result copy: ") + cudaGetErrorString(ce)));
+            }
+            const MapStats &st = ro.stats[k];
+            cvl_result_view &v = r->v;
+            v.num_curvelets = (uint32_t)C;
+            v.chain_width = (uint32_t)W;
+            v.chains = (const uint32_t *)r->chains_p;
+            v.info = (const double *)r->info_p;
+            v.valid_pairs = st.valid_pairs;
+            v.total_neighbor_pairs = (int64_t)st.pairs;
+            v.max_num_of_neighbors = st.max_deg;
+            v.truncated_anchors = st.truncated;
+            v.num_edges = (uint32_t)counts[m0 + k];
+            v.flags = v.truncated_anchors ? CVL_FLAG_TRUNCATED : 0u;
+        }
+        if (cudaEventRecord(e->copied[buf], e->copy_stream) != cudaSuccess)
+            return cleanup(fail(CVL_ECUDA, "event record failed"));
+        copy_pending[buf] = true;
+    }
+    CVL_CUDA(cudaStreamSynchronize(e->copy_stream));
+    for (int32_t m = 0; m < num_maps; ++m) {
+        res[m]->v.device_ms = device_ms;
+        out[m] = res[m];
+    }
+    e->last_device_ms = device_ms;
+    return CVL_OK;
+}

@@ -240,6 +240,17 @@ typedef struct cvl_batch_stats {
 int cvl_batch_result_stats(const cvl_batch_result *r, cvl_batch_stats *out);
 void cvl_batch_result_free(cvl_batch_result *r);
 
+/* Many maps from host memory to host results in one call, each map as cvl_run
+ * would return it (out[m], freed with cvl_result_free). edges holds the maps'
+ * rows back to back (counts[m] rows each). The maps go through the path in groups
+ * of whole maps of about group_edges edges (<= 0: a sixth of the total, clamped
+ * to [1 Mi, 8 Mi]); while one group computes on the engine's stream, the previous
+ * group's results are copied to page-locked host memory on a second stream, so
+ * the result copies overlap the compute. Each view's device_ms is the whole
+ * call's device time. On error nothing is returned. */
+int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps, int32_t edge_data_sz,
+                 const cvl_params *p, int64_t group_edges, cvl_result **out);
+
 /* ---- serving: continuous batching with memory-budget admission ----------
  * No reference counterpart (the reference runs one map per process). A server
  * owns `workers` engines on one device, each with its own stream and
