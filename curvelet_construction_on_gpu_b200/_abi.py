@@ -81,6 +81,11 @@ class CvlTuning(C.Structure):
 CVL_TUNING_BUCKETS = 4
 
 
+class CvlDeviceResults(C.Structure):
+    _fields_ = [("num_curvelets", C.c_uint32), ("chain_width", C.c_uint32), ("chains", C.c_void_p),
+                ("info", C.c_void_p), ("done_event", C.c_void_p)]
+
+
 class CvlContourParams(C.Structure):
     _fields_ = [("min_group_size", C.c_uint32), ("gap", C.c_double)]
 
@@ -147,6 +152,8 @@ SIGNATURES = [
     ("cvl_engine_last_kernel_times", C.c_int, [_vp, C.POINTER(C.c_char_p), _dp, C.c_int]),
     ("cvl_engine_last_launch_count", C.c_int, [_vp]),
     ("cvl_measure_fp64_peak", C.c_int, [_vp, _dp]),
+    ("cvl_run_device", C.c_int, [_vp, _vp, C.c_int32, C.c_int32, C.POINTER(CvlParams), _vp, C.POINTER(_vp)]),
+    ("cvl_engine_device_results", C.c_int, [_vp, C.POINTER(CvlDeviceResults)]),
     ("cvl_run_maps", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(CvlParams),
                                C.c_int64, C.POINTER(_vp)]),
     ("cvl_contour_params_default", None, [C.POINTER(CvlContourParams)]),

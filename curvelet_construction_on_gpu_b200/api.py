@@ -256,6 +256,28 @@ class Engine:
         check(self._lib.cvl_result_get(r, C.byref(v)), "cvl_result_get")
         return _view_to_result(v, owner)
 
+    def run_device(self, d_edges: int, num_edges: int, edge_data_sz: int = 4, params: CurveletParams | None = None,
+                   dt_rad: float = 0.0, ready_event: int | None = None, to_host: bool = True) -> Result | None:
+        """cvl_run_device: edges already in this engine's device memory (d_edges: a
+        device pointer, e.g. a torch CUDA tensor's data_ptr()), read in place after
+        ready_event (a cudaEvent_t handle, e.g. torch.cuda.Event().cuda_event) if
+        given. to_host=False leaves the results on the device (device_results())."""
+        params = params or CurveletParams()
+        p = params.to_c(dt_rad)
+        r = C.c_void_p()
+        check(self._lib.cvl_run_device(self._h, C.c_void_p(d_edges), num_edges, edge_data_sz, C.byref(p),
+                                       C.c_void_p(ready_event) if ready_event else None,
+                                       C.byref(r) if to_host else None), "cvl_run_device")
+        return _result_from_handle(self._lib, r) if to_host else None
+
+    def device_results(self) -> dict:
+        """The device-resident outputs of the last run_device(to_host=False):
+        chains/info device pointers (cvl_result_view layout) and the event to wait on."""
+        v = _abi.CvlDeviceResults()
+        check(self._lib.cvl_engine_device_results(self._h, C.byref(v)), "cvl_engine_device_results")
+        return {"num_curvelets": int(v.num_curvelets), "chain_width": int(v.chain_width),
+                "chains": int(v.chains or 0), "info": int(v.info or 0), "done_event": int(v.done_event or 0)}
+
     def run_maps(self, maps, params: CurveletParams | None = None, dt_rad: float = 0.0,
                  group_edges: int = 0, counts=None) -> list:
         """Many maps, host to host (cvl_run_maps): one Result per map, as run()

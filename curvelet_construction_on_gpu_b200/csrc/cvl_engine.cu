@@ -105,6 +105,11 @@ struct cvl_engine {
     std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
     DBuf pairs_in, pb_min, pb_max, pb_valid;
+    // cvl_run_device: what its last run left on the device
+    unsigned long long dev_curvelets = 0;
+    int dev_width = 0;
+    unsigned long long dev_generation = ~0ull;
+    cudaEvent_t dev_done = nullptr;
     // cvl_run_maps: the other group's outputs, a copy stream and its events
     DBuf chains_alt, info_alt;
     cudaStream_t copy_stream = nullptr;
@@ -952,6 +957,7 @@ void cvl_engine_destroy(cvl_engine *e) {
     cudaStreamSynchronize(e->stream);
     for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
     if (e->chunk_done) cudaEventDestroy(e->chunk_done);
+    if (e->dev_done) cudaEventDestroy(e->dev_done);
     if (e->copy_stream) {
         cudaStreamSynchronize(e->copy_stream);
         for (int k = 0; k < 2; ++k) {
@@ -2107,5 +2113,60 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
         out[m] = res[m];
     }
     e->last_device_ms = device_ms;
+    return CVL_OK;
+}
+
+
+// =============================================================================
+// Edges already in device memory
+// =============================================================================
+extern "C" int cvl_run_device(cvl_engine *e, const double *d_edges, int32_t num_edges, int32_t edge_data_sz,
+                              const cvl_params *p, void *ready_event, cvl_result **out) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    if (out) *out = nullptr;
+    CVL_TRY(check_edges_args(d_edges, num_edges, edge_data_sz));
+    CVL_CUDA(cudaSetDevice(e->device));
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, d_edges) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CVL_EINVAL, "d_edges is not a CUDA pointer");
+    }
+    if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != e->device)
+        return fail(CVL_EINVAL, "d_edges must be device or managed memory on the engine's device");
+    if (ready_event) CVL_CUDA(cudaStreamWaitEvent(e->stream, (cudaEvent_t)ready_event, 0));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
+    std::vector<int32_t> mo = {0, num_edges};
+    CVL_TRY(e->alloc(e->map_off, sizeof(int) * mo.size()));
+    CVL_CUDA(cudaMemcpyAsync(e->map_off.p, mo.data(), sizeof(int) * mo.size(), cudaMemcpyHostToDevice, e->stream));
+    RunOut ro;
+    CVL_TRY(run_pipeline(e, d_edges, num_edges, edge_data_sz, (const int *)e->map_off.p, mo, md, cpl, 0, false, ro));
+    e->collect_marks();
+    if (!e->dev_done) CVL_CUDA(cudaEventCreateWithFlags(&e->dev_done, cudaEventDisableTiming));
+    CVL_CUDA(cudaEventRecord(e->dev_done, e->stream));
+    e->dev_curvelets = ro.total_curvelets;
+    e->dev_width = md.gms + 1;
+    e->dev_generation = e->generation;
+    if (!out) return CVL_OK;
+    cvl_result *r = new cvl_result();
+    const int rc = fill_view_from_run(e, ro, num_edges, md.gms + 1, r);
+    if (rc != CVL_OK) {
+        delete r;
+        return rc;
+    }
+    *out = r;
+    return CVL_OK;
+}
+
+extern "C" int cvl_engine_device_results(cvl_engine *e, cvl_device_results *out) {
+    if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
+    if (e->dev_generation != e->generation)
+        return fail(CVL_EINVAL, "no device-resident results: the engine's last run was not cvl_run_device");
+    out->num_curvelets = (uint32_t)e->dev_curvelets;
+    out->chain_width = (uint32_t)e->dev_width;
+    out->chains = (const uint32_t *)e->chains.p;
+    out->info = (const double *)e->info.p;
+    out->done_event = (void *)e->dev_done;
     return CVL_OK;
 }

@@ -123,6 +123,32 @@ int cvl_run(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_
 int cvl_run_f32(cvl_engine *e, const float *edges, int32_t num_edges, int32_t edge_data_sz,
                 const cvl_params *p, cvl_result **out);
 
+/* The plain form on edges already in device memory, e.g. written by an edge
+ * detector on the same GPU, so they never cross to the host. d_edges is a
+ * device (or managed) pointer on the engine's device, AoS rows of edge_data_sz
+ * doubles, read in place. The engine's stream waits for ready_event (a
+ * cudaEvent_t the producer recorded after writing the edges) or, if it is NULL,
+ * for nothing: the caller then has already finished writing them.
+ * out != NULL: results come back as cvl_run's. out == NULL: they stay on the
+ * device, readable through cvl_engine_device_results until the engine's next run.
+ * CVL_EINVAL for a host pointer or one on another device. */
+int cvl_run_device(cvl_engine *e, const double *d_edges, int32_t num_edges, int32_t edge_data_sz,
+                   const cvl_params *p, void *ready_event, cvl_result **out);
+
+/* Device-resident outputs of the engine's last cvl_run_device: chains and info
+ * laid out as in cvl_result_view, in the engine's device memory. They are valid
+ * until the engine runs again or is destroyed. done_event (may be NULL) receives
+ * a cudaEvent_t to wait on before reading them from another stream; the engine
+ * owns it. */
+typedef struct cvl_device_results {
+    uint32_t num_curvelets;
+    uint32_t chain_width;
+    const uint32_t *chains; /* device pointer */
+    const double *info;     /* device pointer */
+    void *done_event;       /* cudaEvent_t recorded after the outputs were written */
+} cvl_device_results;
+int cvl_engine_device_results(cvl_engine *e, cvl_device_results *out);
+
 /* Views a result. chains/info point into page-locked host memory owned by the
  * result; they stay valid until cvl_result_free, which may also be called after
  * the engine was destroyed. */
