@@ -374,36 +374,42 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
         const unsigned long long off = a.pair_off[i];
         const int deg = (int)(a.pair_off[i + 1] - off);
 
+        // one pass over the anchor's pairs: the map counts, and the seeds of both
+        // direction runs (valid pairs of run f, in neighbour order). Run 0's seed s
+        // is at slot s, run 1's at slot max_cand - 1 - s: together at most deg slots.
         unsigned valid_cnt = 0, close_cnt = 0;
-        for (int k = lane; k < deg; k += 32) {
-            const unsigned fl = a.pflag[off + k];
+        int ns_run0 = 0, ns_run1 = 0;
+        for (int k0 = 0; k0 < deg; k0 += 32) {
+            const int k = k0 + lane;
+            unsigned fl = 0, cl = 3u;
+            if (k < deg) {
+                fl = a.pflag[off + k];
+                cl = a.pcls[off + k] & 3u;
+            }
             valid_cnt += fl & 1u;
             close_cnt += (fl >> 1) & 1u;
+            const bool t0 = (fl & 1u) && cl == 0u;
+            const bool t1 = (fl & 1u) && cl == 1u;
+            const unsigned b0 = __ballot_sync(FULL, t0);
+            const unsigned b1 = __ballot_sync(FULL, t1);
+            if (t0 || t1) {
+                const int slot = t0 ? ns_run0 + __popc(b0 & lt_mask) : md.max_cand - 1 - (ns_run1 + __popc(b1 & lt_mask));
+                seed_q[slot] = (unsigned)(off + k - a.p_begin) | ((fl & 2u) ? CLOSE_BIT : 0u);
+                seed_orig[slot] = a.B.orig[a.csr_ids[off + k]];
+            }
+            ns_run0 += __popc(b0);
+            ns_run1 += __popc(b1);
         }
         valid_cnt = __reduce_add_sync(FULL, valid_cnt);
         close_cnt = __reduce_add_sync(FULL, close_cnt);
+        __syncwarp();
 
         unsigned n_out = 0;
         for (int f = 0; f < 2; ++f) {
-            // the run's seeds: valid pairs of direction run f, in neighbour order
-            int ns = 0;
-            for (int k0 = 0; k0 < deg; k0 += 32) {
-                const int k = k0 + lane;
-                bool take = false;
-                unsigned fl = 0;
-                if (k < deg) {
-                    fl = a.pflag[off + k];
-                    take = (fl & 1u) && ((a.pcls[off + k] & 3u) == (unsigned)f);
-                }
-                const unsigned bal = __ballot_sync(FULL, take);
-                if (take) {
-                    const int s = ns + __popc(bal & lt_mask);
-                    seed_q[s] = (unsigned)(off + k - a.p_begin) | ((fl & 2u) ? CLOSE_BIT : 0u);
-                    seed_orig[s] = a.B.orig[a.csr_ids[off + k]];
-                }
-                ns += __popc(bal);
-            }
-            __syncwarp();
+            const int ns = f == 0 ? ns_run0 : ns_run1;
+            // seed s of this run -> its slot in seed_q / seed_orig
+            const int s_base = f == 0 ? 0 : md.max_cand - 1;
+            const int s_step = f == 0 ? 1 : -1;
 
             unsigned n_acc = 0;  // curvelets of this run
             unsigned n_fit = 0;  // of those, written to the arena (all, unless it ran out)
@@ -412,7 +418,7 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
             // a run with fewer than two seeds, or group_max_sz <= 2, grows none.
             if (!a.count_only && ns > 1 && md.gms > 2) {
                 auto load_bundle = [&](int s, T *mn, T *mx) {
-                    const unsigned sq = seed_q[s];
+                    const unsigned sq = seed_q[s_base + s_step * s];
                     if (sq & CLOSE_BIT) {
 #pragma unroll
                         for (int u = 0; u < CPL; ++u) {
@@ -583,7 +589,7 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
                             const unsigned short *my = chains + (size_t)s * md.gms;
                             unsigned *ids = a.rec.ids + slot * (unsigned long long)md.gms;
                             ids[0] = (unsigned)orig;
-                            for (unsigned z = 1; z < ln; ++z) ids[z] = (unsigned)seed_orig[my[z]];
+                            for (unsigned z = 1; z < ln; ++z) ids[z] = (unsigned)seed_orig[s_base + s_step * (int)my[z]];
                             a.rec.k[slot * 2 + 0] = rs[0];
                             a.rec.k[slot * 2 + 1] = rs[1];
                             a.rec.meta[slot] = meta;
