@@ -248,10 +248,28 @@ def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
         used += 1
         if secs > budget_s:
             break
-    return {"value": edges / secs, "unit": METRIC, "cores": threads, "kind": kind,
-            "sample": f"{used} of {len(maps)} map(s) (whole maps of at most 600k edges, in workload order), "
-                      f"{edges} edges, timed as the reference's own CSR + form_pairwise_bundles + "
-                      f"build_curvelets_greedy phases (file I/O excluded)"}
+    out = {"value": edges / secs, "unit": METRIC, "cores": threads, "kind": kind, "cpu_model": _cpu_model(),
+           "sample": f"{used} of {len(maps)} map(s) (whole maps of at most 600k edges, in workload order), "
+                     f"{edges} edges, timed as the reference's own CSR + form_pairwise_bundles + "
+                     f"build_curvelets_greedy phases (file I/O excluded)"}
+    # the same on one thread (--nthreads 1), on the first map of the sample
+    if kind == "reference" and cand:
+        m = min(cand, key=lambda x: abs(x.shape[0] - 60_000))
+        r = O.ref_run(m, nthreads=1, want_outputs=False)
+        dt = (r.ms["csr"] + r.ms["pairwise"] + r.ms["greedy"]) / 1e3
+        out["single_thread"] = {"value": m.shape[0] / dt, "unit": METRIC, "cores": 1,
+                                "sample": f"one map of {m.shape[0]} edges"}
+    return out
+
+
+def _cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
 
 
 def run_reference(args, maps, cfg, world, rank):
@@ -621,6 +639,7 @@ def run_contours(args, maps, cfg, world, rank, local, pg):
             rc = O.ref_link_contours(e, r.chains, fw, cp.min_group_size, cp.gap)
             line["cpu_baseline"] = {
                 "value": n_edges / (ref_s + rc.seconds), "unit": METRIC, "cores": threads, "kind": "reference",
+                "cpu_model": _cpu_model(),
                 "sample": f"the whole map ({n_edges} edges): cpu_curvelet CSR + pairwise + greedy on {threads} "
                           f"threads ({ref_s * 1e3:.1f} ms) + original_code construct_the_link_graph + "
                           f"extract_regular_contours_from_the_link_graph, single-threaded as written "
