@@ -685,7 +685,11 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     (void)gbps;
 
     for (int attempt = 0;; ++attempt) {
-        unsigned long long cap = std::max<unsigned long long>(e->arena_hint, 4ull * (unsigned long long)n + 4096ull);
+        // the growth warps reserve the arena in chunks of at most GROWTH_ARENA_CHUNK
+        // records, no more than their anchors (anchors_per_warp): the chunk tails they
+        // leave unused are at most one record per anchor plus one chunk per launch
+        unsigned long long cap = std::max<unsigned long long>(e->arena_hint, 4ull * (unsigned long long)n + 4096ull) +
+                                 (unsigned long long)n + (unsigned long long)GROWTH_ARENA_CHUNK * (nchunks + 1);
         if (mode == 0) {
             CVL_TRY(e->alloc(e->rec_ids, sizeof(unsigned) * cap * md.gms));
             CVL_TRY(e->alloc(e->rec_k, sizeof(double) * cap * 2));

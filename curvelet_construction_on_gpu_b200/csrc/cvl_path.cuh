@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB) k_bundles(BundleArgsT<T>
 // seeds are the run's valid pairs in neighbour order; groups of K seeds walk the
 // seed list in lock step (:479-545), each intersection (:832-854) one
 // __reduce_or_sync vote; first-wins dedup (:876-916); each run's accepted chains
-// go as compact records to one exactly sized reservation in the record arena.
+// go as compact records to the warp's current chunk of the record arena.
 // ---------------------------------------------------------------------------
 template <typename T>
 struct GrowthArgsT {
@@ -337,6 +337,8 @@ __host__ __device__ inline size_t growth_smem_per_warp(int max_cand, int gms) {
 // warps per SM. A block is one warp: a block's SM slot frees as soon as its own
 // anchors are done (measured 2% faster than 4-warp blocks).
 constexpr int GROWTH_THREADS = 32;
+// records a growth warp reserves in the arena at a time (at most its anchors per warp)
+constexpr int GROWTH_ARENA_CHUNK = 8;
 template <typename T, int CPL, int K, int MINB>
 __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT<T> a) {
     extern __shared__ __align__(16) unsigned char gr_smem[];
@@ -365,6 +367,11 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
 
     int acc_map = -1;
     unsigned acc_valid = 0u, acc_close = 0u;
+    // the warp's arena chunk: [ch_cur, ch_end)
+    unsigned long long ch_cur = 0, ch_end = 0;
+    const unsigned chunk_recs = (unsigned)(a.anchors_per_warp < GROWTH_ARENA_CHUNK
+                                               ? (a.anchors_per_warp > 0 ? a.anchors_per_warp : 1)
+                                               : GROWTH_ARENA_CHUNK);
     // The grid has one warp per anchors_per_warp anchors, and a warp strides over
     // the chunk: its anchors lie far apart, so the work of dense regions is shared
     // out across warps (measured 8% faster than contiguous runs per warp).
@@ -569,10 +576,21 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
                     }
                     __syncwarp();
                 }
-                // flush: one exact arena reservation per (anchor, run), records in seed order
+                // flush: the run's records go, in seed order, to the warp's current arena
+                // chunk; a new chunk (one atomic) when it has no room
                 unsigned long long rbase = 0;
-                if (lane == 0 && n_acc) rbase = atomicAdd(a.arena_ctr, (unsigned long long)n_acc);
-                rbase = __shfl_sync(FULL, rbase, 0);
+                if (n_acc) {
+                    if (ch_cur + n_acc > ch_end) {
+                        const unsigned long long want = n_acc > chunk_recs ? n_acc : chunk_recs;
+                        unsigned long long b = 0;
+                        if (lane == 0) b = atomicAdd(a.arena_ctr, want);
+                        b = __shfl_sync(FULL, b, 0);
+                        ch_cur = b;
+                        ch_end = b + want;
+                    }
+                    rbase = ch_cur;
+                    ch_cur += n_acc;
+                }
                 const bool fits = rbase + n_acc <= a.arena_cap;
                 if (n_acc && !fits && lane == 0) atomicOr(a.err, ERR_ARENA);
                 if (n_acc && fits) {
