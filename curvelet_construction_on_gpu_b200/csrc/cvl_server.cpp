@@ -80,8 +80,8 @@ struct cvl_server {
     std::vector<int64_t> lat_edges;
     std::vector<uint64_t> lat_ids;
 
-    // the lane a worker serves first (the last worker prefers large maps when there are several)
-    int preferred_lane(int w) const { return (cfg.workers >= 2 && w == cfg.workers - 1) ? 1 : 0; }
+    // the lane a worker serves first (the last large_workers workers prefer large maps when there are several)
+    int preferred_lane(int w) const { return (cfg.workers >= 2 && w >= cfg.workers - cfg.large_workers) ? 1 : 0; }
 
     // lane whose head request fits the remaining budget, preferred lane first; -1 if none
     int lane_to_take(int w) const {
@@ -241,13 +241,14 @@ extern "C" {
 void cvl_server_cfg_default(cvl_server_cfg *c) {
     if (!c) return;
     c->device = 0;
-    c->workers = 3;
+    c->workers = 4;
     c->mem_budget_bytes = (size_t)40 << 30;
     c->admit_bytes_per_edge = 2048;
     c->max_batch_edges = 2 << 20;
     c->large_map_edges = 1000000;
     c->host_reserve_bytes = (size_t)2 << 30;
     c->small_takes_large = 0;
+    c->large_workers = 0;
 }
 
 int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out) {
@@ -257,6 +258,9 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
     cvl_server_cfg_default(&c);
     if (cfg) c = *cfg;
     if (c.workers < 1 || c.workers > 16) return cvl_fail(CVL_EINVAL, "workers must be in [1, 16]");
+    if (c.large_workers == 0) c.large_workers = std::max(1, c.workers / 2);
+    if (c.workers >= 2 && c.large_workers >= c.workers) c.large_workers = c.workers - 1;
+    if (c.large_workers < 1) return cvl_fail(CVL_EINVAL, "large_workers must be 0 (automatic) or in [1, workers - 1]");
     if (c.mem_budget_bytes == 0 || c.admit_bytes_per_edge == 0 || c.max_batch_edges <= 0 || c.large_map_edges <= 0)
         return cvl_fail(CVL_EINVAL, "budget, admission charge and batch sizes must be > 0");
     cvl_server *s = new cvl_server();
@@ -267,7 +271,7 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
         cvl_engine_cfg_default(&ec);
         ec.device = c.device;
         // small-lane workers first on the device (the lowest number is the highest priority)
-        const bool small_lane = !(c.workers >= 2 && w == c.workers - 1);
+        const bool small_lane = !(c.workers >= 2 && w >= c.workers - c.large_workers);
         ec.stream_priority = small_lane ? -1000 : 0;
         cvl_engine *e = nullptr;
         const int rc = cvl_engine_create(&ec, &e);
