@@ -87,7 +87,8 @@ class CvlDeviceResults(C.Structure):
 
 
 class CvlContourParams(C.Structure):
-    _fields_ = [("min_group_size", C.c_uint32), ("gap", C.c_double)]
+    _fields_ = [("min_group_size", C.c_uint32), ("gap", C.c_double), ("fit_polyarcs", C.c_int), ("dx", C.c_double),
+                ("dt_rad", C.c_double), ("max_k", C.c_double), ("rad", C.c_double), ("token_len", C.c_double)]
 
 
 class CvlContoursView(C.Structure):
@@ -95,7 +96,9 @@ class CvlContoursView(C.Structure):
                 ("link_child", C.POINTER(C.c_int32)), ("link_votes", C.POINTER(C.c_int32)),
                 ("num_fragments", C.c_int64), ("fragment_offsets", C.POINTER(C.c_int64)),
                 ("fragment_ids", C.POINTER(C.c_int32)), ("max_fragment_length", C.c_int32),
-                ("num_edges", C.c_int32), ("device_ms", C.c_float)]
+                ("num_edges", C.c_int32), ("device_ms", C.c_float), ("num_polyarcs", C.c_int64),
+                ("polyarc_offsets", C.POINTER(C.c_int64)), ("polyarc_ids", C.POINTER(C.c_int32)),
+                ("polyarc_info", C.POINTER(C.c_double))]
 
 # (name, restype, argtypes) of every entry point declared in include/cvl.h
 _vp = C.c_void_p

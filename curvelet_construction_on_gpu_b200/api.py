@@ -114,9 +114,20 @@ class ContourParams:
     edges of a fragment (1.5 in original_code/main.cpp:146)."""
     min_group_size: int = 4
     gap: float = 1.5
+    # C^1 polyarcs along the fragments (fit_polyarcs_to_all_edgel_chains,
+    # original_code/form_curvelet_process.cpp:661-796), with form_curvelet_mex's
+    # dx, dt, max_k, rad and token_len (original_code/main.cpp:145-151)
+    fit_polyarcs: bool = False
+    dx: float = 0.4
+    dt_rad: float = (15.0 / 180.0) * M_PI
+    max_k: float = 0.3
+    rad: float = 3.5
+    token_len: float = 1.0
 
     def to_c(self) -> _abi.CvlContourParams:
-        return _abi.CvlContourParams(int(self.min_group_size), float(self.gap))
+        return _abi.CvlContourParams(int(self.min_group_size), float(self.gap), 1 if self.fit_polyarcs else 0,
+                                     float(self.dx), float(self.dt_rad), float(self.max_k), float(self.rad),
+                                     float(self.token_len))
 
 
 @dataclass
@@ -130,6 +141,18 @@ class Contours:
     frag_ids: np.ndarray
     num_edges: int
     device_ms: float = 0.0
+    # polyarcs (ContourParams.fit_polyarcs): CSR chains and info [P, 12]
+    # (curvelet::set_output's columns; the centre columns 10-11 are 0 for a line)
+    poly_offsets: np.ndarray | None = None
+    poly_ids: np.ndarray | None = None
+    poly_info: np.ndarray | None = None
+
+    @property
+    def num_polyarcs(self) -> int:
+        return 0 if self.poly_offsets is None else int(self.poly_offsets.shape[0] - 1)
+
+    def polyarcs(self) -> list:
+        return [self.poly_ids[self.poly_offsets[i]:self.poly_offsets[i + 1]] for i in range(self.num_polyarcs)]
 
     @property
     def num_frags(self) -> int:
@@ -164,7 +187,16 @@ def _contours_from_handle(lib, h) -> Contours:
         offs = np.ctypeslib.as_array(v.fragment_offsets, shape=(F + 1,)).copy()
         nid = int(offs[-1])
         ids = np.ctypeslib.as_array(v.fragment_ids, shape=(nid,)).copy() if nid else np.zeros(0, np.int32)
-        return Contours(links, offs, ids, int(v.num_edges), float(v.device_ms))
+        out = Contours(links, offs, ids, int(v.num_edges), float(v.device_ms))
+        if v.polyarc_offsets:
+            P = int(v.num_polyarcs)
+            out.poly_offsets = np.ctypeslib.as_array(v.polyarc_offsets, shape=(P + 1,)).copy()
+            npid = int(out.poly_offsets[-1])
+            out.poly_ids = (np.ctypeslib.as_array(v.polyarc_ids, shape=(npid,)).copy() if npid
+                            else np.zeros(0, np.int32))
+            out.poly_info = (np.ctypeslib.as_array(v.polyarc_info, shape=(P * 12,)).reshape(P, 12).copy() if P
+                             else np.zeros((0, 12)))
+        return out
     finally:
         lib.cvl_contours_free(h)
 
@@ -320,7 +352,8 @@ class Engine:
         """Edges -> curvelets -> link graph -> fragments in one device pass.
         Returns (Result or None, Contours)."""
         params = params or CurveletParams()
-        cp = (contour_params or ContourParams(gap=params.gap)).to_c()
+        cp = (contour_params or ContourParams(gap=params.gap, dx=params.dx, max_k=params.max_k, rad=params.nrad,
+                                              dt_rad=dt_rad if dt_rad > 0 else (params.dt_deg / 180.0) * M_PI)).to_c()
         e = _edges(edges)
         p = params.to_c(dt_rad)
         r = C.c_void_p()

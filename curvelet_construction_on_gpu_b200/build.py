@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
               "-Xcompiler", "-fPIC,-O2", "-shared"]
 LIB_SOURCES = ["cvl_engine.cu", "cvl_server.cpp", "cvl_io.cpp"]
-LIB_DEPS = ["cvl_engine.cu", "cvl_server.cpp", "cvl_io.cpp", "cvl_internal.h", "cvl_pinned.h", "cvl_kernels.cuh", "cvl_path.cuh", "cvl_scan.cuh", "cvl_contours.cuh"]
+LIB_DEPS = ["cvl_engine.cu", "cvl_server.cpp", "cvl_io.cpp", "cvl_internal.h", "cvl_pinned.h", "cvl_kernels.cuh", "cvl_path.cuh", "cvl_scan.cuh", "cvl_contours.cuh", "cvl_polyarcs.cuh"]
 
 
 def _nvcc() -> str:

@@ -22,6 +22,7 @@
 #include "cvl_pinned.h"
 #include "cvl_contours.cuh"
 #include "cvl_path.cuh"
+#include "cvl_polyarcs.cuh"
 #include "cvl_scan.cuh"
 
 using namespace cvl;
@@ -118,11 +119,13 @@ struct cvl_engine {
     // downstream stage (link graph, contour fragments)
     struct ContourBufs {
         DBuf chains_in, cnt, off, cursor, bucket, outdeg, indeg, child, parent, succ, pred, flags, linked, firsts,
-            region, ctr, fsrc, fnf, fnb, isfrag, flen, fidx, idoff, loff, lpe, lce, lvotes, fragoff, fragids, err;
+            region, ctr, fsrc, fnf, fnb, isfrag, flen, fidx, idoff, loff, lpe, lce, lvotes, fragoff, fragids, err,
+            pstart, psize, pinfo, pcount, poff, pstart2, psize2, pinfo2;
         DBuf *all(int i) {
             DBuf *b[] = {&chains_in, &cnt, &off, &cursor, &bucket, &outdeg, &indeg, &child, &parent, &succ,
                          &pred, &flags, &linked, &firsts, &region, &ctr, &fsrc, &fnf, &fnb, &isfrag,
-                         &flen, &fidx, &idoff, &loff, &lpe, &lce, &lvotes, &fragoff, &fragids, &err};
+                         &flen, &fidx, &idoff, &loff, &lpe, &lce, &lvotes, &fragoff, &fragids, &err,
+                         &pstart, &psize, &pinfo, &pcount, &poff, &pstart2, &psize2, &pinfo2};
             return i < (int)(sizeof(b) / sizeof(b[0])) ? b[i] : nullptr;
         }
     } cw;
@@ -1725,6 +1728,9 @@ struct cvl_contours {
     void *links_p = nullptr;  // pe, ce, votes: 3 x num_links int32
     void *offs_p = nullptr;
     void *ids_p = nullptr;
+    std::vector<int64_t> poly_offsets;
+    std::vector<int32_t> poly_ids;
+    std::vector<double> poly_info;
     cvl_contours_view v{};
     ~cvl_contours() {
         if (pool) {
@@ -1893,6 +1899,88 @@ int contours_on_device(cvl_engine *e, const double *d_edges, int n, int sz, cons
         mx = std::max<int32_t>(mx, (int32_t)(v.fragment_offsets[f + 1] - v.fragment_offsets[f]));
     v.max_fragment_length = mx;
     v.num_edges = n;
+    v.num_polyarcs = 0;
+    v.polyarc_offsets = nullptr;
+    v.polyarc_ids = nullptr;
+    v.polyarc_info = nullptr;
+    if (cp.fit_polyarcs && h_frags > 0) {
+        // the polyarc model: form_curvelet_process's dx, dt, max_k on CC_curve_model_3d's
+        // fixed grid steps (0.1 px, 0.08 rad)
+        cvl_params mp;
+        cvl_params_default(&mp);
+        mp.dx = cp.dx;
+        mp.dt_rad = cp.dt_rad;
+        mp.max_k = cp.max_k;
+        mp.sx = 0.1;
+        mp.st = 0.08;
+        Model pm;
+        int pcpl = 2;
+        CVL_TRY(make_model(e, &mp, mp.nrad, 3u, mp.max_candidates, pm, pcpl));
+        const unsigned long long slots = h_ids - h_frags;  // at most N - 1 per fragment of N edges
+        CVL_TRY(e->alloc(w.pstart, sizeof(long long) * std::max<unsigned long long>(slots, 1)));
+        CVL_TRY(e->alloc(w.psize, sizeof(int) * std::max<unsigned long long>(slots, 1)));
+        CVL_TRY(e->alloc(w.pinfo, sizeof(double) * 12 * std::max<unsigned long long>(slots, 1)));
+        CVL_TRY(e->alloc(w.pcount, sizeof(unsigned) * h_frags));
+        CVL_TRY(e->alloc(w.poff, sizeof(unsigned long long) * (h_frags + 1)));
+        PolyArgs pa;
+        pa.md = pm;
+        pa.edges = d_edges;
+        pa.sz = sz;
+        pa.nfrags = (int)h_frags;
+        pa.frag_off = (const long long *)w.fragoff.p;
+        pa.frag_ids = (const int *)w.fragids.p;
+        pa.rad = cp.rad;
+        pa.token_len = cp.token_len;
+        pa.poly_start = (long long *)w.pstart.p;
+        pa.poly_size = (int *)w.psize.p;
+        pa.poly_info = (double *)w.pinfo.p;
+        pa.poly_count = (unsigned *)w.pcount.p;
+        const int pb = (int)std::max(1u, (h_frags + 3) / 4);
+        switch (pcpl) {
+            case 1: k_polyarcs<1><<<pb, 128, 0, s>>>(pa); break;
+            case 3: k_polyarcs<3><<<pb, 128, 0, s>>>(pa); break;
+            case 4: k_polyarcs<4><<<pb, 128, 0, s>>>(pa); break;
+            default: k_polyarcs<2><<<pb, 128, 0, s>>>(pa); break;
+        }
+        CVL_TRY(check_launch("k_polyarcs"));
+        CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)w.pcount.p, h_frags,
+                                                     (unsigned long long *)w.poff.p)));
+        unsigned long long h_poly = 0;
+        CVL_CUDA(cudaMemcpyAsync(&h_poly, (unsigned long long *)w.poff.p + h_frags, sizeof(h_poly),
+                                 cudaMemcpyDeviceToHost, s));
+        CVL_CUDA(cudaStreamSynchronize(s));
+        CVL_TRY(e->alloc(w.pstart2, sizeof(long long) * std::max<unsigned long long>(h_poly, 1)));
+        CVL_TRY(e->alloc(w.psize2, sizeof(int) * std::max<unsigned long long>(h_poly, 1)));
+        CVL_TRY(e->alloc(w.pinfo2, sizeof(double) * 12 * std::max<unsigned long long>(h_poly, 1)));
+        k_polyarcs_pack<<<(int)((h_frags + 255) / 256), 256, 0, s>>>(
+            (int)h_frags, (const long long *)w.fragoff.p, (const unsigned *)w.pcount.p,
+            (const unsigned long long *)w.poff.p, (const long long *)w.pstart.p, (const int *)w.psize.p,
+            (const double *)w.pinfo.p, (long long *)w.pstart2.p, (int *)w.psize2.p, (double *)w.pinfo2.p);
+        CVL_TRY(check_launch("k_polyarcs_pack"));
+        e->mark("polyarcs");
+        std::vector<long long> st(h_poly);
+        std::vector<int> sizes(h_poly);
+        c->poly_info.resize(12 * h_poly);
+        if (h_poly) {
+            CVL_CUDA(cudaMemcpyAsync(st.data(), w.pstart2.p, sizeof(long long) * h_poly, cudaMemcpyDeviceToHost, s));
+            CVL_CUDA(cudaMemcpyAsync(sizes.data(), w.psize2.p, sizeof(int) * h_poly, cudaMemcpyDeviceToHost, s));
+            CVL_CUDA(cudaMemcpyAsync(c->poly_info.data(), w.pinfo2.p, sizeof(double) * 12 * h_poly,
+                                     cudaMemcpyDeviceToHost, s));
+        }
+        CVL_CUDA(cudaStreamSynchronize(s));
+        c->poly_offsets.assign(h_poly + 1, 0);
+        for (unsigned long long q = 0; q < h_poly; ++q) c->poly_offsets[q + 1] = c->poly_offsets[q] + sizes[q];
+        c->poly_ids.resize((size_t)c->poly_offsets[h_poly] + 1);
+        for (unsigned long long q = 0; q < h_poly; ++q)
+            std::memcpy(c->poly_ids.data() + c->poly_offsets[q], v.fragment_ids + st[q], sizeof(int32_t) * sizes[q]);
+        v.num_polyarcs = (int64_t)h_poly;
+        v.polyarc_offsets = c->poly_offsets.data();
+        v.polyarc_ids = c->poly_ids.data();
+        v.polyarc_info = c->poly_info.data();
+    } else if (cp.fit_polyarcs) {
+        c->poly_offsets.assign(1, 0);
+        v.polyarc_offsets = c->poly_offsets.data();
+    }
     return CVL_OK;
 }
 
@@ -1905,6 +1993,9 @@ int contour_params_of(const cvl_contour_params *cp, double gap, cvl_contour_para
     else
         out.gap = gap;
     if (!(out.gap >= 0.0) || !std::isfinite(out.gap)) return fail(CVL_EINVAL, "gap must be finite and >= 0");
+    if (out.fit_polyarcs && (!(out.dx > 0) || !(out.dt_rad > 0) || !std::isfinite(out.max_k) || !(out.rad > 0) ||
+                             !(out.token_len > 0) || !std::isfinite(out.dx) || !std::isfinite(out.dt_rad)))
+        return fail(CVL_EINVAL, "polyarc parameters: dx, dt_rad, rad and token_len must be finite and > 0");
     return CVL_OK;
 }
 
@@ -1916,6 +2007,12 @@ void cvl_contour_params_default(cvl_contour_params *p) {
     if (!p) return;
     p->min_group_size = 4;
     p->gap = 1.5;
+    p->fit_polyarcs = 0;
+    p->dx = 0.4;
+    p->dt_rad = (15.0 / 180.0) * CVL_PI;
+    p->max_k = 0.3;
+    p->rad = 3.5;
+    p->token_len = 1.0;
 }
 
 int cvl_link_contours(cvl_engine *e, const double *edges, int32_t num_edges, int32_t edge_data_sz,

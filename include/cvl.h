@@ -437,6 +437,15 @@ int cvl_measure_fp64_peak(cvl_engine *e, double *tflops);
 typedef struct cvl_contour_params {
     uint32_t min_group_size; /* construct_the_link_graph(4, ...), form_curvelet_process.cpp:79 */
     double gap;              /* 1.5, original_code/main.cpp:146 */
+    /* C^1 polyarcs along the fragments: fit_polyarcs_to_all_edgel_chains
+     * (form_curvelet_process.cpp:661-796), output type 2 of original_code/main.cpp.
+     * The bundle grid steps are CC_curve_model_3d's fixed 0.1 px and 0.08 rad. */
+    int fit_polyarcs;        /* 1: fit them (0) */
+    double dx;               /* position uncertainty, px (0.4, main.cpp:148) */
+    double dt_rad;           /* orientation uncertainty, rad ((15/180) pi, main.cpp:149) */
+    double max_k;            /* curvature bound (0.3, main.cpp:151) */
+    double rad;              /* compute_properties' R: the grouping radius (3.5, main.cpp:145) */
+    double token_len;        /* compute_properties' token length (1, main.cpp:150) */
 } cvl_contour_params;
 
 void cvl_contour_params_default(cvl_contour_params *p);
@@ -457,6 +466,16 @@ typedef struct cvl_contours_view {
     int32_t max_fragment_length; /* curve_fragment_graph::edgel_chain_max_length */
     int32_t num_edges;
     float device_ms; /* the stage's device time (cvl_run_contours: the whole path) */
+    /* polyarcs (fit_polyarcs = 1; else 0 and NULL), polyarcmap order: fragments in
+     * order, each one's polyarcs from its start. Each polyarc's chain is a run of
+     * its fragment's ids. info columns per curvelet::set_output (curvelet.cpp:132-144,
+     * CC_curve_model_3d.cpp:530-545): 0 forward (1), 1-2 the best cell's k_max and
+     * k_min, 3 the start edge's orientation, 4-5 its position, 6 theta, 7 k, 8 length,
+     * 9 quality, 10-11 the arc's centre (0 for a line: the reference leaves them unset). */
+    int64_t num_polyarcs;
+    const int64_t *polyarc_offsets; /* [num_polyarcs + 1] into polyarc_ids */
+    const int32_t *polyarc_ids;     /* 0-based edge ids */
+    const double *polyarc_info;     /* [num_polyarcs][12] */
 } cvl_contours_view;
 
 /* The stage on curvelets the caller holds: chains as cvl_result_view gives them

@@ -802,3 +802,187 @@ bad:
     free(links);
     return -1;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Downstream: C^1 polyarcs along the contour fragments                     */
+/* (original_code/form_curvelet_process.cpp:661-796, CC_curve_model_3d.cpp, */
+/*  curvelet.cpp, polyarcmap.hpp)                                            */
+/* ---------------------------------------------------------------------- */
+
+#define ORC_K_TH 1e-4 /* k_th, original_code/curvelet_utils.hpp:15 */
+
+typedef struct {
+    int num;
+    int64_t *offsets; /* [num + 1] into ids */
+    int *ids;         /* 0-based edge ids */
+    double *info;     /* [num][12]: curvelet::set_output's columns, unset ones 0 */
+} orc_polyarcs;
+
+void orc_polyarcs_free(orc_polyarcs *p)
+{
+    free(p->offsets);
+    free(p->ids);
+    free(p->info);
+    memset(p, 0, sizeof(*p));
+}
+
+/* form_a_hypothesis(ref, e2, max_k, ref_first, forward = true, centered = false,
+ * leading = true) (form_curvelet_process.cpp:388-444): a model only when e2 lies
+ * ahead of ref (dot > 0), with the CC_curve_model_3d bundle
+ * (CC_curve_model_3d.cpp:181-335, the same transport as compute_curve_bundle of
+ * cpu_curvelet). Returns 1 for a valid bundle, 0 for none or an empty one. */
+static int orc_hypothesis(const orc_model *m, const double *edges, int sz, int a, int b, double *bmin,
+                          double *bmax)
+{
+    const double *A = edges + (size_t)a * sz, *B = edges + (size_t)b * sz;
+    if (!(orc_dot(orc_angle_pt_pt(A[0], A[1], B[0], B[1]), A[2]) > 0)) return 0;
+    for (unsigned c = 0; c < m->P * m->Q; ++c) {
+        bmin[c] = -m->max_k;
+        bmax[c] = m->max_k;
+    }
+    return orc_curve_bundle(m, A[0], A[1], B[0], B[1], A[2], B[2], bmin, bmax);
+}
+
+/* fit_polyarc_to_chain over every fragment, then
+ * compute_best_fit_according_to_curvelets (polyarcmap.hpp:98-111). dx, dt (rad),
+ * max_k, rad and token_len are form_curvelet_process's; the bundle grid steps are
+ * CC_curve_model_3d's fixed _dx_ = 0.1 and _dt_ = 0.08. */
+int orc_polyarcs_fit(const double *edges, int num_edges, int sz, const int64_t *frag_off, const int *frag_ids,
+                     int nfrags, double dx, double dt, double max_k, double rad, double token_len,
+                     orc_polyarcs *out)
+{
+    memset(out, 0, sizeof(*out));
+    if (num_edges <= 0 || sz < 4 || nfrags < 0) return -1;
+    orc_model m;
+    m.nrad = rad;
+    m.dx = dx;
+    m.dt = dt;
+    m.max_k = max_k;
+    m.sx = 0.1;
+    m.st = 0.08;
+    m.P = (unsigned)(2 * floor(dx / 0.1 + 0.5) + 1);  /* CC_curve_model_3d.cpp:196-200 */
+    m.Q = (unsigned)(2 * floor(dt / 0.08 + 0.5) + 1);
+    m.gms = 0;
+    const unsigned cells = m.P * m.Q;
+    double *cmin = (double *)malloc(sizeof(double) * cells * 4);
+    double *cmax = cmin + cells, *rmin = cmax + cells, *rmax = rmin + cells;
+    const int64_t total = nfrags ? frag_off[nfrags] : 0;
+    out->offsets = (int64_t *)malloc(sizeof(int64_t) * ((size_t)total + 1));
+    out->ids = (int *)malloc(sizeof(int) * ((size_t)total * 2 + 1));
+    out->info = (double *)calloc((size_t)total * 12 + 1, sizeof(double));
+    out->offsets[0] = 0;
+    int64_t nid = 0;
+    for (int f = 0; f < nfrags; ++f) {
+        const int *ids = frag_ids + frag_off[f];
+        const int N = (int)(frag_off[f + 1] - frag_off[f]);
+        int i = 0;
+        while (i < N - 1) { /* fit_polyarc_to_chain, form_curvelet_process.cpp:683-769 */
+            const int iA = i, a = ids[i];
+            ++i;
+            if (!orc_hypothesis(&m, edges, sz, a, ids[i], cmin, cmax)) continue;
+            int j = i;
+            while (j < N - 1) {
+                if (!orc_hypothesis(&m, edges, sz, a, ids[j + 1], rmin, rmax)) break;
+                /* CC_curve_model_3d(cm1, cm2): Kmin = std::max, Kmax = std::min (hpp:70-84) */
+                int ok = 0;
+                for (unsigned c = 0; c < cells; ++c) {
+                    rmin[c] = (cmin[c] < rmin[c]) ? rmin[c] : cmin[c];
+                    rmax[c] = (rmax[c] < cmax[c]) ? rmax[c] : cmax[c];
+                    ok = ok || (rmax[c] > rmin[c]);
+                }
+                if (!ok) break;
+                memcpy(cmin, rmin, sizeof(double) * cells);
+                memcpy(cmax, rmax, sizeof(double) * cells);
+                ++j;
+            }
+            /* the polyarc is ids[iA .. j]; curve_fit_is_reasonable -> compute_best_fit
+             * (CC_curve_model_3d.cpp:338-383, :444-451): the open cell nearest the grid
+             * centre, first in row-major order */
+            unsigned best = cells;
+            double mind = 100;
+            for (unsigned ci = 0; ci < m.P; ci++)
+                for (unsigned cj = 0; cj < m.Q; cj++) {
+                    const unsigned c = ci * m.Q + cj;
+                    if (cmax[c] > cmin[c]) {
+                        const double ddx = 0.1 * ((double)ci - ((double)m.P - 1.0) / 2.0);
+                        const double ddt = 0.08 * ((double)cj - ((double)m.Q - 1.0) / 2.0);
+                        const double d = ddx * ddx + ddt * ddt;
+                        if (d < mind) {
+                            mind = d;
+                            best = c;
+                        }
+                    }
+                }
+            if (best == cells) best = 0; /* not reached: the bundle is valid */
+            double k = (cmax[best] + cmin[best]) / 2;
+            const double kmax = cmax[best], kmin = cmin[best];
+            const int size = j - iA + 1;
+            /* curvelet::compute_properties (curvelet.cpp:80-104): the anchor is the
+             * chain's front, so every step counts before it */
+            double L = 0;
+            for (int q = iA; q < j; ++q) L += sqrt(orc_pt_sqd(edges, sz, ids[q], ids[q + 1]));
+            const double quality = 2 / (1.0 * rad / L + 1.0 * L / token_len / size);
+            /* compute_best_fit_according_to_curvelets -> update_best_fit
+             * (CC_curve_model_3d.cpp:400-441) with _pt = the front edge */
+            const double *PT = edges + (size_t)a * sz;
+            const double *P1 = edges + (size_t)ids[iA + size / 2] * sz;
+            const double *P2 = edges + (size_t)ids[j] * sz;
+            double theta, angle = 0.0, cx = 0.0, cy = 0.0;
+            int arc = 0;
+            if (fabs(k) < ORC_K_TH) {
+                k = 0.0;
+                theta = atan2(P2[1] - PT[1], P2[0] - PT[0]);
+            } else {
+                const double d1 = PT[0] * PT[0] + PT[1] * PT[1], d2 = P1[0] * P1[0] + P1[1] * P1[1],
+                             d3 = P2[0] * P2[0] + P2[1] * P2[1];
+                const double a11 = 2.0 * (PT[0] - P1[0]), a12 = 2.0 * (PT[1] - P1[1]), a21 = 2.0 * (P2[0] - P1[0]),
+                             a22 = 2.0 * (P2[1] - P1[1]);
+                const double b1 = d1 - d2, b2 = d3 - d2;
+                const double det = a11 * a22 - a21 * a12;
+                if (fabs(det) < ORC_K_TH) {
+                    k = 0.0;
+                    theta = atan2(P2[1] - PT[1], P2[0] - PT[0]);
+                } else {
+                    cx = (b1 * a22 - b2 * a12) / det;
+                    cy = (b2 * a11 - b1 * a21) / det;
+                    const double v1x = PT[0] - cx, v1y = PT[1] - cy, v2x = P2[0] - cx, v2y = P2[1] - cy;
+                    const double c = v1x * v2y - v1y * v2x, d = v1x * v2x + v1y * v2y;
+                    angle = atan2(fabs(c), d);
+                    theta = atan2(c * v1x, -c * v1y);
+                    k = 1.0 / sqrt(v2x * v2x + v2y * v2y);
+                    arc = 1;
+                }
+            }
+            /* curvelet::update_length (curvelet.cpp:162-169) */
+            if (fabs(angle) > 0 && fabs(k) > ORC_K_TH && arc) L = angle / fabs(k);
+            /* fit_polyarc_to_chain ends with compute_best_fit_according_to_curvelets over
+             * every polyarc so far (form_curvelet_process.cpp:772), so a polyarc of
+             * fragment f is fitted again at the end of each later fragment. A refit
+             * repeats a line and an arc with |k| >= k_th exactly; an arc with |k| < k_th
+             * becomes a line (k = 0, theta along the chord), keeping its centre, angle and
+             * length, and stays one. */
+            if (arc && fabs(k) < ORC_K_TH && f < nfrags - 1) {
+                k = 0.0;
+                theta = atan2(P2[1] - PT[1], P2[0] - PT[0]);
+            }
+            double *row = out->info + (size_t)out->num * 12;
+            row[0] = 1.0; /* forward */
+            row[1] = kmax; /* _ref_pt, overwritten by compute_best_fit (:378-379) */
+            row[2] = kmin;
+            row[3] = PT[2]; /* _ref_theta */
+            row[4] = PT[0];
+            row[5] = PT[1];
+            row[6] = theta;
+            row[7] = k;
+            row[8] = L;
+            row[9] = quality;
+            row[10] = arc ? cx : 0.0;
+            row[11] = arc ? cy : 0.0;
+            for (int q = iA; q <= j; ++q) out->ids[nid++] = ids[q];
+            out->offsets[++out->num] = nid;
+            i = j;
+        }
+    }
+    free(cmin);
+    return 0;
+}

@@ -365,3 +365,93 @@ def ref_link_contours(edges, chains, forward=None, min_group_size=4, gap=1.5) ->
         return _contours_from(o, o.seconds)
     finally:
         _orig.origref_contours_free(C.byref(o))
+
+
+class _OrigPolyarcs(C.Structure):
+    _fields_ = [("num_polyarcs", C.c_int32), ("offsets", C.POINTER(C.c_int64)), ("ids", C.POINTER(C.c_int32)),
+                ("info", C.POINTER(C.c_double)), ("seconds", C.c_double)]
+
+
+@dataclass
+class Polyarcs:
+    """Polyarcs in polyarcmap order: CSR chains (offsets [P+1], 0-based ids) and
+    info [P, 12] (curvelet::set_output's columns; unset columns 0)."""
+    offsets: np.ndarray
+    ids: np.ndarray
+    info: np.ndarray
+    seconds: float = 0.0
+
+    @property
+    def num(self) -> int:
+        return int(self.offsets.shape[0] - 1)
+
+
+def ref_polyarcs(edges, chains, min_group_size=4, gap=1.5, dx=0.4, dt=(15.0 / 180.0) * np.pi, max_k=0.3,
+                 rad=3.5, token_len=1.0) -> Polyarcs:
+    """The reference's original_code fit_polyarcs_to_all_edgel_chains after the link
+    graph and the one-chains (oracle/orig_harness.cpp: origref_polyarcs)."""
+    ref_link_contours  # noqa: B018 (loads the library through the same path)
+    global _orig
+    if _orig is None:
+        L = C.CDLL(ORIG_SO)
+        L.origref_link_contours.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_uint32),
+                                            C.c_int, C.c_int, C.POINTER(C.c_uint8), C.c_uint, C.c_double,
+                                            C.POINTER(_OrigContours)]
+        L.origref_contours_free.argtypes = [C.POINTER(_OrigContours)]
+        _orig = L
+    if not hasattr(_orig, "_poly_set"):
+        _orig.origref_polyarcs.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_uint32), C.c_int,
+                                           C.c_int, C.c_uint, C.c_double, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.POINTER(_OrigPolyarcs)]
+        _orig.origref_polyarcs_free.argtypes = [C.POINTER(_OrigPolyarcs)]
+        _orig._poly_set = True
+    e, ep, n, sz, ch = _contour_args(edges, chains)
+    o = _OrigPolyarcs()
+    rc = _orig.origref_polyarcs(ep, n, sz, ch.ctypes.data_as(C.POINTER(C.c_uint32)), ch.shape[0], ch.shape[1],
+                                min_group_size, gap, dx, dt, max_k, rad, token_len, C.byref(o))
+    if rc != 0:
+        raise ValueError(f"origref_polyarcs: {rc}")
+    try:
+        P = o.num_polyarcs
+        offs = _arr(o.offsets, P + 1, np.int64)
+        ids = _arr(o.ids, int(offs[-1]), np.int32) if offs[-1] else np.zeros(0, np.int32)
+        info = _arr(o.info, 12 * P, np.float64).reshape(P, 12)
+        return Polyarcs(offs, ids, info, o.seconds)
+    finally:
+        _orig.origref_polyarcs_free(C.byref(o))
+
+
+class _OrcPolyarcs(C.Structure):
+    _fields_ = [("num", C.c_int), ("offsets", C.POINTER(C.c_int64)), ("ids", C.POINTER(C.c_int)),
+                ("info", C.POINTER(C.c_double))]
+
+
+def polyarcs(edges, frag_offsets, frag_ids, dx=0.4, dt=(15.0 / 180.0) * np.pi, max_k=0.3, rad=3.5,
+             token_len=1.0) -> Polyarcs:
+    """The C restatement of the polyarc fit (oracle/cvl_oracle.c: orc_polyarcs_fit)
+    on given contour fragments (CSR, 0-based ids)."""
+    L = lib()
+    if not hasattr(L, "_poly_set"):
+        L.orc_polyarcs_fit.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int), C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.POINTER(_OrcPolyarcs)]
+        L.orc_polyarcs_free.argtypes = [C.POINTER(_OrcPolyarcs)]
+        L._poly_set = True
+    e, ep, n, sz = _edges_arg(edges)
+    fo = np.ascontiguousarray(frag_offsets, dtype=np.int64)
+    fi = np.ascontiguousarray(frag_ids, dtype=np.int32)
+    if fi.size == 0:
+        fi = np.zeros(1, np.int32)
+    o = _OrcPolyarcs()
+    rc = L.orc_polyarcs_fit(ep, n, sz, fo.ctypes.data_as(C.POINTER(C.c_int64)), fi.ctypes.data_as(C.POINTER(C.c_int)),
+                            fo.shape[0] - 1, dx, dt, max_k, rad, token_len, C.byref(o))
+    if rc != 0:
+        raise ValueError(f"orc_polyarcs_fit: {rc}")
+    try:
+        P = o.num
+        offs = _arr(o.offsets, P + 1, np.int64)
+        ids = _arr(o.ids, int(offs[-1]), np.int32) if offs[-1] else np.zeros(0, np.int32)
+        info = _arr(o.info, 12 * P, np.float64).reshape(P, 12)
+        return Polyarcs(offs, ids, info)
+    finally:
+        L.orc_polyarcs_free(C.byref(o))

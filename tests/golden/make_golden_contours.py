@@ -12,7 +12,11 @@ tests/golden/contours.npz:
       full for the two small files, SHA-256 digests for TO_edges.txt;
   fuzz<seed>/{edges, chains} + fuzz<seed>/<mg>_<gap>/...: random curvelet sets
       (synth.contour_fuzz) with junctions, reversed links, gaps and cycles;
-  rings<seed>/...: closed contours (synth.contour_rings).
+  rings<seed>/...: closed contours (synth.contour_rings);
+  poly/<case>/{offsets, ids, info}: the C^1 polyarcs that original_code's
+      fit_polyarcs_to_all_edgel_chains (form_curvelet_process.cpp:661-796) fits
+      along those fragments (min_group_size 4, gap 1.5; fuzz cases also at 2, 3.5),
+      read as its output type 2 (digests for TO_edges.txt).
 
     python tests/golden/make_golden_contours.py
 """
@@ -78,7 +82,28 @@ def main() -> None:
         c = O.ref_link_contours(e, ch, None, 4, 1.5)
         put(out, f"rings{seed}/4_1.5", c, True)
         print("rings", seed, c.num_frags)
+    # polyarcs along the fragments
+    for f in REF_FILES:
+        name = f.replace(".txt", "")
+        e = O.read_edge_file(os.path.join(REF_DIR, f))
+        r = O.ref_run(e, nthreads=8)
+        put_poly(out, f"poly/{name}", O.ref_polyarcs(e, r.chains), e.shape[0] < 10000)
+    for seed in (0, 1):
+        e, ch = out[f"fuzz{seed}/edges"], out[f"fuzz{seed}/chains"]
+        put_poly(out, f"poly/fuzz{seed}", O.ref_polyarcs(e, ch), True)
+        put_poly(out, f"poly/fuzz{seed}_2_3.5", O.ref_polyarcs(e, ch, 2, 3.5), True)
+        e, ch = out[f"rings{seed}/edges"], out[f"rings{seed}/chains"]
+        put_poly(out, f"poly/rings{seed}", O.ref_polyarcs(e, ch), True)
     np.savez_compressed(os.path.join(HERE, "contours.npz"), **out)
+
+
+def put_poly(out: dict, key: str, p, full: bool) -> None:
+    if full:
+        out[f"{key}/offsets"], out[f"{key}/ids"], out[f"{key}/info"] = p.offsets, p.ids, p.info
+    else:
+        out[f"{key}/digests"] = np.array([digest(p.offsets), digest(p.ids)])
+        out[f"{key}/info"] = p.info  # 1,466 rows for TO_edges: small enough to keep in full
+    print(key, p.num)
 
 
 if __name__ == "__main__":

@@ -95,3 +95,48 @@ def test_fragment_array_layout():
     a = c.as_array()
     assert a.tolist() == [[5, 6, 7, 0], [1, 2, 3, 4]]
     assert [f.tolist() for f in c.fragments()] == [[4, 5, 6], [0, 1, 2, 3]]
+
+
+# ---- polyarcs along the fragments (fit_polyarcs_to_all_edgel_chains) ----------
+def assert_same_polyarcs(p_offsets, p_ids, p_info, gc, key):
+    if f"{key}/offsets" in gc.files:
+        assert np.array_equal(p_offsets, gc[f"{key}/offsets"]), key
+        assert np.array_equal(p_ids, gc[f"{key}/ids"]), key
+    else:
+        assert [_digest(p_offsets), _digest(p_ids)] == gc[f"{key}/digests"].tolist(), key
+    return gc[f"{key}/info"]
+
+
+def _poly_cases():
+    return [("TO_edges_digit1", None), ("TO_edges_ABC_0006_thresh1", None), ("TO_edges", None),
+            ("fuzz0", (4, 1.5)), ("fuzz0_2_3.5", (2, 3.5)), ("fuzz1", (4, 1.5)), ("fuzz1_2_3.5", (2, 3.5)),
+            ("rings0", (4, 1.5)), ("rings1", (4, 1.5))]
+
+
+@pytest.mark.parametrize("case,params", _poly_cases())
+def test_polyarc_restatement_matches_reference(oracle, gc, golden_files, case, params):
+    """orc_polyarcs_fit equals original_code's fit bit for bit: chains and all 12 columns."""
+    if params is None:
+        e = golden_files[f"{case}/edges"]
+        ch = golden_files[f"{case}/chains"] if f"{case}/chains" in golden_files.files else oracle.run(e, nthreads=8).chains
+        mg, gap = 4, 1.5
+    else:
+        base = case.split("_")[0]
+        e, ch = gc[f"{base}/edges"], gc[f"{base}/chains"]
+        mg, gap = params
+    c = oracle.link_contours(e, ch, mg, gap)
+    p = oracle.polyarcs(e, c.frag_offsets, c.frag_ids)
+    info = assert_same_polyarcs(p.offsets, p.ids, p.info, gc, f"poly/{case}")
+    assert np.array_equal(p.info.view(np.uint64), info.view(np.uint64)), case
+
+
+def test_polyarc_restatement_matches_live_original_code(oracle):
+    if not oracle.orig_available():
+        pytest.skip("original_code harness not built here")
+    e, ch = synth.contour_fuzz(8, n_edges=2000, width=6)
+    for mg, gap in ((2, 2.0), (3, 3.0)):
+        c = oracle.link_contours(e, ch, mg, gap)
+        a = oracle.polyarcs(e, c.frag_offsets, c.frag_ids, dx=0.5, max_k=0.4)
+        b = oracle.ref_polyarcs(e, ch, mg, gap, dx=0.5, max_k=0.4)
+        assert np.array_equal(a.ids, b.ids) and np.array_equal(a.offsets, b.offsets)
+        assert np.array_equal(a.info.view(np.uint64), b.info.view(np.uint64))

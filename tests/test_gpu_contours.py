@@ -131,3 +131,63 @@ def test_cli_fragments_file(tmp_path, gc, golden_files, key):
                         gc[f"file/{key}/3_2.0/frag_ids"], 0).as_array()
     got = (tmp_path / "outputs" / f"frag_{key}.txt").read_text()
     assert got == "".join("".join(f"{v}\t" for v in row) + "\n" for row in want.tolist())
+
+
+# ---- C^1 polyarcs along the fragments --------------------------------------------
+POLY_EXACT = [0, 3, 4, 5, 7, 9, 10, 11]  # no transcendental input: bit-identical
+POLY_TOL = [1, 2, 6, 8]                   # the bundle's k range (sin), theta and arc length (atan2)
+
+
+def assert_polyarc_info(a, b, max_k=0.3, label=""):
+    assert a.shape == b.shape, label
+    assert np.array_equal(a[:, POLY_EXACT].view(np.uint64), b[:, POLY_EXACT].view(np.uint64)), label
+    d = np.abs(a[:, POLY_TOL] - b[:, POLY_TOL])
+    mag = np.maximum(np.abs(a[:, POLY_TOL]), np.abs(b[:, POLY_TOL]))
+    floor = 1e-9 * np.array([max_k, max_k, 1.0, 1.0])
+    assert np.all(d <= np.maximum(1e-9 * mag, floor)), (label, d.max(0))
+    return float(np.mean(a.view(np.uint64) == b.view(np.uint64)))
+
+
+@pytest.mark.parametrize("case,mg,gap", [("TO_edges_digit1", 4, 1.5), ("TO_edges_ABC_0006_thresh1", 4, 1.5),
+                                         ("TO_edges", 4, 1.5), ("fuzz0", 4, 1.5), ("fuzz0_2_3.5", 2, 3.5),
+                                         ("fuzz1_2_3.5", 2, 3.5), ("rings0", 4, 1.5), ("rings1", 4, 1.5)])
+def test_polyarcs_vs_reference(engine, gc, golden_files, case, mg, gap):
+    from tests.test_contours_cpu import assert_same_polyarcs
+    cp = cvl.ContourParams(mg, gap, fit_polyarcs=True)
+    if case.startswith("TO_edges"):
+        e = golden_files[f"{case}/edges"]
+        res, c = engine.run_contours(e, contour_params=cp)
+    else:
+        base = case.split("_")[0]
+        e, ch = gc[f"{base}/edges"], gc[f"{base}/chains"]
+        c = engine.link_contours(e, ch, cp)
+    info = assert_same_polyarcs(c.poly_offsets, c.poly_ids, c.poly_info, gc, f"poly/{case}")
+    bit = assert_polyarc_info(c.poly_info, info, label=case)
+    print(f"[polyarcs] {case}: {c.num_polyarcs} polyarcs, {bit:.4f} of info values bit-identical")
+
+
+def test_polyarcs_full_size_vs_restatement(engine, oracle):
+    """The 1920x1080 map fused: edges -> curvelets -> fragments -> polyarcs."""
+    e = synth.plain_hd(1000)
+    res, c = engine.run_contours(e, contour_params=cvl.ContourParams(fit_polyarcs=True))
+    oc = oracle.link_contours(e, res.chains)
+    p = oracle.polyarcs(e, oc.frag_offsets, oc.frag_ids)
+    assert np.array_equal(c.poly_offsets, p.offsets) and np.array_equal(c.poly_ids, p.ids)
+    bit = assert_polyarc_info(c.poly_info, p.info, label="plain_hd")
+    print(f"[polyarcs plain_hd] {c.num_polyarcs} polyarcs, {bit:.4f} bit-identical, whole path {c.device_ms:.2f} ms")
+    # off by default; other model parameters
+    assert engine.run_contours(e, want_curvelets=False)[1].poly_offsets is None
+    cp = cvl.ContourParams(2, 2.0, fit_polyarcs=True, dx=0.5, max_k=0.4)
+    _, c2 = engine.run_contours(e, contour_params=cp, want_curvelets=False)
+    oc2 = oracle.link_contours(e, res.chains, 2, 2.0)
+    p2 = oracle.polyarcs(e, oc2.frag_offsets, oc2.frag_ids, dx=0.5, max_k=0.4)
+    assert np.array_equal(c2.poly_ids, p2.ids)
+    assert_polyarc_info(c2.poly_info, p2.info, max_k=0.4, label="plain_hd dx 0.5")
+
+
+def test_polyarcs_edge_cases(engine):
+    e, ch = synth.contour_fuzz(3, n_edges=500)
+    c = engine.link_contours(e, ch[:0], cvl.ContourParams(fit_polyarcs=True))  # no fragments
+    assert c.num_polyarcs == 0 and c.poly_offsets.tolist() == [0]
+    with pytest.raises(cvl.CvlError):
+        engine.link_contours(e, ch, cvl.ContourParams(fit_polyarcs=True, token_len=0.0))
