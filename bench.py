@@ -93,7 +93,7 @@ def _workload(name: str, rank: int):
         return [synth.plain_hd(1000 + rank)], {"image": "1920x1080", "curves": 1500, "clutter": 0.2}
     if name == "contours":
         return [synth.plain_hd(1000 + rank)], {"image": "1920x1080", "curves": 1500, "clutter": 0.2,
-                                               "min_group_size": 4, "gap": 1.5}
+                                               "min_group_size": 4, "gap": 1.5, "polyarcs": True}
     if name == "plain_small":
         return [synth.plain_small(0 + rank)], {"image": "480x320", "curves": 50, "clutter": 0.1}
     if name == "stress":
@@ -568,7 +568,7 @@ def run_contours(args, maps, cfg, world, rank, local, pg):
     import curvelet_construction_on_gpu_b200 as cvl
     eng = cvl.Engine(device=local)
     e = maps[0]
-    cp = cvl.ContourParams(cfg["min_group_size"], cfg["gap"])
+    cp = cvl.ContourParams(cfg["min_group_size"], cfg["gap"], fit_polyarcs=cfg["polyarcs"])
     n_edges = int(e.shape[0])
     pinned = _pinned(e)
     for _ in range(args.warmup):
@@ -596,11 +596,14 @@ def run_contours(args, maps, cfg, world, rank, local, pg):
         for _ in range(args.steps):
             r2, c2 = eng.run_contours(pinned, contour_params=cp)
             bo += r2.chains.nbytes + r2.info.nbytes + c2.links.nbytes + c2.frag_offsets.nbytes + c2.frag_ids.nbytes
+            if c2.poly_offsets is not None:
+                bo += c2.poly_offsets.nbytes + c2.poly_ids.nbytes + c2.poly_info.nbytes
             del r2, c2
         wall = _max_over_ranks(pg, time.perf_counter() - t0)
         e2e = {"value": _sum_over_ranks(pg, float(n_edges)) * args.steps / wall, "unit": METRIC,
                "h2d_bytes_per_step": int(e.nbytes), "d2h_bytes_per_step": int(bo // args.steps),
-               "path": "cvl_run_contours (C ABI): pinned host edges in; curvelets, links and fragments out"}
+               "path": "cvl_run_contours (C ABI): pinned host edges in; curvelets, links, fragments and "
+                       "polyarcs out"}
     if rank != 0:
         eng.close()
         return
@@ -623,6 +626,8 @@ def run_contours(args, maps, cfg, world, rank, local, pg):
         "stage_ms": {k: float(np.mean([d.get(k, 0.0) for d in stage_ms])) for k in stage_ms[0]},
         "contour_stage": {"ms": cms, "edges_per_s": n_edges / (cms / 1e3) if cms > 0 else None,
                           "links_per_s": c.links.shape[0] / (cms / 1e3) if cms > 0 else None},
+        "polyarc_stage": {"ms": float(np.mean([k.get("polyarcs", 0.0) for k in stage_ms])),
+                          "polyarcs": c.num_polyarcs},
         "roofline": {"bound": "hbm", "kernel": "contour stage (k_link_* + k_trace_* + k_frag_*)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
@@ -651,6 +656,14 @@ def run_contours(args, maps, cfg, world, rank, local, pg):
                 "contour_stage_ms": rc.seconds * 1e3,
                 "same_result": bool(np.array_equal(rc.links, c.links) and np.array_equal(rc.frag_ids, c.frag_ids)
                                     and np.array_equal(rc.frag_offsets, c.frag_offsets))}
+            # the polyarc fit on the CPU: the C restatement (linear). The reference's own
+            # fit refits every earlier polyarc at the end of each fragment (quadratic) and
+            # is not timed here.
+            t0 = time.perf_counter()
+            pc = O.polyarcs(e, rc.frag_offsets, rc.frag_ids)
+            line["cpu_baseline"]["polyarc_stage"] = {
+                "ms": 1e3 * (time.perf_counter() - t0), "kind": "port", "cores": 1, "polyarcs": pc.num,
+                "same_chains": bool(np.array_equal(pc.ids, c.poly_ids) and np.array_equal(pc.offsets, c.poly_offsets))}
         else:
             t0 = time.perf_counter()
             r = O.run(e, nthreads=threads)

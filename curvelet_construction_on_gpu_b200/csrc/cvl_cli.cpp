@@ -8,6 +8,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
@@ -49,6 +50,8 @@ void print_usage(const char *prog) {
               << "                             to ../outputs/<file>, one fragment per row, 1-based ids\n"
               << "  --gap <val>                Fragment gap: consecutive edges closer than this (default: 1.5)\n"
               << "  --link-min-group <N>       Curvelets with at least N edges form links (default: 4)\n"
+              << "  --polyarcs <file>          Also fit C^1 polyarcs along the fragments and write them to\n"
+              << "                             ../outputs/<file> (1-based ids) and its info file (12 columns)\n"
               << "  --help                     Show this help message\n";
 }
 
@@ -87,7 +90,7 @@ bool parse_int(const char *arg, const char *name, int &v) {
 
 // Flag table of param_settings.hpp:86-155.
 bool parse_args(int argc, char **argv, CliParams &cp, bool &use_double, std::string &out_file, int &nthreads,
-                bool &show_help, std::string &frag_file, cvl_contour_params &lp) {
+                bool &show_help, std::string &frag_file, std::string &poly_file, cvl_contour_params &lp) {
     show_help = false;
     for (int i = 1; i < argc; i++) {
         const char *a = argv[i];
@@ -137,6 +140,8 @@ bool parse_args(int argc, char **argv, CliParams &cp, bool &use_double, std::str
         } else if (!std::strcmp(a, "--gap") && has) {
             if (!parse_num(next(), "--gap", cp.p.gap)) return false;
             lp.gap = cp.p.gap;
+        } else if (!std::strcmp(a, "--polyarcs") && has) {
+            poly_file = next();
         } else if (!std::strcmp(a, "--link-min-group") && has) {
             if (!parse_uns(next(), "--link-min-group", lp.min_group_size)) return false;
         } else {
@@ -211,14 +216,24 @@ int main(int argc, char **argv) {
     CliParams cp;
     cvl_params_default(&cp.p);
     bool help = false;
-    std::string frag_file;
+    std::string frag_file, poly_file;
     cvl_contour_params lp;
     cvl_contour_params_default(&lp);
-    if (!parse_args(argc, argv, cp, use_double, out_file, nthreads, help, frag_file, lp)) return help ? 0 : 1;
-    if (!frag_file.empty() && !use_double) {
-        std::cerr << "Error: --fragments runs in double only" << std::endl;
+    if (!parse_args(argc, argv, cp, use_double, out_file, nthreads, help, frag_file, poly_file, lp))
+        return help ? 0 : 1;
+    if ((!frag_file.empty() || !poly_file.empty()) && !use_double) {
+        std::cerr << "Error: --fragments and --polyarcs run in double only" << std::endl;
         return 1;
     }
+    if (!poly_file.empty()) {
+        // form_curvelet_mex's model parameters (original_code/main.cpp:145-151) from the flags
+        lp.fit_polyarcs = 1;
+        lp.dx = cp.p.dx;
+        lp.dt_rad = (cp.p.dt_deg / 180.0) * 3.14159265358979323846;
+        lp.max_k = cp.p.max_k;
+        lp.rad = cp.p.nrad;
+    }
+    const bool downstream = !frag_file.empty() || !poly_file.empty();
     (void)nthreads;
     std::cout << "Using scalar type: " << (use_double ? "double" : "float") << std::endl;
     // run_curvelet<double> or run_curvelet<float> (main.cpp:110)
@@ -236,7 +251,7 @@ int main(int argc, char **argv) {
     }
     cvl_result *res = nullptr;
     cvl_contours *frags = nullptr;
-    const int rc = !frag_file.empty()
+    const int rc = downstream
                        ? cvl_run_contours(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &lp, &res, &frags)
                    : use_double ? cvl_run(eng, edges.data(), n, cp.p.edge_data_sz, &cp.p, &res)
                                 : cvl_run_f32(eng, edges_f.data(), n, cp.p.edge_data_sz, &cp.p, &res);
@@ -284,12 +299,34 @@ int main(int argc, char **argv) {
         std::cout << "Link graph: " << cv.num_links << " links; contour fragments: " << cv.num_fragments
                   << " (longest " << cv.max_fragment_length << ")" << std::endl;
         std::ofstream f;
-        if (open_out(frag_file, f)) {
+        if (!frag_file.empty() && open_out(frag_file, f)) {
             for (int64_t i = 0; i < cv.num_fragments; i++) {
                 const int64_t b = cv.fragment_offsets[i], e = cv.fragment_offsets[i + 1];
                 for (int64_t j = 0; j < cv.max_fragment_length; j++)
                     f << (b + j < e ? cv.fragment_ids[b + j] + 1 : 0) << "\t";
                 f << "\n";
+            }
+        }
+        if (!poly_file.empty()) {
+            // output type 2 of original_code/main.cpp: polyarc chains (1-based, as wide as the
+            // longest, zero-padded) and their 12 info columns (curvelet::set_output)
+            std::cout << "Polyarcs: " << cv.num_polyarcs << std::endl;
+            int64_t w = 0;
+            for (int64_t i = 0; i < cv.num_polyarcs; i++)
+                w = std::max<int64_t>(w, cv.polyarc_offsets[i + 1] - cv.polyarc_offsets[i]);
+            std::ofstream pf, pi;
+            if (open_out(poly_file, pf)) {
+                for (int64_t i = 0; i < cv.num_polyarcs; i++) {
+                    const int64_t b = cv.polyarc_offsets[i], e = cv.polyarc_offsets[i + 1];
+                    for (int64_t j = 0; j < w; j++) pf << (b + j < e ? cv.polyarc_ids[b + j] + 1 : 0) << "\t";
+                    pf << "\n";
+                }
+            }
+            if (open_out(info_name(poly_file), pi)) {
+                for (int64_t i = 0; i < cv.num_polyarcs; i++) {
+                    for (int j = 0; j < 12; j++) pi << cv.polyarc_info[i * 12 + j] << "\t";
+                    pi << "\n";
+                }
             }
         }
         cvl_contours_free(frags);

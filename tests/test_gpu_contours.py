@@ -191,3 +191,33 @@ def test_polyarcs_edge_cases(engine):
     assert c.num_polyarcs == 0 and c.poly_offsets.tolist() == [0]
     with pytest.raises(cvl.CvlError):
         engine.link_contours(e, ch, cvl.ContourParams(fit_polyarcs=True, token_len=0.0))
+
+
+@pytest.mark.parametrize("key", ["TO_edges_digit1", "TO_edges_ABC_0006_thresh1"])
+def test_cli_polyarcs_files(tmp_path, gc, golden_files, key):
+    """CURVELET --polyarcs writes output type 2: the polyarc chains (1-based, zero-padded
+    to the longest) and their 12 info columns, 6 significant digits as the reference's
+    writer prints them; the usual outputs stay byte-identical."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cli_bin = os.path.join(root, "curvelet_construction_on_gpu_b200", "bin", "CURVELET")
+    for d in ("bin", "test_files", "outputs"):
+        (tmp_path / d).mkdir(exist_ok=True)
+    synth.write_edge_file(str(tmp_path / "test_files" / f"{key}.txt"), golden_files[f"{key}/edges"])
+    r = subprocess.run([cli_bin, "--double", "--edge-file", f"{key}.txt", "--output", f"chain_{key}.txt",
+                        "--polyarcs", f"chain_poly_{key}.txt"], cwd=tmp_path / "bin", capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    cli = np.load(os.path.join(GOLDEN, "cli_outputs.npz"))
+    assert (tmp_path / "outputs" / f"chain_{key}.txt").read_bytes() == cli[f"{key}/chain"].tobytes()
+    offs, ids, info = gc[f"poly/{key}/offsets"], gc[f"poly/{key}/ids"], gc[f"poly/{key}/info"]
+    w = int(np.diff(offs).max())
+    rows = [[int(v) + 1 for v in ids[offs[i]:offs[i + 1]]] + [0] * (w - (offs[i + 1] - offs[i]))
+            for i in range(len(offs) - 1)]
+    got = (tmp_path / "outputs" / f"chain_poly_{key}.txt").read_text()
+    assert got == "".join("".join(f"{v}\t" for v in row) + "\n" for row in rows)
+    printed = np.array([[float(x) for x in ln.split()] for ln in
+                        (tmp_path / "outputs" / f"info_poly_{key}.txt").read_text().splitlines()])
+    assert printed.shape == info.shape
+    mag = np.maximum(np.abs(printed), np.abs(info))
+    assert np.all(np.abs(printed - info) <= 5e-6 * mag + 1e-300)  # 6 significant digits
