@@ -675,17 +675,10 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     growth_fn<R> gf;
     pick_kernels(cpl, tn, bf, gf);
     const size_t gsmem = (size_t)(GROWTH_THREADS / 32) * growth_smem_per_warp(md.max_cand, md.gms);
-    int gbps = 0;
-    {
-        // occupancy of the chosen growth kernel
-        cudaFuncAttributes fa{};
-        (void)fa;
-    }
     const unsigned long long max_chunk_pairs = per_chunk + (unsigned long long)ro.max_deg + 1;
     CVL_TRY(e->alloc(e->bund, sizeof(R) * 64 * (size_t)cpl * std::min<unsigned long long>(P + 1, max_chunk_pairs)));
     const int bblocks = e->prop.multiProcessorCount * 8;
     const int gblocks = e->prop.multiProcessorCount * 8;
-    (void)gbps;
 
     for (int attempt = 0;; ++attempt) {
         // the growth warps reserve the arena in chunks of at most GROWTH_ARENA_CHUNK
