@@ -80,6 +80,8 @@ def _args():
     ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")
     ap.add_argument("--requests", type=int, default=600, help="served stream: requests per rate")
     ap.add_argument("--workers", type=int, default=4, help="served stream: server workers")
+    ap.add_argument("--large-yield-ms", type=int, default=10,
+                    help="served stream: longest hold-back of a large launch between chunks (0: none)")
     ap.add_argument("--large-workers", type=int, default=0,
                     help="served stream: workers on the large-map lane (0: half of them)")
     args = ap.parse_args()
@@ -349,7 +351,7 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
     picks = np.asarray(sequence) if sequence is not None else rng.integers(0, len(maps), n_req)
     n_req = len(picks)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-    srv = cvl.Server(device=device, workers=workers, large_workers=_LARGE_WORKERS)
+    srv = cvl.Server(device=device, workers=workers, large_workers=_LARGE_WORKERS, large_yield_ms=_LARGE_YIELD_MS)
     try:
         # warm-up (workspace and page-locked arena growth): the largest map once per
         # worker, then every map of the pool once (or a few of each class)
@@ -412,7 +414,7 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
         classes[lab] = {"requests": int(sel.sum()), "p50_ms": pct(ms[sel], 50), "p99_ms": pct(ms[sel], 99)}
     edges = float(np.sum(ed))
     return {"rate_maps_per_s": rate, "requests": n_req, "workers": workers,
-            "large_workers": _LARGE_WORKERS or max(1, workers // 2),
+            "large_workers": _LARGE_WORKERS or max(1, workers // 2), "large_yield_ms": _LARGE_YIELD_MS,
             "wall_s": wall,
             "edges_per_s": edges / wall, "maps_per_s": len(ms) / wall,
             "p50_ms": pct(ms, 50), "p95_ms": pct(ms, 95), "p99_ms": pct(ms, 99), "max_ms": float(np.max(ms)),
@@ -741,12 +743,14 @@ def run_stress(args, maps, cfg, world, rank, local, pg):
 
 
 _LARGE_WORKERS = 0  # the served stream's large-lane workers (--large-workers; 0: half of them)
+_LARGE_YIELD_MS = 10  # --large-yield-ms
 
 
 def main():
-    global _LARGE_WORKERS
+    global _LARGE_WORKERS, _LARGE_YIELD_MS
     args = _args()
     _LARGE_WORKERS = args.large_workers
+    _LARGE_YIELD_MS = args.large_yield_ms
     world, rank, local, pg = _dist_init(args)
     maps, cfg = _workload(args.workload, rank)
     try:

@@ -61,7 +61,7 @@ class CvlServerCfg(C.Structure):
     _fields_ = [("device", C.c_int), ("workers", C.c_int), ("mem_budget_bytes", C.c_size_t),
                 ("admit_bytes_per_edge", C.c_size_t), ("max_batch_edges", C.c_int64),
                 ("large_map_edges", C.c_int64), ("host_reserve_bytes", C.c_size_t),
-                ("small_takes_large", C.c_int), ("large_workers", C.c_int)]
+                ("small_takes_large", C.c_int), ("large_workers", C.c_int), ("large_yield_ms", C.c_int)]
 
 
 class CvlServerStats(C.Structure):

@@ -564,7 +564,8 @@ class Server:
     def __init__(self, params: CurveletParams | None = None, device: int = 0, workers: int = 4,
                  mem_budget_bytes: int = 40 << 30, admit_bytes_per_edge: int = 2048,
                  max_batch_edges: int = 2 << 20, large_map_edges: int = 1_000_000,
-                 host_reserve_bytes: int = 2 << 30, small_takes_large: bool = False, large_workers: int = 0):
+                 host_reserve_bytes: int = 2 << 30, small_takes_large: bool = False, large_workers: int = 0,
+                 large_yield_ms: int = 10):
         lib = _abi.load()
         self._lib = lib
         cfg = _abi.CvlServerCfg()
@@ -575,6 +576,7 @@ class Server:
         cfg.host_reserve_bytes = host_reserve_bytes
         cfg.small_takes_large = 1 if small_takes_large else 0
         cfg.large_workers = large_workers
+        cfg.large_yield_ms = large_yield_ms
         self._p = (params or CurveletParams()).to_c()
         h = C.c_void_p()
         check(lib.cvl_server_create(C.byref(cfg), C.byref(self._p), C.byref(h)), "cvl_server_create")

@@ -117,7 +117,7 @@ struct cvl_server {
     void worker(int w);
 
     // Engine hook of a worker running a large launch, called between its chunks:
-    // while small-lane work is queued or running, hold back (10 ms at most), so
+    // while small-lane work is queued or running, hold back (large_yield_ms at most), so
     // that a small map does not share the SMs with a large map's chunks. Only
     // when the server is not backlogged: with requests piling up, the GPU must
     // not idle and the large launch goes on.
@@ -125,7 +125,7 @@ struct cvl_server {
     static void yield_to_small(void *ctx) {
         cvl_server *s = (cvl_server *)ctx;
         std::unique_lock<std::mutex> lk(s->mu);
-        s->cv_yield.wait_for(lk, std::chrono::milliseconds(10), [&] {
+        s->cv_yield.wait_for(lk, std::chrono::milliseconds(s->cfg.large_yield_ms), [&] {
             const size_t queued = s->lanes[0].size() + s->lanes[1].size();
             return s->stop || queued > YIELD_MAX_QUEUED || (s->small_running == 0 && s->lanes[0].empty());
         });
@@ -165,7 +165,8 @@ void cvl_server::worker(int w) {
         }
         cv_yield.notify_all();
         // a large launch yields to small ones between its chunks (with another worker to run them)
-        cvl_engine_set_yield(e, (lane_now == 1 && cfg.workers >= 2) ? &cvl_server::yield_to_small : nullptr, this);
+        cvl_engine_set_yield(e, (lane_now == 1 && cfg.workers >= 2 && cfg.large_yield_ms > 0)
+                                    ? &cvl_server::yield_to_small : nullptr, this);
         // one edge_data_sz per launch: a request with another width goes alone
         size_t cut = 1;
         while (cut < take.size() && take[cut]->sz == take[0]->sz) ++cut;
@@ -249,6 +250,7 @@ void cvl_server_cfg_default(cvl_server_cfg *c) {
     c->host_reserve_bytes = (size_t)2 << 30;
     c->small_takes_large = 0;
     c->large_workers = 0;
+    c->large_yield_ms = 10;
 }
 
 int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out) {
@@ -258,6 +260,7 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
     cvl_server_cfg_default(&c);
     if (cfg) c = *cfg;
     if (c.workers < 1 || c.workers > 16) return cvl_fail(CVL_EINVAL, "workers must be in [1, 16]");
+    if (c.large_yield_ms < 0 || c.large_yield_ms > 1000) return cvl_fail(CVL_EINVAL, "large_yield_ms must be in [0, 1000]");
     if (c.large_workers == 0) c.large_workers = std::max(1, c.workers / 2);
     if (c.workers >= 2 && c.large_workers >= c.workers) c.large_workers = c.workers - 1;
     if (c.large_workers < 1) return cvl_fail(CVL_EINVAL, "large_workers must be 0 (automatic) or in [1, workers - 1]");

@@ -318,6 +318,8 @@ typedef struct cvl_server_cfg {
                                       [1, workers - 1]; 0 = half of them, at least one (0: 2 of 4 workers,
                                       measured to cut the large maps' p99 by 10-30% at 50-80 maps/s and
                                       keep the small maps' within 22-38 ms) */
+    int large_yield_ms;            /* a large-lane launch holds back between its chunks while small-lane
+                                      work is queued or running, for at most this long each time; 0 = never (10) */
 } cvl_server_cfg;
 
 typedef struct cvl_server_stats {
