@@ -435,6 +435,28 @@ struct NbArgsT {
 // COUNT: ncand[i], per-map pairs / max degree / truncated anchors.
 // FILL:  the CSR row of anchor i at pair_off[i] sorted by (d2, scan key), and
 //        optionally the pair classes, pair->anchor map and anchor trig table.
+// The direction class of a neighbour (:454-462): the sign of
+// dot(angle_from_pt_to_pt(te, le), te's orientation) (curvelet_utils.hpp:58-69),
+// 0 ahead, 1 behind, 2 exactly perpendicular. That dot is the cosine of the angle
+// between the neighbour's direction and the orientation, computed through atan2,
+// To2Pi, cos and sin with an error of a few ulps: below 5e-15 in double and 2e-6 in
+// float. v = dx cos(theta) + dy sin(theta) is that cosine times the vector's length,
+// which is at most |dx| + |dy|, and is computed here to about 1e-15 of |dx| + |dy|.
+// So when |v| exceeds 1e-12 (double) or 1e-4 (float) of |dx| + |dy|, the sign of v
+// is the sign of the reference's dot, and the three transcendental calls are
+// skipped; nearer to perpendicular, the reference's own expression decides.
+template <typename T>
+__device__ __forceinline__ unsigned direction_class(T ax, T ay, T lx, T ly, T cosT2, T sinT2) {
+    const double dx = (double)lx - (double)ax, dy = (double)ly - (double)ay;
+    const double v = dx * (double)cosT2 + dy * (double)sinT2;
+    const double margin = (sizeof(T) == sizeof(double) ? 1e-12 : 1e-4) * (fabs(dx) + fabs(dy));
+    if (v > margin) return 0u;
+    if (v < -margin) return 1u;
+    const T dir = to_2pi(cvl_atan2(ly - ay, lx - ax));      // angle_from_pt_to_pt(te, le)
+    const T d = cvl_cos(dir) * cosT2 + cvl_sin(dir) * sinT2;  // dot(dir, te_orient)
+    return (d > 0) ? 0u : ((d < 0) ? 1u : 2u);
+}
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_nb(NbArgsT<T> a) {
     extern __shared__ __align__(16) unsigned char nb_smem[];
@@ -533,9 +555,7 @@ __global__ void __launch_bounds__(256) k_nb(NbArgsT<T> a) {
             if (a.pcls) {
                 // direction filter (:454-462) and close pair (:682)
                 const T lx = a.B.x[nn], ly = a.B.y[nn];
-                const T dir = to_2pi(cvl_atan2(ly - ay, lx - ax));      // angle_from_pt_to_pt(te, le)
-                const T d = cvl_cos(dir) * cosT2 + cvl_sin(dir) * sinT2;  // dot(dir, te_orient)
-                const unsigned run = (d > 0) ? 0u : ((d < 0) ? 1u : 2u);
+                const unsigned run = direction_class(ax, ay, lx, ly, cosT2, sinT2);
                 const T DX = ax - lx, DY = ay - ly;
                 const bool close = (DX * DX + DY * DY < md.four_dx_dx);
                 a.pcls[off + rk] = (unsigned char)(run | (close ? 4u : 0u));

@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(128) k_polyarcs(PolyArgs a) {
             auto hypothesis = [&](int ib, double *bmin, double *bmax) -> bool {
                 const double *B = a.edges + (size_t)ib * a.sz;
                 const double bx = B[0], by = B[1], T0 = B[2];
-                const double dir = to_2pi(cvl_atan2(by - ay, bx - ax));  // vPointPoint(A, B)
-                if (!(cvl_cos(dir) * cosT2 + cvl_sin(dir) * sinT2 > 0)) return false;  // dot(dir, A's orientation)
+                // dot(vPointPoint(A, B), A's orientation) > 0: B ahead of A
+                if (direction_class(ax, ay, bx, by, cosT2, sinT2) != 0u) return false;
                 __syncwarp();  // sM / sP of the previous pair are read
                 for (int j = lane; j < md.Q; j += 32) {
                     const double t = T2 + grid_offset(md.st, j, md.Q);
