@@ -11,7 +11,7 @@ from curvelet_construction_on_gpu_b200 import _abi, autotune, synth
 pytestmark = pytest.mark.gpu
 
 VARIANTS = [
-    dict(cell_size=2), dict(cell_size=8), dict(bundle_blocks_per_sm=3), dict(growth_blocks_per_sm=6),
+    dict(cell_size=2), dict(cell_size=8), dict(bundle_blocks_per_sm=3), dict(growth_blocks_per_sm=6), dict(growth_blocks_per_sm=4),
     dict(seeds_per_group=8), dict(anchors_per_warp=1), dict(anchors_per_warp=16), dict(chunk_pairs=1 << 16),
     dict(cell_size=8, seeds_per_group=8, anchors_per_warp=2, bundle_blocks_per_sm=3, chunk_pairs=1 << 18),
 ]
