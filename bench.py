@@ -422,6 +422,8 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
             "launches": int(st["launches"] - st0["launches"]), "failed": int(st["failed"]),
             "worker_ms": {k: float(st[k] - st0[k]) for k in ("upload_ms", "run_ms", "device_ms", "result_ms")},
             "queue_ms_mean": float(st["queue_ms"] - st0["queue_ms"]) / max(1, len(ms)),
+            "growth_during_stream": {k: float(st[k] - st0[k]) for k in ("device_grows", "device_grow_ms",
+                                                                        "host_grows", "host_grow_ms")},
             "admission": "40 GiB budget, 2048 B per edge", "pool": f"{len(maps)} seeded maps"}
 
 

@@ -61,7 +61,8 @@ class CvlServerCfg(C.Structure):
     _fields_ = [("device", C.c_int), ("workers", C.c_int), ("mem_budget_bytes", C.c_size_t),
                 ("admit_bytes_per_edge", C.c_size_t), ("max_batch_edges", C.c_int64),
                 ("large_map_edges", C.c_int64), ("host_reserve_bytes", C.c_size_t),
-                ("small_takes_large", C.c_int), ("large_workers", C.c_int), ("large_yield_ms", C.c_int)]
+                ("small_takes_large", C.c_int), ("large_workers", C.c_int), ("large_yield_ms", C.c_int),
+                ("device_reserve_bytes", C.c_size_t)]
 
 
 class CvlServerStats(C.Structure):
@@ -70,7 +71,8 @@ class CvlServerStats(C.Structure):
                 ("edges_completed", C.c_uint64), ("admitted_bytes", C.c_size_t), ("p50_ms", C.c_double),
                 ("p95_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
                 ("upload_ms", C.c_double), ("run_ms", C.c_double), ("device_ms", C.c_double),
-                ("result_ms", C.c_double), ("queue_ms", C.c_double)]
+                ("result_ms", C.c_double), ("queue_ms", C.c_double), ("device_grows", C.c_uint64),
+                ("device_grow_ms", C.c_double), ("host_grows", C.c_uint64), ("host_grow_ms", C.c_double)]
 
 
 class CvlTuning(C.Structure):

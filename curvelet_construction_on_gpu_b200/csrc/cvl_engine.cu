@@ -8,6 +8,8 @@
 // The two syncs size the CSR/record and output buffers exactly; everything
 // else stays on the device.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -87,6 +89,7 @@ struct cvl_engine {
     cudaDeviceProp prop{};
     size_t budget = 0;
     size_t held = 0;
+    std::atomic<uint64_t> dev_grows{0}, dev_grow_ns{0};  // workspace allocations and their host time
     int cell_size = 4;
     int seeds_per_group = 4;
     int slots = 10;
@@ -154,7 +157,11 @@ struct cvl_engine {
                 return fail(CVL_ENOMEM, "device memory budget exceeded (" + std::to_string(held + want) + " > " +
                                             std::to_string(budget) + " bytes)");
         }
+        const auto t_grow = std::chrono::steady_clock::now();
         cudaError_t e = cudaMallocFromPoolAsync(&b.p, want, pool, stream);
+        dev_grow_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                           std::chrono::steady_clock::now() - t_grow).count();
+        ++dev_grows;
         if (e != cudaSuccess) {
             b.p = nullptr;
             cudaGetLastError();
@@ -1422,6 +1429,20 @@ void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx) {
     e->yield_ctx = ctx;
 }
 
+int cvl_engine_reserve_device(cvl_engine *e, size_t bytes) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    if (!bytes) return CVL_OK;
+    CVL_CUDA(cudaSetDevice(e->device));
+    void *p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, bytes, e->pool, e->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CVL_ENOMEM, "device memory could not be reserved (" + std::to_string(bytes) + " bytes)");
+    }
+    CVL_CUDA(cudaFreeAsync(p, e->stream));
+    CVL_CUDA(cudaStreamSynchronize(e->stream));
+    return CVL_OK;
+}
+
 int cvl_engine_reserve_host(cvl_engine *e, size_t bytes) {
     if (!e) return fail(CVL_EINVAL, "engine is NULL");
     if (bytes && !e->pinned->reserve(bytes)) return fail(CVL_ENOMEM, "page-locked host memory could not be reserved");
@@ -2267,4 +2288,12 @@ extern "C" int cvl_engine_device_results(cvl_engine *e, cvl_device_results *out)
     out->info = (const double *)e->info.p;
     out->done_event = (void *)e->dev_done;
     return CVL_OK;
+}
+
+void cvl_engine_growth(const cvl_engine *e, uint64_t *dev_grows, double *dev_ms, uint64_t *host_grows,
+                       double *host_ms) {
+    *dev_grows = e->dev_grows.load();
+    *dev_ms = (double)e->dev_grow_ns.load() * 1e-6;
+    *host_grows = e->pinned->grows();
+    *host_ms = e->pinned->grow_ms();
 }

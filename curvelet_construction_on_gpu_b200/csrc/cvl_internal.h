@@ -2,6 +2,7 @@
 // beyond the public C ABI.
 #pragma once
 
+#include <cstdint>
 #include <string>
 
 // Records msg as the calling thread's cvl_last_error() and returns code.
@@ -19,3 +20,14 @@ void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx);
 // Sets aside `bytes` of page-locked host memory in the engine's result arena
 // (one chunk made ahead of time, so results do not pin memory while serving).
 int cvl_engine_reserve_host(cvl_engine *e, size_t bytes);
+
+// Maps `bytes` of device memory into the engine's memory pool ahead of time (an
+// allocation freed at once: the pool keeps what it has), so that later workspace
+// growth is carved from memory already mapped.
+int cvl_engine_reserve_device(cvl_engine *e, size_t bytes);
+
+// Growth of the engine's memory so far: device workspace allocations (calls that
+// allocated from the engine's pool) and page-locked result chunks, with the host
+// time the calls took.
+void cvl_engine_growth(const cvl_engine *e, uint64_t *dev_grows, double *dev_ms, uint64_t *host_grows,
+                       double *host_ms);

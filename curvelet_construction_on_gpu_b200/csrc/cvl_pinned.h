@@ -11,7 +11,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstddef>
+#include <cstdint>
 #include <iterator>
 #include <map>
 #include <mutex>
@@ -41,7 +44,12 @@ class PinnedArena {
         for (const Chunk &c : chunks_) total += c.size;
         const size_t want = round(std::max({bytes, first_, total}));
         void *base = nullptr;
-        if (cudaMallocHost(&base, want) != cudaSuccess) {
+        const auto t0 = std::chrono::steady_clock::now();
+        const cudaError_t ce = cudaMallocHost(&base, want);
+        grow_ns_ += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                        std::chrono::steady_clock::now() - t0).count();
+        ++grows_;
+        if (ce != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
@@ -77,6 +85,10 @@ class PinnedArena {
         c.free[off] = len;
     }
 
+    // chunks pinned so far (cudaMallocHost calls) and the host time they took
+    uint64_t grows() const { return grows_.load(); }
+    double grow_ms() const { return (double)grow_ns_.load() * 1e-6; }
+
     // ensures one free range of at least `bytes` (a chunk made ahead of time)
     bool reserve(size_t bytes) {
         void *p = get(bytes);
@@ -108,6 +120,7 @@ class PinnedArena {
     }
 
     std::mutex mu_;
+    std::atomic<uint64_t> grows_{0}, grow_ns_{0};
     size_t first_;
     std::vector<Chunk> chunks_;
     std::unordered_map<void *, std::pair<size_t, size_t>> live_;

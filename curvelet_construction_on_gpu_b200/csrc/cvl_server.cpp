@@ -251,6 +251,7 @@ void cvl_server_cfg_default(cvl_server_cfg *c) {
     c->small_takes_large = 0;
     c->large_workers = 0;
     c->large_yield_ms = 10;
+    c->device_reserve_bytes = 0;
 }
 
 int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out) {
@@ -285,7 +286,14 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
             return cvl_fail(rc, msg);
         }
         s->engines.push_back(e);
-        const int rr = cvl_engine_reserve_host(e, c.host_reserve_bytes);
+        // device memory for the largest launch the worker will fold (admission's model of
+        // the footprint), mapped now so that the stream never waits on a memory mapping
+        size_t dev_reserve = c.device_reserve_bytes;
+        if (!dev_reserve)
+            dev_reserve = std::min((size_t)c.max_batch_edges * c.admit_bytes_per_edge,
+                                   c.mem_budget_bytes / (size_t)c.workers);
+        int rr = cvl_engine_reserve_device(e, dev_reserve);
+        if (rr == CVL_OK) rr = cvl_engine_reserve_host(e, c.host_reserve_bytes);
         if (rr != CVL_OK) {
             const std::string msg = cvl_last_error();
             for (cvl_engine *x : s->engines) cvl_engine_destroy(x);
@@ -421,6 +429,17 @@ int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out) {
         st.result_ms = s->result_ms;
         st.queue_ms = s->queue_ms;
         l = s->lat_ms;
+    }
+    st.host_grows = s->host.grows();
+    st.host_grow_ms = s->host.grow_ms();
+    for (cvl_engine *e : s->engines) {
+        uint64_t dg = 0, hg = 0;
+        double dms = 0, hms = 0;
+        cvl_engine_growth(e, &dg, &dms, &hg, &hms);
+        st.device_grows += dg;
+        st.device_grow_ms += dms;
+        st.host_grows += hg;
+        st.host_grow_ms += hms;
     }
     if (!l.empty()) {
         std::sort(l.begin(), l.end());

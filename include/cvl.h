@@ -320,6 +320,10 @@ typedef struct cvl_server_cfg {
                                       keep the small maps' within 22-38 ms) */
     int large_yield_ms;            /* a large-lane launch holds back between its chunks while small-lane
                                       work is queued or running, for at most this long each time; 0 = never (10) */
+    size_t device_reserve_bytes;   /* device memory each worker's engine maps ahead of time (its memory pool
+                                      keeps it), so that a launch larger than any before it grows its workspace
+                                      without mapping new memory mid-stream; 0 = max_batch_edges x
+                                      admit_bytes_per_edge, at most mem_budget_bytes / workers (0) */
 } cvl_server_cfg;
 
 typedef struct cvl_server_stats {
@@ -337,6 +341,12 @@ typedef struct cvl_server_stats {
     double device_ms;              /* of which the device time of the runs (CUDA events) */
     double result_ms;              /* each map's rows to its page-locked result */
     double queue_ms;               /* summed over requests: submit -> taken by a worker */
+    /* memory growth so far (each stalls the calling worker; page-locked growth can
+     * hold up the process's other CUDA calls too) */
+    uint64_t device_grows;         /* device workspace allocations of the workers' engines */
+    double device_grow_ms;         /* host time of those calls */
+    uint64_t host_grows;           /* page-locked chunks pinned: request staging and results */
+    double host_grow_ms;           /* host time of those cudaMallocHost calls */
 } cvl_server_stats;
 
 void cvl_server_cfg_default(cvl_server_cfg *cfg);
