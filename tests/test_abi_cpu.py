@@ -97,7 +97,7 @@ def test_server_defaults_and_argument_checks():
     assert (cfg.device, cfg.workers, cfg.mem_budget_bytes) == (0, 4, 40 << 30)
     assert (cfg.admit_bytes_per_edge, cfg.max_batch_edges, cfg.large_map_edges) == (2048, 2 << 20, 1_000_000)
     assert cfg.host_reserve_bytes == 2 << 30 and cfg.small_takes_large == 0 and cfg.large_workers == 0
-    assert cfg.large_yield_ms == 10
+    assert cfg.large_yield_ms == 10 and cfg.device_reserve_bytes == 0
     ec = _abi.CvlEngineCfg()
     lib.cvl_engine_cfg_default(C.byref(ec))
     assert ec.stream_priority == 0
