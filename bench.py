@@ -51,17 +51,17 @@ sys.path.insert(0, ROOT)
 METRIC = "edges/s"
 # per computed (non-close) pair: 63 cells x 20 FP64 flops, divisions counted as 1
 FLOPS_PER_PAIR_CELL = 20
-# DRAM bytes of k_bundles per computed pair, from one ncu capture of the kernel on
-# the 242k-edge 1920x1080 map: dram__bytes_read.sum 0.338025 GB + dram__bytes_write.sum
-# 2.194154 GB over 2,176,780 non-close pairs (profiles/kernels_plain_hd.md). The
-# traffic is the bundle write (1,008 B per pair) plus the pair/anchor reads, so it
-# scales with the pairs a launch processes.
-BUNDLE_DRAM_BYTES_PER_PAIR = (0.338025e9 + 2.194154e9) / 2_176_780
+# DRAM bytes of k_bundles per computed pair, from one ncu capture of the kernel
+# (--set full) on the 242k-edge 1920x1080 map: dram__bytes_read.sum 0.334855 GB +
+# dram__bytes_write.sum 2.185202 GB over 2,176,780 non-close pairs. The traffic is
+# the bundle write (1,008 B per pair) plus the pair/anchor reads, so it scales with
+# the pairs a launch processes.
+BUNDLE_DRAM_BYTES_PER_PAIR = (0.334855e9 + 2.185202e9) / 2_176_780
 # FP64-pipe instructions of k_bundles per cell, from the same capture: the pipe was
-# active 45.38% of 1.046336 ms on 148 SMs (each issues 2 FP64 warp-instructions a
-# cycle at 1.965 GHz), 30.65 active lanes per warp-instruction, 2,176,780 x 63 cells.
+# active 49.02% of 0.999232 ms on 148 SMs (each issues 2 FP64 warp-instructions a
+# cycle at 1.965 GHz), 30.59 active lanes per warp-instruction, 2,176,780 x 63 cells.
 # A division costs about 10 of them, which the algorithmic count above takes as 1 flop.
-BUNDLE_FP64_INSTR_PER_CELL = 0.4538 * 1.046336e-3 * 148 * 2 * 1.965e9 * 30.65 / (2_176_780 * 63)
+BUNDLE_FP64_INSTR_PER_CELL = 0.4902 * 0.999232e-3 * 148 * 2 * 1.965e9 * 30.59 / (2_176_780 * 63)
 
 
 def _args():
@@ -112,7 +112,9 @@ class _Clocks:
     """Samples SM clocks and throttle reasons while the timed region runs."""
 
     def __init__(self, index: int):
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        # the nvidia-smi samples go to $CVL_BENCH_OUT (default bench_out/ beside this file)
+        self.path = os.path.join(os.environ.get("CVL_BENCH_OUT", os.path.join(ROOT, "bench_out")),
+                                 f"clocks_rank{index}.csv")
         self.proc = None
         self.index = index
 
@@ -728,7 +730,7 @@ def run_served(args, maps, cfg, world, rank, local, pg):
 
 
 def run_stress(args, maps, cfg, world, rank, local, pg):
-    """The stress stream: every map once, in its seeded
+    """The stress stream (16 dense 3840x2160 maps among 1,024 small 640x480 maps): every map once, in its seeded
     interleaved order, Poisson at --rate (150 maps/s unless given); small-map
     latency reported apart from the dense maps'."""
     rate = args.rate if args.rate_given else 150.0
