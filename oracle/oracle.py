@@ -137,6 +137,10 @@ def ref_lib():
         L.cvlref_run_f32.argtypes = [C.POINTER(C.c_float)] + L.cvlref_run.argtypes[1:]
         L.cvlref_free.argtypes = [C.POINTER(_RefOut)]
         L.cvlref_pair_bundle.argtypes = [C.c_double] * 12 + [dp, dp, C.POINTER(C.c_int)]
+        ip = C.POINTER(C.c_int)
+        L.cvlref_run_csr.argtypes = [dp, C.c_int, C.c_int] + [C.c_double] * 6 + [C.c_uint, C.c_uint, ip, ip,
+                                                                               C.POINTER(_RefOut)]
+        L.cvlref_run_csr_f32.argtypes = [C.POINTER(C.c_float)] + L.cvlref_run_csr.argtypes[1:]
         _ref = L
     return _ref
 
@@ -217,6 +221,91 @@ def ref_run(edges, nthreads=1, want_outputs=True, scalar="double", **params) -> 
                       int(r.valid_pairs), np_, int(r.max_num_of_neighbors), csr=csr, ms=ms)
     finally:
         ref_lib().cvlref_free(C.byref(r))
+
+
+def ref_run_csr(edges, offsets, ids, scalar="double", **params) -> Result:
+    """The reference's CurveletCPU stage (form_pairwise_bundles, build_curvelets_greedy,
+    cpu_curvelet.hpp:305-634) run on the given neighbour lists instead of the ones
+    build_neighbor_csr_graph makes: the reference's own answer for a chosen CSR,
+    e.g. one whose truncated anchors keep the lowest edge indices of a pixel cell."""
+    p = dict(DEFAULTS, **params)
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    nid = np.ascontiguousarray(ids, dtype=np.int32)
+    ip = C.POINTER(C.c_int)
+    r = _RefOut()
+    if scalar == "float":
+        e = np.ascontiguousarray(edges, dtype=np.float32)
+        f, ptr = ref_lib().cvlref_run_csr_f32, e.ctypes.data_as(C.POINTER(C.c_float))
+    else:
+        e = np.ascontiguousarray(edges, dtype=np.float64)
+        f, ptr = ref_lib().cvlref_run_csr, e.ctypes.data_as(C.POINTER(C.c_double))
+    n, sz = e.shape
+    assert off.shape == (n + 1,) and nid.shape == (int(off[-1]),)
+    rc = f(ptr, n, sz, p["nrad"], p["dx"], p["dt_deg"], p["max_k"], p["sx"], p["st"], p["group_max_sz"],
+           p["max_candidates"], off.ctypes.data_as(ip), nid.ctypes.data_as(ip), C.byref(r))
+    if rc != 0:
+        raise ValueError(f"cvlref_run_csr failed ({rc})")
+    try:
+        w, nc, np_ = r.chain_width, r.num_curvelets, r.total_neighbor_pairs
+        csr = Csr(_arr(r.neighbor_offsets, n + 1, np.int32), _arr(r.neighbor_ids, np_, np.int32),
+                  _arr(r.neighbor_dist2, np_, np.float64), int(r.max_num_of_neighbors))
+        return Result(_arr(r.chains, nc * w, np.uint32).reshape(nc, w),
+                      _arr(r.info, nc * 10, np.float64).reshape(nc, 10),
+                      int(r.valid_pairs), np_, int(r.max_num_of_neighbors), csr=csr)
+    finally:
+        ref_lib().cvlref_free(C.byref(r))
+
+
+def build_csr_f32(edges, nrad=3.5, neighbor_radius=3, max_candidates=128) -> Csr:
+    """The neighbour CSR of run_curvelet<float> (preprocess.hpp:62-274 with T = float),
+    restated in numpy float32 arithmetic, for small maps. Pixel cells are
+    (lrint(x), lrint(y)) of the float coordinates (:84-86); a candidate is an edge of
+    a cell of the (2w+1)^2 window, scanned py outer and px inner (:137-138), whose
+    float squared distance, ((x1-x2)*(x1-x2)) + ((y1-y2)*(y1-y2)) (curvelet_utils.hpp:14-17),
+    is <= rad*rad, a float product (:223, :157-160); the first max_candidates in scan
+    order are kept (:162-164) and sorted by distance (:168-173). Inside a cell, edges
+    come in ascending index, and equal distances keep scan order: the orders the
+    reference's unstable std::sort leaves to libstdc++ (:90-92, :168) are fixed the
+    same way as in the C restatement of the FP64 path (orc_build_csr)."""
+    e = np.ascontiguousarray(edges, dtype=np.float32)
+    n = e.shape[0]
+    if n <= 0 or e.shape[1] < 4:
+        raise ValueError("build_csr_f32 takes a non-empty map of >= 4 values per edge")
+    x, y = e[:, 0], e[:, 1]
+    cx = np.rint(x).astype(np.int64)
+    cy = np.rint(y).astype(np.int64)
+    cells: dict = {}
+    for i in range(n):
+        cells.setdefault((int(cx[i]), int(cy[i])), []).append(i)
+    cells = {k: np.array(v, np.int64) for k, v in cells.items()}
+    rad = np.float32(nrad)
+    rad_sqr = np.float32(rad * rad)
+    w = int(neighbor_radius)
+    offs = [0]
+    ids_out, d2_out = [], []
+    maxdeg = truncated = ties = 0
+    for te in range(n):
+        scan = [cells[(px, py)] for py in range(int(cy[te]) - w, int(cy[te]) + w + 1)
+                for px in range(int(cx[te]) - w, int(cx[te]) + w + 1) if (px, py) in cells]
+        cand = np.concatenate(scan) if scan else np.zeros(0, np.int64)
+        cand = cand[cand != te]
+        dxs = x[te] - x[cand]
+        dys = y[te] - y[cand]
+        d = dxs * dxs + dys * dys  # float32 throughout
+        keep = ~(d > rad_sqr)
+        cand, d = cand[keep][:max_candidates], d[keep][:max_candidates]
+        order = np.argsort(d, kind="stable")
+        cand, d = cand[order], d[order]
+        if len(d) >= max_candidates:
+            truncated += 1
+        if len(d) > 1 and np.any(d[1:] == d[:-1]):
+            ties += 1
+        maxdeg = max(maxdeg, len(d))
+        ids_out.append(cand.astype(np.int32))
+        d2_out.append(d.astype(np.float64))
+        offs.append(offs[-1] + len(d))
+    return Csr(np.array(offs, np.int32), np.concatenate(ids_out) if ids_out else np.zeros(0, np.int32),
+               np.concatenate(d2_out) if d2_out else np.zeros(0), int(maxdeg), int(truncated), int(ties))
 
 
 def pair_bundle(te, le, use_ref=False, **params):

@@ -76,10 +76,16 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
 }  // extern "C"
 
 // run_curvelet<T> without the file I/O (main.cpp:20-96), for T = double and float.
+// With nb_offsets/nb_ids given, the neighbour lists that build_neighbor_csr_graph
+// made are replaced by those before the CurveletCPU stage runs (the graph's edge
+// table stays the reference's own): the reference's bundles, growth and record
+// code then run on a caller-chosen CSR, e.g. one whose truncated anchors keep the
+// lowest edge indices of a pixel cell.
 template <typename T>
 static int run_impl(const T *edges, int num_edges, int edge_data_sz, double nrad, double dx, double dt_deg,
                     double max_k, double sx, double st, unsigned group_max_sz, unsigned max_candidates, int nthreads,
-                    int quiet, int want_outputs, cvlref_out *out)
+                    int quiet, int want_outputs, cvlref_out *out, const int *nb_offsets = nullptr,
+                    const int *nb_ids = nullptr)
 {
     std::memset(out, 0, sizeof(*out));
     quiet_scope q(quiet != 0);
@@ -102,6 +108,29 @@ static int run_impl(const T *edges, int num_edges, int edge_data_sz, double nrad
         return -1;
     }
     out->ms_csr = ms_since(t0);
+    if (nb_offsets != nullptr) {
+        if (nb_offsets[0] != 0) return -3;
+        unsigned maxdeg = 0;
+        for (int a = 0; a < num_edges; ++a) {
+            const int d = nb_offsets[a + 1] - nb_offsets[a];
+            if (d < 0) return -3;
+            if ((unsigned)d > maxdeg) maxdeg = (unsigned)d;
+        }
+        const int np = nb_offsets[num_edges];
+        csr.neighbor_offsets.assign(nb_offsets, nb_offsets + num_edges + 1);
+        csr.neighbor_ids.assign(nb_ids, nb_ids + np);
+        csr.neighbor_dist2.assign((size_t)np, T(0));
+        for (int a = 0; a < num_edges; ++a) {
+            for (int k = nb_offsets[a]; k < nb_offsets[a + 1]; ++k) {
+                const int b = nb_ids[k];
+                if (b < 0 || b >= num_edges || b == a) return -3;
+                csr.neighbor_dist2[(size_t)k] = sq_dist<T>(toed[(size_t)a * sz], toed[(size_t)a * sz + 1],
+                                                           toed[(size_t)b * sz], toed[(size_t)b * sz + 1]);
+            }
+        }
+        csr.total_neighbor_pairs = np;
+        csr.max_num_of_neighbors = maxdeg;
+    }
 
     t0 = std::chrono::steady_clock::now();
     CurveletCPU<T> obj(edge_num, sz, csr, t_dx, t_dt, t_sx, t_st, t_max_k, group_max_sz, nthreads, toed.data(),
@@ -167,6 +196,27 @@ int cvlref_run_f32(const float *edges, int num_edges, int edge_data_sz,
 {
     return run_impl<float>(edges, num_edges, edge_data_sz, nrad, dx, dt_deg, max_k, sx, st, group_max_sz,
                            max_candidates, nthreads, quiet, want_outputs, out);
+}
+
+// The CurveletCPU stage of run_curvelet<double> / <float> on the given neighbour
+// lists (offsets [num_edges + 1], ids [offsets[num_edges]], input edge indices).
+// Returns -3 on lists that are not a CSR over the map's edges.
+int cvlref_run_csr(const double *edges, int num_edges, int edge_data_sz,
+                   double nrad, double dx, double dt_deg, double max_k,
+                   double sx, double st, unsigned group_max_sz, unsigned max_candidates,
+                   const int *nb_offsets, const int *nb_ids, cvlref_out *out)
+{
+    return run_impl<double>(edges, num_edges, edge_data_sz, nrad, dx, dt_deg, max_k, sx, st, group_max_sz,
+                            max_candidates, 1, 1, 1, out, nb_offsets, nb_ids);
+}
+
+int cvlref_run_csr_f32(const float *edges, int num_edges, int edge_data_sz,
+                       double nrad, double dx, double dt_deg, double max_k,
+                       double sx, double st, unsigned group_max_sz, unsigned max_candidates,
+                       const int *nb_offsets, const int *nb_ids, cvlref_out *out)
+{
+    return run_impl<float>(edges, num_edges, edge_data_sz, nrad, dx, dt_deg, max_k, sx, st, group_max_sz,
+                           max_candidates, 1, 1, 1, out, nb_offsets, nb_ids);
 }
 
 void cvlref_free(cvlref_out *out)

@@ -38,6 +38,18 @@ def golden_pairs():
 
 
 @pytest.fixture(scope="session")
+def golden_trunc():
+    """tests/golden/truncated_lowest.npz: the reference's curvelet stage on the
+    lowest-index neighbour lists of maps with truncated anchors."""
+    return np.load(os.path.join(GOLDEN, "truncated_lowest.npz"))
+
+
+def truncated_cases(z):
+    """(case, scalar) pairs of truncated_lowest.npz."""
+    return sorted({tuple(k.split("/")[:2]) for k in z.files if not k.startswith("pin_f32/")})
+
+
+@pytest.fixture(scope="session")
 def engine():
     import curvelet_construction_on_gpu_b200 as cvl
     eng = cvl.Engine()

@@ -8,7 +8,9 @@ Rules (tests/parity.py): counts and chains identical, the info columns without
 a transcendental input bit-identical, the others within the float tolerance.
 The KAT blob150 truncates all 150 anchors at max_candidates, where the choice
 inside a pixel cell follows libstdc++'s unstable sort in the reference and the
-lowest edge ids here; its truncation-independent counts must agree."""
+lowest edge ids here: against the whole reference run its truncation-independent
+counts must agree, and against the reference's curvelet stage run on the
+lowest-index lists (tests/golden/truncated_lowest.npz) everything must."""
 import hashlib
 import os
 import subprocess
@@ -71,6 +73,22 @@ def test_float_sample_files(engine, g32, key):
         print(f"[float file] {key}: {st}")
     else:
         assert hashlib.sha256(np.ascontiguousarray(r.chains).tobytes()).hexdigest() == str(g32[f"{key}/digests"][0])
+
+
+@pytest.mark.parametrize("case", ["blob150", "blob600_mc128", "blob600_mc40"])
+def test_float_truncated_vs_reference_stage(engine, golden_trunc, case):
+    """Every anchor truncated: the float engine against the reference's
+    run_curvelet<float> curvelet stage on the same lowest-index float lists."""
+    k = f"{case}/float"
+    e = golden_trunc[f"{k}/edges"]
+    assert e.dtype == np.float32
+    gms, mc = golden_trunc[f"{k}/params"].tolist()
+    r = engine.run(e, cvl.CurveletParams(group_max_sz=gms, max_candidates=mc, edge_data_sz=e.shape[1]),
+                   scalar="float")
+    assert _counts(r) + [r.truncated_anchors] == golden_trunc[f"{k}/counts"].tolist()
+    st = assert_same_curvelets(r, _Ref(golden_trunc[f"{k}/chains"], golden_trunc[f"{k}/info"]),
+                               label=case + " f32 vs reference stage", scalar="float")
+    print(f"[float truncated] {case}: {st}")
 
 
 def test_float_input_checks(engine):

@@ -203,6 +203,21 @@ def test_group_max_sz_range(engine, oracle, gms):
     assert_same_curvelets(r, o, label=f"gms={gms}")
 
 
+@pytest.mark.parametrize("case", ["blob150", "blob600_mc128", "blob600_mc40"])
+def test_truncated_vs_reference_stage(engine, golden_trunc, case):
+    """Every anchor truncated at max_candidates: the engine (lowest edge indices
+    inside a pixel cell) against the reference's own CurveletCPU stage run on the
+    same lowest-index neighbour lists (tests/golden/make_golden_truncated.py)."""
+    k = f"{case}/double"
+    e = golden_trunc[f"{k}/edges"]
+    gms, mc = golden_trunc[f"{k}/params"].tolist()
+    r = engine.run(e, cvl.CurveletParams(group_max_sz=gms, max_candidates=mc, edge_data_sz=e.shape[1]))
+    assert [r.num_curvelets, r.valid_pairs, r.total_neighbor_pairs, r.max_num_of_neighbors,
+            r.truncated_anchors] == golden_trunc[f"{k}/counts"].tolist()
+    _report(f"truncated {case}", assert_same_curvelets(
+        r, _Ref(golden_trunc[f"{k}/chains"], golden_trunc[f"{k}/info"]), label=case + " vs reference stage"))
+
+
 def test_truncation_blob(engine, oracle):
     rng = np.random.Generator(np.random.PCG64(3))
     e = np.stack([50 + rng.uniform(-2, 2, 600), 50 + rng.uniform(-2, 2, 600), rng.uniform(-3, 3, 600),

@@ -104,3 +104,79 @@ def test_float_fixtures_reproduce_with_live_reference(oracle):
     r = oracle.ref_run(z["TO_edges_digit1/edges"], scalar="float")
     assert np.array_equal(r.chains, z["TO_edges_digit1/chains"])
     assert np.array_equal(r.info.view(np.uint64), z["TO_edges_digit1/info"].view(np.uint64))
+
+
+# ---- truncated anchors (max_candidates cuts inside a pixel cell)
+
+def _csr_digest(offsets, ids, dist2=None):
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(offsets, dtype=np.int32).tobytes())
+    h.update(np.ascontiguousarray(ids, dtype=np.int32).tobytes())
+    if dist2 is not None:
+        h.update(np.ascontiguousarray(dist2, dtype=np.float32).tobytes())
+    return h.hexdigest()
+
+
+def test_restatement_truncated_matches_reference_stage(oracle, golden_trunc):
+    """On maps where every anchor is truncated, the C restatement equals, bit for
+    bit, the reference's own CurveletCPU stage run on the same lowest-index
+    neighbour lists (tests/golden/make_golden_truncated.py)."""
+    from tests.conftest import truncated_cases
+    cases = [c for c, s in truncated_cases(golden_trunc) if s == "double"]
+    assert len(cases) == 3
+    for case in cases:
+        k = f"{case}/double"
+        e = golden_trunc[f"{k}/edges"]
+        gms, mc = golden_trunc[f"{k}/params"].tolist()
+        csr = oracle.build_csr(e, max_candidates=mc)
+        assert _csr_digest(csr.offsets, csr.ids) == str(golden_trunc[f"{k}/csr_sha256"]), case
+        o = oracle.run(e, group_max_sz=gms, max_candidates=mc)
+        assert [o.chains.shape[0], o.valid_pairs, o.total_neighbor_pairs, o.max_num_of_neighbors,
+                o.truncated_anchors] == golden_trunc[f"{k}/counts"].tolist(), case
+        assert np.array_equal(o.chains, golden_trunc[f"{k}/chains"]), case
+        assert np.array_equal(o.info.view(np.uint64), golden_trunc[f"{k}/info"].view(np.uint64)), case
+
+
+def test_float_csr_restatement_pinned(oracle, golden_trunc):
+    """oracle.build_csr_f32 (run_curvelet<float>'s neighbour lists) equals the
+    reference's own float CSR, distances included, on every map without a
+    truncated anchor, and gives the lists the float truncation fixtures used."""
+    import os
+    from tests.conftest import truncated_cases
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_files_f32.npz"))
+    pins = sorted({k.split("/")[1] for k in golden_trunc.files if k.startswith("pin_f32/")})
+    assert len(pins) == 9
+    for name in pins:
+        key = name if name.startswith("TO_edges") else f"kat/{name}"
+        mc = int(z[f"{key}/params"][1]) if f"{key}/params" in z.files else 128
+        c = oracle.build_csr_f32(z[f"{key}/edges"], max_candidates=mc)
+        assert c.truncated_anchors == 0, name
+        assert _csr_digest(c.offsets, c.ids, c.dist2) == str(golden_trunc[f"pin_f32/{name}/csr_sha256"]), name
+    for case in [c for c, s in truncated_cases(golden_trunc) if s == "float"]:
+        k = f"{case}/float"
+        mc = int(golden_trunc[f"{k}/params"][1])
+        c = oracle.build_csr_f32(golden_trunc[f"{k}/edges"], max_candidates=mc)
+        assert c.truncated_anchors == int(golden_trunc[f"{k}/counts"][4]) > 0, case
+        assert _csr_digest(c.offsets, c.ids) == str(golden_trunc[f"{k}/csr_sha256"]), case
+
+
+def test_truncated_fixtures_reproduce_with_live_reference(oracle, golden_trunc):
+    """Where the harness is built: the reference stage on the lowest-index lists
+    gives the fixtures' bits again, and on the reference's own lists it gives
+    what the whole reference run gives (the list override changes nothing else)."""
+    if not oracle.ref_available():
+        pytest.skip("reference harness not built here")
+    from tests.conftest import truncated_cases
+    for case, scalar in truncated_cases(golden_trunc):
+        k = f"{case}/{scalar}"
+        e = golden_trunc[f"{k}/edges"]
+        gms, mc = golden_trunc[f"{k}/params"].tolist()
+        c = oracle.build_csr_f32(e, max_candidates=mc) if scalar == "float" else oracle.build_csr(e, max_candidates=mc)
+        r = oracle.ref_run_csr(e, c.offsets, c.ids, scalar=scalar, group_max_sz=gms, max_candidates=mc)
+        assert np.array_equal(r.chains, golden_trunc[f"{k}/chains"]), k
+        assert np.array_equal(r.info.view(np.uint64), golden_trunc[f"{k}/info"].view(np.uint64)), k
+        full = oracle.ref_run(e, scalar=scalar, group_max_sz=gms, max_candidates=mc)
+        own = oracle.ref_run_csr(e, full.csr.offsets, full.csr.ids, scalar=scalar, group_max_sz=gms,
+                                 max_candidates=mc)
+        assert np.array_equal(own.chains, full.chains) and own.valid_pairs == full.valid_pairs, k
+        assert np.array_equal(own.info.view(np.uint64), full.info.view(np.uint64)), k
