@@ -245,6 +245,14 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                     }
                 } else {
                 const double tt2 = 2.0 * tt;
+                // The k_dt bounds: branch 1 takes its lower one from s_m and its upper
+                // one from s_p, branch 2 the other way round (:731-744, :787-800). The
+                // branch is the pair's, so the operand triples are chosen once here.
+                const double s_lo = g2.branch1 ? s_m : s_p, s_hi = g2.branch1 ? s_p : s_m;
+                const double c_lo = g2.branch1 ? g2.cos_m_DX : g2.cos_p_DX;
+                const double c_hi = g2.branch1 ? g2.cos_p_DX : g2.cos_m_DX;
+                const double n_lo = g2.branch1 ? g2.sin_m_DY : g2.sin_p_DY;
+                const double n_hi = g2.branch1 ? g2.sin_p_DY : g2.sin_m_DY;
 #pragma unroll 1  // (measured: unrolling by 2 spills under the 64-register cap and is 2.6% slower)
                 for (int i = 0; i < md.P; ++i) {
                     const double delta_x2 = s_dx2[i], dx2_2 = s_dx2_2[i];
@@ -253,13 +261,11 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                     const double e1 = (((g2.DX2 - dx2_2 * tt) + g2.DY2) - md.dx2) + s_dx2sq[i];
                     const double k_dx_min = lo2 / e1;
                     const double k_dx_max = hi2 / e1;
-                    const double km = s_m / (-s_m * delta_x2 + g2.cos_m_DX + g2.sin_m_DY);
-                    const double kp = s_p / (-s_p * delta_x2 + g2.cos_p_DX + g2.sin_p_DY);
                     double bmin = -md.max_k, bmax = md.max_k;
                     if (bmin < k_dx_min) bmin = k_dx_min;
                     if (bmax > k_dx_max) bmax = k_dx_max;
-                    const double k2min = g2.branch1 ? km : kp;
-                    const double k2max = g2.branch1 ? kp : km;
+                    const double k2min = s_lo / (-s_lo * delta_x2 + c_lo + n_lo);
+                    const double k2max = s_hi / (-s_hi * delta_x2 + c_hi + n_hi);
                     if (bmin < k2min) bmin = k2min;
                     if (bmax > k2max) bmax = k2max;
                     open = open || (bmax > bmin);
