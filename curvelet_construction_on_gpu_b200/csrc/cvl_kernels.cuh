@@ -457,8 +457,12 @@ __device__ __forceinline__ unsigned direction_class(T ax, T ay, T lx, T ly, T co
     return (d > 0) ? 0u : ((d < 0) ? 1u : 2u);
 }
 
+// The parameter is a __grid_constant__: gather_truncated (not inlined) takes
+// references to its model and binned arrays, and a plain by-value parameter would
+// be copied to every thread's local stack for that (~300 bytes per thread, stored
+// in the prologue of every launch whether or not any anchor is truncated).
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_nb(NbArgsT<T> a) {
+__global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a) {
     extern __shared__ __align__(16) unsigned char nb_smem[];
     __shared__ BlockStats bstats;
     const ModelT<T> &md = a.md;
