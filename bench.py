@@ -52,16 +52,16 @@ METRIC = "edges/s"
 # per computed (non-close) pair: 63 cells x 20 FP64 flops, divisions counted as 1
 FLOPS_PER_PAIR_CELL = 20
 # DRAM bytes of k_bundles per computed pair, from one ncu capture of the kernel
-# (--set full) on the 242k-edge 1920x1080 map: dram__bytes_read.sum 0.334855 GB +
-# dram__bytes_write.sum 2.185202 GB over 2,176,780 non-close pairs. The traffic is
+# (--set full) on the 242k-edge 1920x1080 map: dram__bytes_read.sum 0.334940 GB +
+# dram__bytes_write.sum 2.183544 GB over 2,176,780 non-close pairs. The traffic is
 # the bundle write (1,008 B per pair) plus the pair/anchor reads, so it scales with
 # the pairs a launch processes.
-BUNDLE_DRAM_BYTES_PER_PAIR = (0.334855e9 + 2.185202e9) / 2_176_780
+BUNDLE_DRAM_BYTES_PER_PAIR = (0.334940e9 + 2.183544e9) / 2_176_780
 # FP64-pipe instructions of k_bundles per cell, from the same capture: the pipe was
-# active 49.02% of 0.999232 ms on 148 SMs (each issues 2 FP64 warp-instructions a
-# cycle at 1.965 GHz), 30.59 active lanes per warp-instruction, 2,176,780 x 63 cells.
+# active 48.72% of 0.952480 ms on 148 SMs (each issues 2 FP64 warp-instructions a
+# cycle at 1.965 GHz), 30.57 active lanes per warp-instruction, 2,176,780 x 63 cells.
 # A division costs about 10 of them, which the algorithmic count above takes as 1 flop.
-BUNDLE_FP64_INSTR_PER_CELL = 0.4902 * 0.999232e-3 * 148 * 2 * 1.965e9 * 30.59 / (2_176_780 * 63)
+BUNDLE_FP64_INSTR_PER_CELL = 0.4872 * 0.952480e-3 * 148 * 2 * 1.965e9 * 30.57 / (2_176_780 * 63)
 
 
 def _args():
