@@ -429,6 +429,27 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
             "admission": "40 GiB budget, 2048 B per edge", "pool": f"{len(maps)} seeded maps"}
 
 
+def _measured_peaks() -> dict:
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def path_hbm(n_edges: int, n_curv: int, ms_per_step: float, peaks: dict, edge_bytes: int = 32) -> dict:
+    """The whole path against the HBM roofline, per GPU: the algorithmic bytes of a
+    step are the edges in (4 FP64 values, 32 B per edge) and the curvelets out (a
+    5-column uint32 chain row and 10 FP64 info values, 100 B per curvelet)."""
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    b = float(edge_bytes) * n_edges + 100.0 * n_curv
+    achieved = b / (ms_per_step / 1e3) / 1e9 if ms_per_step > 0 else 0.0
+    return {"bound": "hbm", "scope": "whole path, per GPU", "bytes_per_step": b, "achieved": achieved,
+            "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+            "work": f"{edge_bytes} B per edge in + 100 B per curvelet out",
+            "note": "the path is bound by its FP64 bundle transport and by latency, not by HBM"}
+
+
 def run_ours(args, maps, cfg, world, rank, local, pg):
     import curvelet_construction_on_gpu_b200 as cvl
     eng = cvl.Engine(device=local)
@@ -548,6 +569,8 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
                                   / (fp64_peak * 1e12 / 2.0)) if (fp64_peak and curv_ms > 0) else None,
                          "note": "FP64-pipe instructions per cell from ncu, scaled to this run's k_bundles time, "
                                  "against the DFMA issue peak (measured TFLOP/s / 2)"}},
+        "path_hbm": path_hbm(n_edges, n_curv, sum_ms / args.steps, _measured_peaks(),
+                             edge_bytes=8 * int(maps[0].shape[1])),
         "gpu_launches": launches,
         "clocks": clocks,
         "e2e": e2e,
@@ -616,11 +639,7 @@ def run_contours(args, maps, cfg, world, rank, local, pg):
     if rank != 0:
         eng.close()
         return
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
+    peaks = _measured_peaks()
     hbm = peaks.get("hbm_gbs") or 6650.0
     cms = float(np.mean([k.get("contours", 0.0) for k in stage_ms]))
     alg = _contour_algorithmic_bytes(n_curv, width, c)
