@@ -238,6 +238,7 @@ def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
     edges = 0
     secs = 0.0
     used = 0
+    phases = {"csr": 0.0, "pairwise": 0.0, "greedy": 0.0}
     cand, _ = _ref_sample(maps, 1 << 62)
     for m in cand:
         if m.shape[0] > 600_000:  # keep the sample within the time budget
@@ -246,6 +247,8 @@ def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
         if kind == "reference":
             r = O.ref_run(m, nthreads=threads, want_outputs=False)
             dt = (r.ms["csr"] + r.ms["pairwise"] + r.ms["greedy"]) / 1e3
+            for k in phases:
+                phases[k] += r.ms[k]
         else:
             O.run(m, nthreads=threads)
             dt = time.perf_counter() - t0
@@ -258,6 +261,10 @@ def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
            "sample": f"{used} of {len(maps)} map(s) (whole maps of at most 600k edges, in workload order), "
                      f"{edges} edges, timed as the reference's own CSR + form_pairwise_bundles + "
                      f"build_curvelets_greedy phases (file I/O excluded)"}
+    if kind == "reference":
+        # the reference's three timed phases over the sample (main.cpp:43-66), and the
+        # CSR + greedy subtotal
+        out["phases_ms"] = dict(phases, csr_plus_greedy=phases["csr"] + phases["greedy"])
     # the same on one thread (--nthreads 1), on the first map of the sample
     if kind == "reference" and cand:
         m = min(cand, key=lambda x: abs(x.shape[0] - 60_000))
