@@ -130,6 +130,16 @@ class _Clocks:
                  "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # a timed region shorter than the sampling interval would otherwise end before
+        # the sampler's first row: wait (at most 3 s) until it has written one
+        t0 = time.perf_counter()
+        while self.proc is not None and self.proc.poll() is None and time.perf_counter() - t0 < 3.0:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):
