@@ -142,7 +142,9 @@ __device__ __forceinline__ void cell_tables_init(const ModelT<T> &md, T *dx2, un
 // scaling by 2 is exact without overflow or underflow):
 //   e1  = (((DX2 - (2 dx2) tt) + DY2) - dx^2) + dx2^2          (branch 1's eq, :706)
 //   branch 2's eq (:770) is -(-e1)/2 = e1 * 0.5 exactly, so its
-//   (ttmdx2 -+ dx) / eq == (2 (ttmdx2 -+ dx)) / e1, branch 1's k_dx (:707-708);
+//   (ttmdx2 -+ dx) / eq == (2 (ttmdx2 -+ dx)) / e1, branch 1's k_dx (:707-708),
+//   except where e1 cancels to +0: x - x is +0 in both sums, so branch 2's eq
+//   is -0 there and its k_dx are the negated quotients;
 //   2 (ttmdx2 -+ dx) = (2 tt - 2 dx2) -+ 2 dx exactly.
 // Only the k_dt clamp order differs between the branches.
 //
@@ -259,8 +261,15 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                     const double ttmdx2_2 = tt2 - dx2_2;                         // 2 ttmdx2
                     const double lo2 = ttmdx2_2 - dx_2, hi2 = ttmdx2_2 + dx_2;  // 2 (ttmdx2 -+ dx)
                     const double e1 = (((g2.DX2 - dx2_2 * tt) + g2.DY2) - md.dx2) + s_dx2sq[i];
-                    const double k_dx_min = lo2 / e1;
-                    const double k_dx_max = hi2 / e1;
+                    double k_dx_min = lo2 / e1;
+                    double k_dx_max = hi2 / e1;
+                    // The one value where branch 2's eq is not e1 * 0.5: when e1 cancels to
+                    // +0, branch 2's sum cancels to +0 as well and its eq is -(+0) / 2 = -0,
+                    // so its k_dx are the infinities of the other sign (0 / 0 stays NaN).
+                    if (e1 == 0.0 && !g2.branch1) {
+                        k_dx_min = -k_dx_min;
+                        k_dx_max = -k_dx_max;
+                    }
                     double bmin = -md.max_k, bmax = md.max_k;
                     if (bmin < k_dx_min) bmin = k_dx_min;
                     if (bmax > k_dx_max) bmax = k_dx_max;
