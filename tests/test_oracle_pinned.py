@@ -180,3 +180,30 @@ def test_truncated_fixtures_reproduce_with_live_reference(oracle, golden_trunc):
                                  max_candidates=mc)
         assert np.array_equal(own.chains, full.chains) and own.valid_pairs == full.valid_pairs, k
         assert np.array_equal(own.info.view(np.uint64), full.info.view(np.uint64)), k
+
+
+def test_reference_stage_rejects_malformed_lists(oracle, golden_trunc):
+    """cvlref_run_csr refuses lists that are not a CSR over the map's edges: a
+    first offset other than 0, a decreasing offset, an id out of range, a self pair."""
+    if not oracle.ref_available():
+        pytest.skip("reference harness not built here")
+    e = golden_trunc["blob150/double/edges"]
+    c = oracle.build_csr(e)
+    bad = []
+    off = c.offsets.copy()
+    off[0] = 1
+    bad.append((off, c.ids))
+    off = c.offsets.copy()
+    off[5] = off[4] - 1
+    bad.append((off, c.ids))
+    ids = c.ids.copy()
+    ids[3] = e.shape[0]
+    bad.append((c.offsets, ids))
+    ids = c.ids.copy()
+    ids[c.offsets[7]] = 7
+    bad.append((c.offsets, ids))
+    for o, i in bad:
+        with pytest.raises(ValueError):
+            oracle.ref_run_csr(e, o, i)
+    # and the untouched lists run
+    assert oracle.ref_run_csr(e, c.offsets, c.ids).chains.shape[0] == int(golden_trunc["blob150/double/counts"][0])
