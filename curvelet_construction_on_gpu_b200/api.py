@@ -392,10 +392,15 @@ class Engine:
         finally:
             self._lib.cvl_result_free(r)
 
-    def pair_bundles(self, pairs, params: CurveletParams | None = None, dt_rad: float = 0.0):
+    def pair_bundles(self, pairs, params: CurveletParams | None = None, dt_rad: float = 0.0,
+                     literal: bool = False):
         """Bundles of independent (anchor, neighbour) pairs, rows (te_x, te_y, te_theta, le_x, le_y, le_theta).
-        Returns (bmin [n, cells], bmax [n, cells], valid [n] bool)."""
+        Returns (bmin [n, cells], bmax [n, cells], valid [n] bool). literal=True runs the
+        checking entry point cvl_check_pair_bundles_literal (the reference's two branches
+        as written, on the same device trig values)."""
         params = params or CurveletParams()
+        fn = self._lib.cvl_check_pair_bundles_literal if literal else self._lib.cvl_pair_bundles
+        name = "cvl_check_pair_bundles_literal" if literal else "cvl_pair_bundles"
         q = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1, 6)
         n = q.shape[0]
         p = params.to_c(dt_rad)
@@ -405,18 +410,35 @@ class Engine:
         bmax = np.zeros((max(n, 1), cap))
         valid = np.zeros(max(n, 1), np.uint8)
         # first call sizes the grid
-        check(self._lib.cvl_pair_bundles(self._h, q.ctypes.data_as(_abi._dp), 0, C.byref(p),
-                                         bmin.ctypes.data_as(_abi._dp), bmax.ctypes.data_as(_abi._dp),
-                                         valid.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(cells)),
-              "cvl_pair_bundles")
+        check(fn(self._h, q.ctypes.data_as(_abi._dp), 0, C.byref(p), bmin.ctypes.data_as(_abi._dp),
+                 bmax.ctypes.data_as(_abi._dp), valid.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(cells)), name)
         nc = cells.value
         bmin = np.zeros((max(n, 1), nc))
         bmax = np.zeros((max(n, 1), nc))
-        check(self._lib.cvl_pair_bundles(self._h, q.ctypes.data_as(_abi._dp), n, C.byref(p),
-                                         bmin.ctypes.data_as(_abi._dp), bmax.ctypes.data_as(_abi._dp),
-                                         valid.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(cells)),
-              "cvl_pair_bundles")
+        check(fn(self._h, q.ctypes.data_as(_abi._dp), n, C.byref(p), bmin.ctypes.data_as(_abi._dp),
+                 bmax.ctypes.data_as(_abi._dp), valid.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(cells)), name)
         return bmin[:n], bmax[:n], valid[:n].astype(bool)
+
+    def transport_cells(self, ops, params: CurveletParams | None = None, dt_rad: float = 0.0):
+        """cvl_check_transport_cells: one orientation column of the transport per row of
+        ops [n, 10] = (DX, DY, tt, s_m, s_p, cos_m, sin_m, cos_p, sin_p, branch1).
+        Returns (rewrite_min, rewrite_max, literal_min, literal_max), each [n, P]."""
+        params = params or CurveletParams()
+        q = np.ascontiguousarray(ops, dtype=np.float64).reshape(-1, 10)
+        n = q.shape[0]
+        p = params.to_c(dt_rad)
+        rows = C.c_int32(0)
+        one = np.zeros(1)
+        check(self._lib.cvl_check_transport_cells(self._h, q.ctypes.data_as(_abi._dp), 0, C.byref(p),
+                                                  one.ctypes.data_as(_abi._dp), C.byref(rows)),
+              "cvl_check_transport_cells")
+        P = rows.value
+        out = np.zeros((max(n, 1), 4, P))
+        check(self._lib.cvl_check_transport_cells(self._h, q.ctypes.data_as(_abi._dp), n, C.byref(p),
+                                                  out.ctypes.data_as(_abi._dp), C.byref(rows)),
+              "cvl_check_transport_cells")
+        out = out[:n]
+        return out[:, 0], out[:, 1], out[:, 2], out[:, 3]
 
     # ---- batches
     def upload_batch(self, maps: list) -> "Batch":

@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/cvl.h"
 #include "cvl_internal.h"
 #include "cvl_pinned.h"
@@ -1151,8 +1153,12 @@ int cvl_build_curvelets(cvl_engine *e, const cvl_graph *g, const cvl_params *p, 
     return CVL_OK;
 }
 
-int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p, double *bmin, double *bmax,
-                     uint8_t *valid, int32_t *cells) {
+namespace {
+
+// Pairs through k_pair_bundles on the engine's stream (form 0: the production
+// transport; form 1: the reference's two branches as written).
+int pair_bundles_form(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p, int form, double *bmin,
+                      double *bmax, uint8_t *valid, int32_t *cells) {
     if (!e || !pairs || !bmin || !bmax || !valid || !cells || n < 0) return fail(CVL_EINVAL, "invalid argument");
     CVL_CUDA(cudaSetDevice(e->device));
     Model md;
@@ -1167,12 +1173,46 @@ int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_pa
     cudaStream_t s = e->stream;
     CVL_CUDA(cudaMemcpyAsync(e->pairs_in.p, pairs, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
     const int blocks = grid_for(e, n, 4, 16);
-    k_pair_bundles<<<blocks, 128, 0, s>>>(md, (const double *)e->pairs_in.p, n, (double *)e->pb_min.p,
-                                          (double *)e->pb_max.p, (unsigned char *)e->pb_valid.p);
+    k_pair_bundles<<<blocks, 128, 0, s>>>(md, (const double *)e->pairs_in.p, n, form, (double *)e->pb_min.p,
+                                          (double *)e->pb_max.p, (unsigned char *)e->pb_valid.p, nullptr);
     CVL_TRY(check_launch("k_pair_bundles"));
     CVL_CUDA(cudaMemcpyAsync(bmin, e->pb_min.p, sizeof(double) * (size_t)n * md.cells, cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaMemcpyAsync(bmax, e->pb_max.p, sizeof(double) * (size_t)n * md.cells, cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaMemcpyAsync(valid, e->pb_valid.p, (size_t)n, cudaMemcpyDeviceToHost, s));
+    CVL_CUDA(cudaStreamSynchronize(s));
+    return CVL_OK;
+}
+
+}  // namespace
+
+int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p, double *bmin, double *bmax,
+                     uint8_t *valid, int32_t *cells) {
+    return pair_bundles_form(e, pairs, n, p, 0, bmin, bmax, valid, cells);
+}
+
+int cvl_check_pair_bundles_literal(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p, double *bmin,
+                                   double *bmax, uint8_t *valid, int32_t *cells) {
+    return pair_bundles_form(e, pairs, n, p, 1, bmin, bmax, valid, cells);
+}
+
+int cvl_check_transport_cells(cvl_engine *e, const double *ops, int32_t n, const cvl_params *p, double *out,
+                              int32_t *rows) {
+    if (!e || !ops || !out || !rows || n < 0) return fail(CVL_EINVAL, "invalid argument");
+    CVL_CUDA(cudaSetDevice(e->device));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? std::max(p->max_candidates, 1u) : 1u, md, cpl));
+    *rows = md.P;
+    if (n == 0) return CVL_OK;
+    const size_t out_n = (size_t)n * 4 * md.P;
+    CVL_TRY(e->alloc(e->pairs_in, sizeof(double) * 10 * (size_t)n));
+    CVL_TRY(e->alloc(e->pb_min, sizeof(double) * out_n));
+    cudaStream_t s = e->stream;
+    CVL_CUDA(cudaMemcpyAsync(e->pairs_in.p, ops, sizeof(double) * 10 * (size_t)n, cudaMemcpyHostToDevice, s));
+    k_transport_cells<<<grid_for(e, n, 128, 8), 128, 0, s>>>(md, (const double *)e->pairs_in.p, n,
+                                                             (double *)e->pb_min.p);
+    CVL_TRY(check_launch("k_transport_cells"));
+    CVL_CUDA(cudaMemcpyAsync(out, e->pb_min.p, sizeof(double) * out_n, cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaStreamSynchronize(s));
     return CVL_OK;
 }
@@ -1601,7 +1641,6 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[CVL_NOALLOC_SCRATCH_BY
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
-unsigned char *g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
 
 inline size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -1609,69 +1648,54 @@ size_t noalloc_bytes(size_t n, size_t cells) {
     return 256 + round256(48 * n) + 2 * round256(8 * n * cells) + round256(n);
 }
 
-// k_pair_bundles with the valid pairs counted: warp per pair, one atomic per
-// valid pair into the scratch counter.
-__global__ void __launch_bounds__(128) k_pair_bundles_counted(Model md, const double *__restrict__ pairs, int n,
-                                                              double *__restrict__ bmin_out,
-                                                              double *__restrict__ bmax_out,
-                                                              unsigned char *__restrict__ valid_out,
-                                                              unsigned *__restrict__ valid_count) {
-    __shared__ double tab[4][4 * QMAX];
-    __shared__ double cell_dx2[CELLS_MAX];
-    __shared__ unsigned char cell_j[CELLS_MAX];
-    __shared__ unsigned short cell_rank[CELLS_MAX];
-    cell_tables_init(md, cell_dx2, cell_j, cell_rank);
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *sT = tab[wib], *cT = sT + QMAX, *sM = cT + QMAX, *sP = sM + QMAX;
-    for (int p = blockIdx.x * 4 + wib; p < n; p += gridDim.x * 4) {
-        const double *q = pairs + (size_t)p * 6;
-        const double te_x = q[0], te_y = q[1], T2 = q[2], le_x = q[3], le_y = q[4], T0 = q[5];
-        for (int j = lane; j < md.Q; j += 32) {
-            const double t = T2 + md.st * ((double)j - ((double)md.Q - 1.0) / 2.0);
-            sT[j] = sin(t);
-            cT[j] = cos(t);
-            sM[j] = sin(t - (T0 - md.dt));
-            sP[j] = sin(t - (T0 + md.dt));
-        }
-        __syncwarp();
-        const double t_p = T0 + md.dt, t_m = T0 - md.dt;
-        const PairGeom g = pair_geom(md, te_x, te_y, cos(T2), sin(T2), le_x, le_y, sin(t_p), cos(t_p), sin(t_m),
-                                     cos(t_m));
-        bool lv = false;
-        for (int c = lane; c < md.cells; c += 32) {
-            double bmin = -md.max_k, bmax = md.max_k;
-            if (!g.close) {
-                const int jj = cell_j[c];
-                const double tt = sT[jj] * g.DX - cT[jj] * g.DY;
-                bundle_cell_tt(md, g.DX2, g.DY2, g.sin_p_DY, g.cos_p_DX, g.sin_m_DY, g.cos_m_DX, g.branch1,
-                               cell_dx2[c], tt, sM[jj], sP[jj], bmin, bmax);
-            }
-            lv = lv || (bmax > bmin);
-            bmin_out[(size_t)p * md.cells + c] = bmin;
-            bmax_out[(size_t)p * md.cells + c] = bmax;
-        }
-        const bool valid = g.close ? true : (bool)__any_sync(FULL, lv);
-        if (lane == 0) {
-            valid_out[p] = valid ? 1 : 0;
-            if (valid) atomicAdd(valid_count, 1u);
-        }
-        __syncwarp();
+// The set-up of a device: the scratch's device address, looked up with that
+// device current. The address belongs to the device's current context, so it is
+// kept with that context's id (cuCtxGetId): after a context is destroyed and
+// created again (cudaDeviceReset, for one), the module is loaded again, the array
+// can land elsewhere, and the next call does the set-up again.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+struct NoallocSetup {
+    unsigned long long ctx_id = 0;  // 0: not set up
+    unsigned char *base = nullptr;
+};
+NoallocSetup g_noalloc_setup[NOALLOC_MAX_DEVICES];
+
+int current_context_id(unsigned long long *id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *f0 = nullptr, *f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0{}, q1{};
+        CVL_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000, cudaEnableDefault, &q0));
+        CVL_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault, &q1));
+        if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return fail(CVL_ECUDA, "the driver does not provide cuCtxGetCurrent / cuCtxGetId");
+        get_current = (CtxGetCurrentFn)f0;
+        get_id = (CtxGetIdFn)f1;
     }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return fail(CVL_ECUDA, "no current CUDA context");
+    if (get_id(ctx, id) != CUDA_SUCCESS) return fail(CVL_ECUDA, "cuCtxGetId failed");
+    return CVL_OK;
 }
 
-// Set-up, once per device, with that device current: the scratch's address.
 int noalloc_scratch(int dev, unsigned char **out) {
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(CVL_EUNSUPPORTED, "device ordinal above 63");
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_base[dev]) {
+    unsigned long long id = 0;
+    CVL_TRY(current_context_id(&id));
+    NoallocSetup &su = g_noalloc_setup[dev];
+    if (su.ctx_id != id || !su.base) {
         void *ptr = nullptr;
         const cudaError_t ce = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (ce != cudaSuccess || !ptr)
             return fail(CVL_ECUDA, std::string("scratch address: ") + cudaGetErrorString(ce));
-        g_noalloc_base[dev] = (unsigned char *)ptr;
+        su.base = (unsigned char *)ptr;
+        su.ctx_id = id;
     }
-    *out = g_noalloc_base[dev];
+    *out = su.base;
     return CVL_OK;
 }
 
@@ -1704,6 +1728,13 @@ int cvl_pair_bundles_noalloc(const double *pairs, int32_t n, const cvl_params *p
         return fail(CVL_ENODEV, "no CUDA device");
     }
     CVL_CUDA(cudaGetDevice(&dev));
+    cudaStream_t s = cudaStreamPerThread;
+    // The call ends with a synchronisation of the calling thread's stream, which a
+    // capture in progress on that stream would not survive.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CVL_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(CVL_EINVAL, "cvl_pair_bundles_noalloc cannot run while the calling thread's stream is capturing");
     unsigned char *base = nullptr;
     CVL_TRY(noalloc_scratch(dev, &base));
     int sms = 0;
@@ -1716,13 +1747,12 @@ int cvl_pair_bundles_noalloc(const double *pairs, int32_t n, const cvl_params *p
     double *d_bmax = (double *)((unsigned char *)d_bmin + round256(8 * cells_n));
     unsigned char *d_valid = (unsigned char *)d_bmax + round256(8 * cells_n);
 
-    cudaStream_t s = cudaStreamPerThread;
     CVL_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned), s));
     CVL_CUDA(cudaMemcpyAsync(d_pairs, pairs, 48 * (size_t)n, cudaMemcpyHostToDevice, s));
     long long blocks = ((long long)n + 3) / 4;
     blocks = std::max(1LL, std::min(blocks, (long long)sms * 16));
-    k_pair_bundles_counted<<<(int)blocks, 128, 0, s>>>(md, d_pairs, n, d_bmin, d_bmax, d_valid, d_count);
-    CVL_TRY(check_launch("k_pair_bundles_counted"));
+    k_pair_bundles<<<(int)blocks, 128, 0, s>>>(md, d_pairs, n, 0, d_bmin, d_bmax, d_valid, d_count);
+    CVL_TRY(check_launch("k_pair_bundles"));
     CVL_CUDA(cudaMemcpyAsync(bmin, d_bmin, 8 * cells_n, cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaMemcpyAsync(bmax, d_bmax, 8 * cells_n, cudaMemcpyDeviceToHost, s));
     CVL_CUDA(cudaMemcpyAsync(valid, d_valid, (size_t)n, cudaMemcpyDeviceToHost, s));

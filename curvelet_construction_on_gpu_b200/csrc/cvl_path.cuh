@@ -87,6 +87,58 @@ __device__ __forceinline__ void bundle_cell_tt(const Model &md, double DX2, doub
     if (bmax > k2max) bmax = k2max;
 }
 
+// One (pair, j) column of the FP64 transport, cells (i, j) for i = 0 .. P-1, in
+// the rewritten form k_bundles runs (see the comment above k_bundles):
+//   e1   = (((DX2 - (2 dx2) tt) + DY2) - dx^2) + dx2^2     (branch 1's eq, :706)
+//   k_dx = ((2 tt - 2 dx2) -+ 2 dx) / e1                   (both branches)
+// with the two quotients negated in a branch-2 cell whose e1 is +0, and the
+// k_dt operand triples chosen once per pair. dx2[i], dx2_2[i] = 2 dx2[i] and
+// dx2sq[i] = dx2[i]^2 are the per-i constants; store(i, bmin, bmax) takes each
+// cell. Returns whether any cell of the column is open (bmax > bmin).
+// k_bundles and k_pair_bundles (form 0) both run this function.
+template <class Store>
+__device__ __forceinline__ bool bundle_column_fp64(const Model &md, const double *dx2, const double *dx2_2,
+                                                   const double *dx2sq, const PairGeom &g2, double tt, double s_m,
+                                                   double s_p, Store &&store) {
+    const double dx_2 = 2.0 * md.dx;
+    const double tt2 = 2.0 * tt;
+    // The k_dt bounds: branch 1 takes its lower one from s_m and its upper one from
+    // s_p, branch 2 the other way round (:731-744, :787-800). The branch is the
+    // pair's, so the operand triples are chosen once here.
+    const double s_lo = g2.branch1 ? s_m : s_p, s_hi = g2.branch1 ? s_p : s_m;
+    const double c_lo = g2.branch1 ? g2.cos_m_DX : g2.cos_p_DX;
+    const double c_hi = g2.branch1 ? g2.cos_p_DX : g2.cos_m_DX;
+    const double n_lo = g2.branch1 ? g2.sin_m_DY : g2.sin_p_DY;
+    const double n_hi = g2.branch1 ? g2.sin_p_DY : g2.sin_m_DY;
+    bool open = false;
+#pragma unroll 1  // (measured: unrolling by 2 spills under the 64-register cap and is 2.6% slower)
+    for (int i = 0; i < md.P; ++i) {
+        const double delta_x2 = dx2[i], d2_2 = dx2_2[i];
+        const double ttmdx2_2 = tt2 - d2_2;                          // 2 ttmdx2
+        const double lo2 = ttmdx2_2 - dx_2, hi2 = ttmdx2_2 + dx_2;  // 2 (ttmdx2 -+ dx)
+        const double e1 = (((g2.DX2 - d2_2 * tt) + g2.DY2) - md.dx2) + dx2sq[i];
+        double k_dx_min = lo2 / e1;
+        double k_dx_max = hi2 / e1;
+        // The one value where branch 2's eq is not e1 * 0.5: when e1 cancels to
+        // +0, branch 2's sum cancels to +0 as well and its eq is -(+0) / 2 = -0,
+        // so its k_dx are the infinities of the other sign (0 / 0 stays NaN).
+        if (e1 == 0.0 && !g2.branch1) {
+            k_dx_min = -k_dx_min;
+            k_dx_max = -k_dx_max;
+        }
+        double bmin = -md.max_k, bmax = md.max_k;
+        if (bmin < k_dx_min) bmin = k_dx_min;
+        if (bmax > k_dx_max) bmax = k_dx_max;
+        const double k2min = s_lo / (-s_lo * delta_x2 + c_lo + n_lo);
+        const double k2max = s_hi / (-s_hi * delta_x2 + c_hi + n_hi);
+        if (bmin < k2min) bmin = k2min;
+        if (bmax > k2max) bmax = k2max;
+        open = open || (bmax > bmin);
+        store(i, bmin, bmax);
+    }
+    return open;
+}
+
 // Cell constants: delta_x2 (:697), orientation index j, and the best-cell rank of
 // fill_curvelet_info (:202-219): cells with d < 100 ordered by (d, row-major index);
 // 0xffff = never eligible.
@@ -189,7 +241,6 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
     const int pl = t / md.Q, jl = t - pl * md.Q;
     const bool lane_on = pl < PPB;
     const T delta_t2 = grid_offset(md.st, jl, md.Q);  // :698
-    const T dx_2 = T(2) * md.dx;
     const int A2 = 2 * md.Q + 2;
     const unsigned long long np = a.p_end - a.p_begin;
     int it = 0;
@@ -246,41 +297,11 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                         dst[32 * CPL + i * md.Q + jl] = bmax;
                     }
                 } else {
-                const double tt2 = 2.0 * tt;
-                // The k_dt bounds: branch 1 takes its lower one from s_m and its upper
-                // one from s_p, branch 2 the other way round (:731-744, :787-800). The
-                // branch is the pair's, so the operand triples are chosen once here.
-                const double s_lo = g2.branch1 ? s_m : s_p, s_hi = g2.branch1 ? s_p : s_m;
-                const double c_lo = g2.branch1 ? g2.cos_m_DX : g2.cos_p_DX;
-                const double c_hi = g2.branch1 ? g2.cos_p_DX : g2.cos_m_DX;
-                const double n_lo = g2.branch1 ? g2.sin_m_DY : g2.sin_p_DY;
-                const double n_hi = g2.branch1 ? g2.sin_p_DY : g2.sin_m_DY;
-#pragma unroll 1  // (measured: unrolling by 2 spills under the 64-register cap and is 2.6% slower)
-                for (int i = 0; i < md.P; ++i) {
-                    const double delta_x2 = s_dx2[i], dx2_2 = s_dx2_2[i];
-                    const double ttmdx2_2 = tt2 - dx2_2;                         // 2 ttmdx2
-                    const double lo2 = ttmdx2_2 - dx_2, hi2 = ttmdx2_2 + dx_2;  // 2 (ttmdx2 -+ dx)
-                    const double e1 = (((g2.DX2 - dx2_2 * tt) + g2.DY2) - md.dx2) + s_dx2sq[i];
-                    double k_dx_min = lo2 / e1;
-                    double k_dx_max = hi2 / e1;
-                    // The one value where branch 2's eq is not e1 * 0.5: when e1 cancels to
-                    // +0, branch 2's sum cancels to +0 as well and its eq is -(+0) / 2 = -0,
-                    // so its k_dx are the infinities of the other sign (0 / 0 stays NaN).
-                    if (e1 == 0.0 && !g2.branch1) {
-                        k_dx_min = -k_dx_min;
-                        k_dx_max = -k_dx_max;
-                    }
-                    double bmin = -md.max_k, bmax = md.max_k;
-                    if (bmin < k_dx_min) bmin = k_dx_min;
-                    if (bmax > k_dx_max) bmax = k_dx_max;
-                    const double k2min = s_lo / (-s_lo * delta_x2 + c_lo + n_lo);
-                    const double k2max = s_hi / (-s_hi * delta_x2 + c_hi + n_hi);
-                    if (bmin < k2min) bmin = k2min;
-                    if (bmax > k2max) bmax = k2max;
-                    open = open || (bmax > bmin);
-                    dst[i * md.Q + jl] = bmin;
-                    dst[32 * CPL + i * md.Q + jl] = bmax;
-                }
+                    open = bundle_column_fp64(md, s_dx2, s_dx2_2, s_dx2sq, g2, tt, s_m, s_p,
+                                              [&](int i, double lo, double hi) {
+                                                  dst[i * md.Q + jl] = lo;
+                                                  dst[32 * CPL + i * md.Q + jl] = hi;
+                                              });
                 }
                 if (open) s_open[buf][pl] = 1;
             }
@@ -727,51 +748,115 @@ __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, in
 
 
 // ---------------------------------------------------------------------------
-// Standalone transport for independent pairs (cvl_pair_bundles): warp per pair,
-// the same bundle_cell as the fused kernel.
-// pairs[p] = (te_x, te_y, te_theta, le_x, le_y, le_theta)
+// Standalone transport for independent pairs (cvl_pair_bundles,
+// cvl_pair_bundles_noalloc): warp per pair, lane j < Q computes the column of
+// orientation sample j, as a k_bundles lane does.
+//   form 0: bundle_column_fp64, the arithmetic k_bundles runs;
+//   form 1: bundle_cell_tt, the reference's two branches as written, a check
+//           of form 0 on the same trig values.
+// pairs[p] = (te_x, te_y, te_theta, le_x, le_y, le_theta). valid_count, when
+// not null, gets one atomic per valid pair.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_pair_bundles(Model md, const double *__restrict__ pairs, int n,
+__global__ void __launch_bounds__(128) k_pair_bundles(Model md, const double *__restrict__ pairs, int n, int form,
                                                       double *__restrict__ bmin_out, double *__restrict__ bmax_out,
-                                                      unsigned char *__restrict__ valid_out) {
-    __shared__ double tab[4][4 * QMAX];
-    __shared__ double cell_dx2[CELLS_MAX];
-    __shared__ unsigned char cell_j[CELLS_MAX];
-    __shared__ unsigned short cell_rank[CELLS_MAX];
-    cell_tables_init(md, cell_dx2, cell_j, cell_rank);
+                                                      unsigned char *__restrict__ valid_out,
+                                                      unsigned *__restrict__ valid_count) {
+    __shared__ double s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
+    for (int i = threadIdx.x; i < md.P; i += blockDim.x) {
+        const double d = grid_offset(md.sx, i, md.P);  // delta_x2 (:697)
+        s_dx2[i] = d;
+        s_dx2_2[i] = 2.0 * d;
+        s_dx2sq[i] = d * d;
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *sT = tab[wib], *cT = sT + QMAX, *sM = cT + QMAX, *sP = sM + QMAX;
     for (int p = blockIdx.x * 4 + wib; p < n; p += gridDim.x * 4) {
         const double *q = pairs + (size_t)p * 6;
         const double te_x = q[0], te_y = q[1], T2 = q[2], le_x = q[3], le_y = q[4], T0 = q[5];
-        for (int j = lane; j < md.Q; j += 32) {
-            const double t = T2 + md.st * ((double)j - ((double)md.Q - 1.0) / 2.0);
-            sT[j] = sin(t);
-            cT[j] = cos(t);
-            sM[j] = sin(t - (T0 - md.dt));
-            sP[j] = sin(t - (T0 + md.dt));
-        }
-        __syncwarp();
         const double t_p = T0 + md.dt, t_m = T0 - md.dt;
         const PairGeom g = pair_geom(md, te_x, te_y, cos(T2), sin(T2), le_x, le_y, sin(t_p), cos(t_p), sin(t_m),
                                      cos(t_m));
         bool lv = false;
-        for (int c = lane; c < md.cells; c += 32) {
-            double bmin = -md.max_k, bmax = md.max_k;
-            if (!g.close) {
-                const int jj = cell_j[c];
-                const double tt = sT[jj] * g.DX - cT[jj] * g.DY;
-                bundle_cell_tt(md, g.DX2, g.DY2, g.sin_p_DY, g.cos_p_DX, g.sin_m_DY, g.cos_m_DX, g.branch1,
-                               cell_dx2[c], tt, sM[jj], sP[jj], bmin, bmax);
+        const int j = lane;
+        if (j < md.Q) {
+            double *omin = bmin_out + (size_t)p * md.cells;
+            double *omax = bmax_out + (size_t)p * md.cells;
+            auto store = [&](int i, double lo, double hi) {
+                omin[i * md.Q + j] = lo;
+                omax[i * md.Q + j] = hi;
+            };
+            if (g.close) {
+                // the default bundle (:682-687)
+                for (int i = 0; i < md.P; ++i) store(i, -md.max_k, md.max_k);
+            } else {
+                const double T2t = T2 + grid_offset(md.st, j, md.Q);  // :698-702
+                const double s_m = sin(T2t - (T0 - md.dt));           // :728
+                const double s_p = sin(T2t - (T0 + md.dt));           // :729
+                const double tt = sin(T2t) * g.DX - cos(T2t) * g.DY;  // :705
+                if (form == 0) {
+                    lv = bundle_column_fp64(md, s_dx2, s_dx2_2, s_dx2sq, g, tt, s_m, s_p, store);
+                } else {
+                    for (int i = 0; i < md.P; ++i) {
+                        double lo = -md.max_k, hi = md.max_k;
+                        bundle_cell_tt(md, g.DX2, g.DY2, g.sin_p_DY, g.cos_p_DX, g.sin_m_DY, g.cos_m_DX, g.branch1,
+                                       s_dx2[i], tt, s_m, s_p, lo, hi);
+                        lv = lv || (hi > lo);
+                        store(i, lo, hi);
+                    }
+                }
             }
-            lv = lv || (bmax > bmin);
-            bmin_out[(size_t)p * md.cells + c] = bmin;
-            bmax_out[(size_t)p * md.cells + c] = bmax;
         }
+        // bundle_valid_check (:821-830); a close pair is valid (:682-687)
         const bool valid = g.close ? true : (bool)__any_sync(FULL, lv);
-        if (lane == 0) valid_out[p] = valid ? 1 : 0;
+        if (lane == 0) {
+            valid_out[p] = valid ? 1 : 0;
+            if (valid && valid_count) atomicAdd(valid_count, 1u);
+        }
         __syncwarp();
+    }
+}
+
+// Checking kernel (cvl_check_transport_cells): the FP64 transport of one column
+// on operand sets given directly, so that cells built to cancel reach the device
+// code. ops[r] = (DX, DY, tt, s_m, s_p, cos_m, sin_m, cos_p, sin_p, branch1), with
+// cos/sin of T0 -+ dt as pair_geom takes them. out[r] = [form][bmin, bmax][P]:
+// bundle_column_fp64 (form 0, the production arithmetic) and bundle_cell_tt
+// (form 1, the reference's expressions as written). A thread per row.
+__global__ void k_transport_cells(Model md, const double *__restrict__ ops, int n, double *__restrict__ out) {
+    __shared__ double s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
+    for (int i = threadIdx.x; i < md.P; i += blockDim.x) {
+        const double d = grid_offset(md.sx, i, md.P);
+        s_dx2[i] = d;
+        s_dx2_2[i] = 2.0 * d;
+        s_dx2sq[i] = d * d;
+    }
+    __syncthreads();
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const double *o = ops + (size_t)r * 10;
+        PairGeom g;
+        g.DX = o[0];
+        g.DY = o[1];
+        g.DX2 = g.DX * g.DX;
+        g.DY2 = g.DY * g.DY;
+        g.cos_m_DX = g.DX * o[5];
+        g.sin_m_DY = g.DY * o[6];
+        g.cos_p_DX = g.DX * o[7];
+        g.sin_p_DY = g.DY * o[8];
+        g.close = false;
+        g.branch1 = o[9] != 0.0;
+        const double tt = o[2], s_m = o[3], s_p = o[4];
+        double *dst = out + (size_t)r * 4 * md.P;
+        bundle_column_fp64(md, s_dx2, s_dx2_2, s_dx2sq, g, tt, s_m, s_p, [&](int i, double lo, double hi) {
+            dst[i] = lo;
+            dst[md.P + i] = hi;
+        });
+        for (int i = 0; i < md.P; ++i) {
+            double lo = -md.max_k, hi = md.max_k;
+            bundle_cell_tt(md, g.DX2, g.DY2, g.sin_p_DY, g.cos_p_DX, g.sin_m_DY, g.cos_m_DX, g.branch1, s_dx2[i], tt,
+                           s_m, s_p, lo, hi);
+            dst[2 * md.P + i] = lo;
+            dst[3 * md.P + i] = hi;
+        }
     }
 }
 

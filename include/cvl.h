@@ -190,6 +190,25 @@ int cvl_build_curvelets(cvl_engine *e, const cvl_graph *g, const cvl_params *p, 
 int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p,
                      double *bmin, double *bmax, uint8_t *valid, int32_t *cells);
 
+/* ---- checking entry points ------------------------------------------- */
+/* No reference counterpart: they exist so that tests can reach the device code of
+ * the transport at chosen operands.
+ *
+ * cvl_check_pair_bundles_literal: cvl_pair_bundles through the reference's two
+ * branches as written (cpu_curvelet.hpp:693-809, one formula per branch) on the
+ * same device trig values, where cvl_pair_bundles runs the rewritten arithmetic of
+ * the path's bundle kernel. The two must agree bit for bit. */
+int cvl_check_pair_bundles_literal(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p,
+                                   double *bmin, double *bmax, uint8_t *valid, int32_t *cells);
+/* cvl_check_transport_cells: one orientation column (cells (i, j), i < P) of the
+ * transport per row of ops[n][10] = (DX, DY, tt, s_m, s_p, cos(T0 - dt),
+ * sin(T0 - dt), cos(T0 + dt), sin(T0 + dt), branch1 != 0), the operands of
+ * cpu_curvelet.hpp:693-809 given directly, so that cells built to cancel reach the
+ * device. out[n][4][P]: the path's rewritten arithmetic (bmin, then bmax), then
+ * the reference's two branches as written (bmin, bmax). *rows = P. */
+int cvl_check_transport_cells(cvl_engine *e, const double *ops, int32_t n, const cvl_params *p, double *out,
+                              int32_t *rows);
+
 /* ---- pair bundles without any allocation ------------------------------ */
 /* No reference counterpart. The same computation and outputs as
  * cvl_pair_bundles, plus the number of valid pairs (the count
@@ -211,12 +230,20 @@ int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_pa
  * 7 x 9 = 63-cell grid. Larger n returns CVL_EOVERFLOW and does no work; split
  * the pairs over several calls.
  *
+ * The scratch is part of the library's device code: every CUDA context in which
+ * the library's kernels are loaded holds its 16 MiB until the context ends,
+ * whether or not this entry point is ever called.
+ *
  * The first call on a device does the set-up (it looks up the scratch's
- * address with the device current). Make that call before any stream capture
- * on the device. Calls that overlap in time on one device, from several host
- * threads, share the scratch and race: serialise them. Each call clears its
- * valid-pair counter before use and returns after its results are in the
- * caller's host buffers. */
+ * address with the device current), and so does the first call after the
+ * device's context was destroyed and created again (cudaDeviceReset, for one):
+ * the address is kept with the id of the context it belongs to. Make the first
+ * call before any stream capture on the device. No call may be made while the
+ * calling thread's stream (cudaStreamPerThread) is capturing: the call
+ * synchronises that stream, so it returns CVL_EINVAL instead. Calls that overlap
+ * in time on one device, from several host threads, share the scratch and race:
+ * serialise them. Each call clears its valid-pair counter before use and returns
+ * after its results are in the caller's host buffers. */
 #define CVL_NOALLOC_SCRATCH_BYTES (16u << 20)
 int cvl_pair_bundles_noalloc(const double *pairs, int32_t n, const cvl_params *p, double *bmin, double *bmax,
                              uint8_t *valid, uint32_t *valid_pairs, int32_t *cells);
