@@ -103,7 +103,7 @@ struct cvl_engine {
     DBuf bx, by, bth, bsp, bcp, bsm, bcm, bcell, bmap;
     DBuf ncand, deg, pair_off, csr_ids, csr_d2, rec_ids, rec_k, rec_meta, count, out_off;
     DBuf chains, info, stats, err, work, scratch, scratch_chain, scratch_res, scan_tmp, flush, deg_orig, off_orig,
-        gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start, crank;
+        gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, pslot, chunk_start, crank;
     cvl_tuning tune[CVL_TUNING_BUCKETS];                   // per size bucket of the batch
     cvl_yield_fn yield_fn = nullptr;                       // called between chunks (serving)
     void *yield_ctx = nullptr;
@@ -209,7 +209,7 @@ struct cvl_engine {
         DBuf *all[] = {&edges, &map_off, &ehash, &bcount, &bstart, &bfill, &pos_of, &orig_of, &bx, &by, &bth, &bsp,
                        &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
                        &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
-                       &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
+                       &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &pslot, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
                        &pb_max, &pb_valid, &chains_alt, &info_alt};
         for (DBuf *b : all) {
             if (b->p) cudaFreeAsync(b->p, stream);
@@ -467,10 +467,11 @@ template <typename T, int CPL, int MINB>
 int launch_bundles(cvl_engine *e, BundleArgsT<T> &a, int blocks) {
     // one block per PPB pairs and no grid stride: short blocks, so that a
     // higher-priority stream's blocks get SMs as soon as any block ends
-    const long long ppb = BUNDLE_THREADS / a.md.Q;
+    constexpr int pair_bytes = 2 * 32 * CPL * (int)sizeof(T);
+    const long long ppb = bundles_pairs_per_block(a.md.Q, pair_bytes);
     const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
     blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
-    k_bundles<T, CPL, MINB><<<blocks, BUNDLE_THREADS, 0, e->stream>>>(a);
+    k_bundles<T, CPL, MINB><<<blocks, BUNDLE_THREADS, (size_t)ppb * pair_bytes, e->stream>>>(a);
     return check_launch("k_bundles");
 }
 
@@ -569,7 +570,7 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     CVL_TRY(e->alloc(e->out_off, sizeof(unsigned long long) * (n + 1)));
     CVL_TRY(e->alloc(e->stats, sizeof(MapStats) * M));
     CVL_TRY(e->alloc(e->err, sizeof(unsigned) * 4));
-    CVL_TRY(e->alloc(e->work, sizeof(unsigned long long) * 2));
+    CVL_TRY(e->alloc(e->work, sizeof(unsigned long long) * 4));  // arena counter, bundle slot counter
 
     BinnedT<R> B;
     B.x = (R *)e->bx.p;
@@ -590,7 +591,7 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     CVL_CUDA(cudaMemsetAsync(e->bfill.p, 0, sizeof(unsigned) * (T + 1), s));
     CVL_CUDA(cudaMemsetAsync(e->stats.p, 0, sizeof(MapStats) * M, s));
     CVL_CUDA(cudaMemsetAsync(e->err.p, 0, sizeof(unsigned) * 4, s));
-    CVL_CUDA(cudaMemsetAsync(e->work.p, 0, sizeof(unsigned long long) * 2, s));
+    CVL_CUDA(cudaMemsetAsync(e->work.p, 0, sizeof(unsigned long long) * 4, s));
 
     // ---- (a) binning
     const int gb = short_grid(n, 256);
@@ -685,7 +686,10 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     pick_kernels(cpl, tn, bf, gf);
     const size_t gsmem = (size_t)(GROWTH_THREADS / 32) * growth_smem_per_warp(md.max_cand, md.gms);
     const unsigned long long max_chunk_pairs = per_chunk + (unsigned long long)ro.max_deg + 1;
-    CVL_TRY(e->alloc(e->bund, sizeof(R) * 64 * (size_t)cpl * std::min<unsigned long long>(P + 1, max_chunk_pairs)));
+    const unsigned long long chunk_cap = std::min<unsigned long long>(P + 1, max_chunk_pairs);
+    CVL_TRY(e->alloc(e->bund, sizeof(R) * 64 * (size_t)cpl * chunk_cap));
+    CVL_TRY(e->alloc(e->pslot, sizeof(unsigned) * chunk_cap));
+    unsigned *slot_ctr = (unsigned *)((unsigned long long *)e->work.p + 2);
     const int bblocks = e->prop.multiProcessorCount * 8;
     const int gblocks = e->prop.multiProcessorCount * 8;
 
@@ -735,8 +739,13 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
             ba.pcls = (const unsigned char *)e->pcls.p;
             ba.atrig = (const R *)e->atrig.p;
             ba.bund = (R *)e->bund.p;
+            ba.pslot = (unsigned *)e->pslot.p;
+            ba.slot_ctr = slot_ctr;
             ba.pflag = (unsigned char *)e->pflag.p;
-            if (ba.p_end > ba.p_begin) CVL_TRY(bf(e, ba, bblocks));
+            if (ba.p_end > ba.p_begin) {
+                CVL_CUDA(cudaMemsetAsync(slot_ctr, 0, sizeof(unsigned), s));
+                CVL_TRY(bf(e, ba, bblocks));
+            }
             e->mark("bundles");
             GrowthArgsT<R> ga{};
             ga.md = md;
@@ -750,6 +759,7 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
             ga.pcls = (const unsigned char *)e->pcls.p;
             ga.pflag = (const unsigned char *)e->pflag.p;
             ga.bund = (const R *)e->bund.p;
+            ga.pslot = (const unsigned *)e->pslot.p;
             ga.rec = rec;
             ga.arena_cap = cap;
             ga.arena_ctr = arena_ctr;

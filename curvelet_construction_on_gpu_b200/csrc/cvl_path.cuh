@@ -213,11 +213,23 @@ struct BundleArgsT {
     const int *pair_anchor;
     const unsigned char *pcls;
     const T *atrig;                     // [N][2Q+2]: sin(T2t_j), cos(T2t_j), cos(T2), sin(T2)
-    T *bund;                            // [p_end - p_begin][2][32 * CPL]
+    T *bund;                            // [slots][2][32 * CPL]: valid non-close pairs only, compacted
+    unsigned *pslot;                    // [p_end - p_begin]: bund slot of each valid non-close pair
+    unsigned *slot_ctr;                 // slots taken in this chunk (zero before the launch)
     unsigned char *pflag;               // [P]: bit 0 valid, bit 1 close
 };
 
 constexpr int BUNDLE_THREADS = 128;
+// Shared memory a k_bundles block stages its pairs' bundles in, at most.
+constexpr int BUNDLE_STAGE_BYTES = 24576;
+
+// Pairs a k_bundles block takes: one (pair, j) lane per thread, as many pairs as
+// the staging area holds (18 for the default 7 x 9 grid in FP64).
+__host__ __device__ inline int bundles_pairs_per_block(int Q, int pair_bytes) {
+    const int ppb = BUNDLE_THREADS / Q;
+    const int cap = BUNDLE_STAGE_BYTES / pair_bytes;
+    return ppb < cap ? ppb : cap;
+}
 
 // MINB: the resident 256-thread blocks per SM the register allocation is capped for
 // (3 or 4; with 128-thread blocks, twice as many of those). 128 threads measured 1%
@@ -225,28 +237,30 @@ constexpr int BUNDLE_THREADS = 128;
 template <typename T, int CPL, int MINB>
 __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS)) k_bundles(BundleArgsT<T> a) {
     const ModelT<T> &md = a.md;
+    constexpr int BW = 2 * 32 * CPL;
+    extern __shared__ __align__(16) unsigned char bn_smem[];
+    T *s_b = (T *)bn_smem;  // [PPB][BW]: the block's bundles until their validity is known
     __shared__ T s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
-    __shared__ unsigned char s_open[2][BUNDLE_THREADS];
+    __shared__ unsigned char s_open[BUNDLE_THREADS];
+    __shared__ unsigned char s_src[BUNDLE_THREADS];  // staged pair of each compacted slot of the block
+    __shared__ unsigned s_rel[BUNDLE_THREADS];       // slot of each staged pair in the block's run (~0: none)
+    __shared__ unsigned s_nv, s_base;
     for (int i = threadIdx.x; i < md.P; i += blockDim.x) {
         const T d = grid_offset(md.sx, i, md.P);  // delta_x2 (:697)
         s_dx2[i] = d;
         s_dx2_2[i] = T(2) * d;
         s_dx2sq[i] = d * d;
     }
-    for (int t = threadIdx.x; t < 2 * BUNDLE_THREADS; t += blockDim.x) (&s_open[0][0])[t] = 0;
+    for (int t = threadIdx.x; t < BUNDLE_THREADS; t += blockDim.x) s_open[t] = 0;
     __syncthreads();
-    constexpr int BW = 2 * 32 * CPL;
     const int t = threadIdx.x;
-    const int PPB = BUNDLE_THREADS / md.Q;
+    const int PPB = bundles_pairs_per_block(md.Q, BW * (int)sizeof(T));
     const int pl = t / md.Q, jl = t - pl * md.Q;
     const bool lane_on = pl < PPB;
     const T delta_t2 = grid_offset(md.st, jl, md.Q);  // :698
     const int A2 = 2 * md.Q + 2;
     const unsigned long long np = a.p_end - a.p_begin;
-    int it = 0;
-    for (unsigned long long g = (unsigned long long)blockIdx.x * PPB; g < np;
-         g += (unsigned long long)gridDim.x * PPB, ++it) {
-        const int buf = it & 1;
+    for (unsigned long long g = (unsigned long long)blockIdx.x * PPB; g < np; g += (unsigned long long)gridDim.x * PPB) {
         const unsigned long long q = g + pl;
         if (lane_on && q < np) {
             const unsigned long long p = a.p_begin + q;
@@ -263,7 +277,7 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                 const T s_m = cvl_sin(T2t - (T0 - md.dt));   // :728
                 const T s_p = cvl_sin(T2t - (T0 + md.dt));   // :729
                 const T tt = sTj * g2.DX - cTj * g2.DY;     // :705
-                T *dst = a.bund + q * BW;
+                T *dst = s_b + pl * BW;
                 bool open = false;
                 if constexpr (!std::is_same<T, double>::value) {
                     // float mode: :693-809 with their C++ types
@@ -303,20 +317,55 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                                                   dst[32 * CPL + i * md.Q + jl] = hi;
                                               });
                 }
-                if (open) s_open[buf][pl] = 1;
+                if (open) s_open[pl] = 1;
             }
         }
         __syncthreads();
-        if (t < PPB) {
-            const unsigned long long qq = g + t;
-            if (qq < np) {
-                const unsigned long long p = a.p_begin + qq;
-                const bool closep = (a.pcls[p] & 4u) != 0;
-                const bool valid = closep || s_open[buf][t] != 0;
-                a.pflag[p] = (unsigned char)((valid ? 1u : 0u) | (closep ? 2u : 0u));
+        // warp 0: each pair's flags; the valid non-close pairs take consecutive
+        // slots of the chunk's compacted bundle buffer (one atomic per block)
+        if (t < 32) {
+            unsigned nv = 0;
+            for (int k0 = 0; k0 < PPB; k0 += 32) {
+                const int k = k0 + t;
+                const unsigned long long qq = g + k;
+                bool need = false;
+                if (k < PPB && qq < np) {
+                    const unsigned long long p = a.p_begin + qq;
+                    const bool closep = (a.pcls[p] & 4u) != 0;
+                    const bool valid = closep || s_open[k] != 0;
+                    a.pflag[p] = (unsigned char)((valid ? 1u : 0u) | (closep ? 2u : 0u));
+                    need = valid && !closep;
+                }
+                const unsigned bal = __ballot_sync(FULL, need);
+                if (k < PPB) {
+                    s_open[k] = 0;
+                    s_rel[k] = need ? nv + __popc(bal & ((1u << t) - 1u)) : ~0u;
+                    if (need) s_src[s_rel[k]] = (unsigned char)k;
+                }
+                nv += __popc(bal);
             }
-            s_open[buf][t] = 0;
+            unsigned base = 0;
+            if (t == 0 && nv) base = atomicAdd(a.slot_ctr, nv);
+            base = __shfl_sync(FULL, base, 0);
+            if (t == 0) {
+                s_nv = nv;
+                s_base = base;
+            }
+            for (int k = t; k < PPB; k += 32)
+                if (s_rel[k] != ~0u) a.pslot[g + k] = base + s_rel[k];
         }
+        __syncthreads();
+        // the valid pairs' bundles to their slots: one contiguous run per block, 16-byte stores
+        {
+            constexpr int VP = BW * (int)sizeof(T) / 16;  // 16-byte words per pair
+            const int nv = (int)s_nv;
+            uint4 *gdst = (uint4 *)(a.bund + (size_t)s_base * BW);
+            for (int v = t; v < nv * VP; v += BUNDLE_THREADS) {
+                const int r = v / VP, w = v - r * VP;
+                gdst[v] = ((const uint4 *)(s_b + (size_t)s_src[r] * BW))[w];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -338,7 +387,8 @@ struct GrowthArgsT {
     const int *csr_ids;
     const unsigned char *pcls;
     const unsigned char *pflag;
-    const T *bund;
+    const T *bund;                      // the chunk's compacted bundles (k_bundles)
+    const unsigned *pslot;              // [chunk pairs]: bund slot of each valid non-close pair
     Records rec;                        // record arena
     unsigned long long arena_cap;
     unsigned long long *arena_ctr;
@@ -439,7 +489,9 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
             const unsigned b1 = __ballot_sync(FULL, t1);
             if (t0 || t1) {
                 const int slot = t0 ? ns_run0 + __popc(b0 & lt_mask) : md.max_cand - 1 - (ns_run1 + __popc(b1 & lt_mask));
-                seed_q[slot] = (unsigned)(off + k - a.p_begin) | ((fl & 2u) ? CLOSE_BIT : 0u);
+                // a valid non-close pair's bundle is at its compacted slot; a close pair
+                // keeps the default bundle and reads none
+                seed_q[slot] = (fl & 2u) ? CLOSE_BIT : a.pslot[off + k - a.p_begin];
                 seed_orig[slot] = a.B.orig[a.csr_ids[off + k]];
             }
             ns_run0 += __popc(b0);
