@@ -76,9 +76,12 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-map-per-launch comparison")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the served rate sweep (configs[3])")
+    ap.add_argument("--no-stress", action="store_true", help="skip the stress stream (configs[4])")
+    ap.add_argument("--no-small", action="store_true", help="skip batched vs plain on the 1,024 small maps")
     ap.add_argument("--rate", type=float, default=50.0, help="served stream: offered maps/s")
     ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")
-    ap.add_argument("--requests", type=int, default=600, help="served stream: requests per rate")
+    ap.add_argument("--requests", type=int, default=400, help="served stream: requests per rate")
     ap.add_argument("--workers", type=int, default=4, help="served stream: server workers")
     ap.add_argument("--large-yield-ms", type=int, default=10,
                     help="served stream: longest hold-back of a large launch between chunks (0: none)")
@@ -194,17 +197,62 @@ def _progress(msg: str) -> None:
 REF_SAFE_EDGES = (1 << 32) // (2 * 10 * (128 + 1))
 
 
-def _ref_sample(maps, max_edges: int):
-    """Whole maps the reference can hold, in workload order, until max_edges."""
+def _physical_cores() -> int:
+    """Physical cores of this host (distinct (package, core) pairs), not hardware threads."""
+    try:
+        seen, phys, core = set(), None, None
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("physical id"):
+                phys = line.split(":", 1)[1].strip()
+            elif line.startswith("core id"):
+                core = line.split(":", 1)[1].strip()
+            elif not line.strip():
+                if core is not None:
+                    seen.add((phys, core))
+                phys = core = None
+        if core is not None:
+            seen.add((phys, core))
+        if seen:
+            return len(seen)
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def _by_class(maps, labels):
+    """Map indices per image class, each class in workload order."""
+    out = {}
+    for i, lab in enumerate(labels or ["all"] * len(maps)):
+        out.setdefault(lab, []).append(i)
+    return out
+
+
+def _ref_sample(maps, max_edges: int, labels=None, max_map_edges: int | None = None):
+    """Whole maps the reference can hold (below REF_SAFE_EDGES, and max_map_edges when
+    given), stratified across the image classes: round robin over the classes, each in
+    workload order, until max_edges."""
+    classes = _by_class(maps, labels)
+    queues = {k: [i for i in v if maps[i].shape[0] < REF_SAFE_EDGES and
+                  (max_map_edges is None or maps[i].shape[0] <= max_map_edges)] for k, v in classes.items()}
     out, tot = [], 0
-    for m in maps:
-        if m.shape[0] >= REF_SAFE_EDGES:
-            continue
-        out.append(m)
-        tot += m.shape[0]
-        if tot >= max_edges:
-            break
+    while any(queues.values()) and tot < max_edges:
+        for k in sorted(queues):
+            if queues[k] and tot < max_edges:
+                i = queues[k].pop(0)
+                out.append(maps[i])
+                tot += maps[i].shape[0]
     return out, tot
+
+
+def _ref_step_sample(maps, labels):
+    """The reference arm's per-step sample: the smallest map of each image class (the
+    lowest densities, where the reference's cost per edge is lowest)."""
+    out = []
+    for k, idx in sorted(_by_class(maps, labels).items()):
+        ok = [i for i in idx if maps[i].shape[0] < REF_SAFE_EDGES]
+        if ok:
+            out.append(maps[min(ok, key=lambda i: maps[i].shape[0])])
+    return out, int(sum(m.shape[0] for m in out))
 
 
 def _dist_init(args):
@@ -239,20 +287,19 @@ def _barrier(pg):
         pg.barrier()
 
 
-def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
-    """The reference's own code (oracle/_ref) on this host's cores, on a bounded
-    sample of the workload: whole maps in order until ~budget_s of CPU work."""
+def _cpu_baseline(maps, budget_s: float = 20.0, labels=None) -> dict:
+    """The reference's own code (oracle/_ref) on this host's physical cores, on a
+    bounded sample of the workload: whole maps, stratified across the image classes
+    (round robin, each class in workload order), until ~budget_s of CPU work."""
     from oracle import oracle as O
-    threads = os.cpu_count() or 1
+    threads = _physical_cores()
     kind = "reference" if O.ref_available() else "port"
     edges = 0
     secs = 0.0
     used = 0
     phases = {"csr": 0.0, "pairwise": 0.0, "greedy": 0.0}
-    cand, _ = _ref_sample(maps, 1 << 62)
+    cand, _ = _ref_sample(maps, 1 << 62, labels, max_map_edges=600_000)  # 600k: within the time budget
     for m in cand:
-        if m.shape[0] > 600_000:  # keep the sample within the time budget
-            continue
         t0 = time.perf_counter()
         if kind == "reference":
             r = O.ref_run(m, nthreads=threads, want_outputs=False)
@@ -267,8 +314,10 @@ def _cpu_baseline(maps, budget_s: float = 20.0) -> dict:
         used += 1
         if secs > budget_s:
             break
-    out = {"value": edges / secs, "unit": METRIC, "cores": threads, "kind": kind, "cpu_model": _cpu_model(),
-           "sample": f"{used} of {len(maps)} map(s) (whole maps of at most 600k edges, in workload order), "
+    out = {"value": edges / secs, "unit": METRIC, "cores": threads, "logical_cpus": os.cpu_count(), "kind": kind,
+           "cpu_model": _cpu_model(),
+           "sample": f"{used} of {len(maps)} map(s) (whole maps of at most 600k edges, round robin over the "
+                     f"image classes), "
                      f"{edges} edges, timed as the reference's own CSR + form_pairwise_bundles + "
                      f"build_curvelets_greedy phases (file I/O excluded)"}
     if kind == "reference":
@@ -303,10 +352,13 @@ def run_reference(args, maps, cfg, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcvlref.so was not built "
                           "(the reference sources were absent at build time)"}))
         return
-    threads = os.cpu_count() or 1
-    # each step: the whole workload when it is small enough, else a bounded sample
-    # of whole maps that the reference can hold (REF_SAFE_EDGES)
-    sample, tot = _ref_sample(maps, 300_000)
+    threads = _physical_cores()
+    # each step: the whole workload when it is one map, else the smallest map of each
+    # image class that the reference can hold (REF_SAFE_EDGES)
+    if len(maps) == 1:
+        sample, tot = maps, int(maps[0].shape[0])
+    else:
+        sample, tot = _ref_step_sample(maps, cfg.get("_labels"))
     for _ in range(args.warmup):
         O.ref_run(sample[0], nthreads=threads, want_outputs=False)
     step_s = []
@@ -323,8 +375,11 @@ def run_reference(args, maps, cfg, world, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": dict(workload=args.workload, sample_edges=tot, sample_maps=len(sample),
                            **{k: v for k, v in cfg.items() if not k.startswith("_")}),
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
-                             "sample": f"{len(sample)} of {len(maps)} map(s), {tot} edges per step"},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "logical_cpus": os.cpu_count(),
+                             "kind": "reference", "cpu_model": _cpu_model(),
+                             "sample": f"{len(sample)} of {len(maps)} map(s), {tot} edges per step"
+                                       + ("" if len(maps) == 1 else
+                                          ": the smallest map of each image class the reference can hold")},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -337,25 +392,96 @@ def _stage_sums(times) -> dict:
     return out
 
 
-def _plain_device_ms(eng, maps, steps: int) -> float:
-    """Mean device ms per step of the plain form: one map per launch, maps resident."""
+def _plain_wall_ms(eng, maps, steps: int) -> float:
+    """Mean wall ms per step of the plain form: one map per launch (cvl_batch_run on
+    single-map batches resident in HBM), one after another, host syncs and launch
+    gaps included, as a caller that runs maps one at a time sees it."""
     singles = [eng.upload_batch([m]) for m in maps]
     for b in singles[:2]:
         eng.run_batch(b).close()
     total = 0.0
     for _ in range(steps):
         eng.flush_l2()
+        t0 = time.perf_counter()
         for b in singles:
-            r = eng.run_batch(b)
-            total += r.stats()["device_ms"]
-            r.close()
+            eng.run_batch(b).close()
+        total += time.perf_counter() - t0
     for b in singles:
         b.close()
-    return total / steps
+    return 1e3 * total / steps
+
+
+def _small_maps(eng, maps, steps: int, pg) -> dict:
+    """Batched against plain on a stream of small maps: the 1,024 small 640x480 maps
+    of the stress mix (the config-0 generator), where the per-launch cost of the
+    plain form is not hidden by the work. Resident: one ragged launch against 1,024
+    sequential single-map launches, both by wall clock. e2e: cvl_run_maps against
+    1,024 sequential cvl_run calls, pinned host edges in, results out."""
+    n_edges = int(sum(m.shape[0] for m in maps))
+    batch = eng.upload_batch(maps)
+    for _ in range(2):
+        eng.run_batch(batch).close()
+    dev, wall = [], []
+    for _ in range(steps):
+        eng.flush_l2()
+        t0 = time.perf_counter()
+        r = eng.run_batch(batch)
+        wall.append(time.perf_counter() - t0)
+        dev.append(r.stats()["device_ms"])
+        launches = int(r.stats()["launches"])
+        r.close()
+    batch.close()
+    b_wall = _max_over_ranks(pg, float(np.mean(wall)))
+    p_ms = _max_over_ranks(pg, _plain_wall_ms(eng, maps, steps))
+    pinned = _pinned(np.concatenate(maps, axis=0))
+    counts = np.array([m.shape[0] for m in maps], np.int32)
+    singles = [pinned[o - c:o] for o, c in zip(np.cumsum(counts), counts)]
+    held = eng.run_maps(pinned, counts=counts)
+    del held
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for res in eng.run_maps(pinned, counts=counts):
+            del res
+    be2e = _max_over_ranks(pg, (time.perf_counter() - t0) / steps)
+    for m in singles[:4]:
+        eng.run(m)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for m in singles:
+            res = eng.run(m)
+            del res
+    pe2e = _max_over_ranks(pg, (time.perf_counter() - t0) / steps)
+    return {"maps": len(maps), "edges": n_edges, "steps": steps,
+            "batched": {"wall_ms": 1e3 * b_wall, "device_ms": float(np.mean(dev)), "launches": launches,
+                        "edges_per_s": n_edges / b_wall},
+            "plain": {"wall_ms": p_ms, "edges_per_s": n_edges / (p_ms / 1e3),
+                      "form": "1,024 sequential cvl_batch_run calls on resident single-map batches"},
+            "batched_vs_plain": p_ms / (1e3 * b_wall),
+            "e2e": {"batched_ms": 1e3 * be2e, "plain_ms": 1e3 * pe2e, "batched_vs_plain": pe2e / be2e,
+                    "batched_edges_per_s": n_edges / be2e, "plain_edges_per_s": n_edges / pe2e,
+                    "form": "cvl_run_maps against sequential cvl_run, pinned host edges, results to host"}}
+
+
+def _distinct_pool(maps, labels, copies: int, rank: int):
+    """The served streams' pool: the workload's maps and copies-1 more copies of
+    each, translated by whole pixels (a seeded offset per copy), so that a stream
+    of a few hundred requests meets few repeated inputs. A whole-pixel translation
+    moves every pixel cell with its edges, so each copy is a valid map of the
+    same size class."""
+    pool, labs = list(maps), list(labels)
+    rng = np.random.default_rng(77 + rank)
+    for _ in range(copies - 1):
+        for m, lab in zip(maps, labels):
+            t = m.copy()
+            t[:, 0] += float(rng.integers(1, 64))
+            t[:, 1] += float(rng.integers(1, 64))
+            pool.append(t)
+            labs.append(lab)
+    return pool, labs
 
 
 def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, seed: int = 7,
-            sequence=None, warm_all: bool = True) -> dict:
+            sequence=None, warm_all: bool = True, n_warm: int | None = None) -> dict:
     """Open-loop Poisson stream through cvl_server_*: arrivals at `rate` maps/s,
     submitted on schedule by one thread while another takes the results in
     completion order. The maps are `sequence` (indices into maps) when given,
@@ -377,7 +503,7 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
         order = np.argsort([m.shape[0] for m in maps])
         warm = [srv.submit(maps[int(order[-1])]) for _ in range(workers)]
         if warm_all:
-            warm += [srv.submit(m) for m in maps]
+            warm += [srv.submit(m) for m in maps[:n_warm]]
         else:
             seen = {}
             for i, lab in enumerate(labels):
@@ -417,6 +543,7 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
         wall = time.perf_counter() - t0
         st = srv.stats()
         ms, ed, rid = srv.latencies(with_ids=True)
+        rt = srv.request_times()
         st0 = warm_stats
     finally:
         srv.close()
@@ -427,10 +554,18 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
     def pct(a, q):
         return float(np.percentile(a, q, method="inverted_cdf")) if len(a) else None
 
+    rt = rt[np.array([int(r) in label_of for r in rt["id"]], bool)] if len(rt) else rt
     classes = {}
     for lab in sorted(set(label_of.values())):
         sel = np.array([label_of[int(r)] == lab for r in rid], bool)
         classes[lab] = {"requests": int(sel.sum()), "p50_ms": pct(ms[sel], 50), "p99_ms": pct(ms[sel], 99)}
+        # where the slowest 5% of the class spent their time (means, ms)
+        rsel = rt[np.array([label_of[int(r)] == lab for r in rt["id"]], bool)] if len(rt) else rt
+        if len(rsel):
+            cut = np.percentile(rsel["total_ms"], 95)
+            tail = rsel[rsel["total_ms"] >= cut]
+            classes[lab]["tail5"] = {k: float(np.mean(tail[k])) for k in
+                                     ("total_ms", "queue_ms", "upload_ms", "run_ms", "result_ms", "launch_maps")}
     edges = float(np.sum(ed))
     return {"rate_maps_per_s": rate, "requests": n_req, "workers": workers,
             "large_workers": _LARGE_WORKERS or max(1, workers // 2), "large_yield_ms": _LARGE_YIELD_MS,
@@ -443,7 +578,11 @@ def _served(maps, labels, rate: float, n_req: int, workers: int, device: int, se
             "queue_ms_mean": float(st["queue_ms"] - st0["queue_ms"]) / max(1, len(ms)),
             "growth_during_stream": {k: float(st[k] - st0[k]) for k in ("device_grows", "device_grow_ms",
                                                                         "host_grows", "host_grow_ms")},
-            "admission": "40 GiB budget, 2048 B per edge", "pool": f"{len(maps)} seeded maps"}
+            "reserved_gib": float(st["reserved_bytes"]) / 2 ** 30,
+            "admission": "40 GiB budget; each request charged its workspace footprint (40 pairs, 8 curvelets "
+                         "per edge), each worker's workspace reserved at creation",
+            "pool": f"{len(maps)} seeded maps" + (f" (the workload's {n_warm} and translated copies)"
+                                                  if n_warm and n_warm < len(maps) else "")}
 
 
 def _measured_peaks() -> dict:
@@ -505,10 +644,11 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     plain = None
     if len(maps) > 1 and not args.no_plain:
         _progress("plain form (one map per launch)")
-        pms = _plain_device_ms(eng, maps, max(1, min(args.steps, 3)))
+        pms = _plain_wall_ms(eng, maps, max(1, min(args.steps, 3)))
         pms = _max_over_ranks(pg, pms)
         plain = {"value": _sum_over_ranks(pg, float(n_edges)) / (pms / 1e3), "unit": METRIC, "ms_per_step": pms,
-                 "form": "one map per launch, maps resident, same engine"}
+                 "form": "one map per launch (cvl_batch_run), maps resident, same engine, wall clock with the "
+                         "host syncs between launches"}
 
     # e2e through the public C ABI with host buffers: the one-shot call for a
     # single map, the batch calls (upload, run, download every map) for a batch
@@ -546,12 +686,35 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
                         "cvl_run_maps (C ABI): pinned host edges in, one result per map out; groups of maps "
                         "pipelined, result copies overlapping the next group's compute")}
 
+    small = stress = None
+    sweep = []
+    stress_maps = None
+    if len(maps) > 1 and (not args.no_small or not args.no_stress):
+        from curvelet_construction_on_gpu_b200 import synth
+        _progress("stress mix maps")
+        stress_maps, stress_kinds = synth.stress_mix(5000 + 10_000 * rank)
+    if stress_maps is not None and not args.no_small:
+        _progress("small maps: batched vs plain")
+        small = _small_maps(eng, [m for m, k in zip(stress_maps, stress_kinds) if k == "small"],
+                            max(1, min(args.steps, 3)), pg)
+
     served = None
     if len(maps) > 1 and not args.no_served and cfg.get("_labels"):
-        _progress(f"served stream at {args.rate} maps/s")
         batch.close()
         eng.close()
-        served = _served(maps, cfg["_labels"], args.rate, args.requests, args.workers, local)
+        rates = [args.rate] if args.no_sweep else sorted({float(r) for r in args.rates.split(",") if r} | {args.rate})
+        pool, labels = _distinct_pool(maps, cfg["_labels"], 1 if args.no_sweep else 4, rank)
+        for rate in rates:
+            _progress(f"served stream at {rate:g} maps/s")
+            sv = _served(pool, labels, rate, args.requests, args.workers, local, n_warm=len(maps))
+            sweep.append(sv)
+            if rate == args.rate:
+                served = sv
+        del pool
+    if stress_maps is not None and not args.no_stress:
+        _progress("stress stream at 150 maps/s")
+        stress = _served(stress_maps, stress_kinds, 150.0, len(stress_maps), args.workers, local,
+                         sequence=list(range(len(stress_maps))), warm_all=False)
 
     if rank != 0:
         return
@@ -597,9 +760,15 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
         line["batched_vs_plain"] = value / plain["value"]
     if served is not None:
         line["served"] = served
+    if len(sweep) > 1:
+        line["served_sweep"] = sweep
+    if stress is not None:
+        line["stress"] = stress
+    if small is not None:
+        line["small_maps"] = small
     if world == 1 and not args.no_cpu_baseline:
         _progress("cpu baseline")
-        line["cpu_baseline"] = _cpu_baseline(maps)
+        line["cpu_baseline"] = _cpu_baseline(maps, labels=cfg.get("_labels"))
     line["config"].pop("_labels", None)
     print(json.dumps(line))
     eng.close()
@@ -685,7 +854,7 @@ def run_contours(args, maps, cfg, world, rank, local, pg):
     }
     if world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
-        threads = os.cpu_count() or 1
+        threads = _physical_cores()
         if O.ref_available() and O.orig_available():
             r = O.ref_run(e, nthreads=threads)
             ref_s = (r.ms["csr"] + r.ms["pairwise"] + r.ms["greedy"]) / 1e3
@@ -728,7 +897,7 @@ def run_reference_contours(args, maps, cfg, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref harnesses were not built "
                           "(the reference sources were absent at build time)"}))
         return
-    threads = os.cpu_count() or 1
+    threads = _physical_cores()
     e = maps[0]
     r = O.ref_run(e, nthreads=threads)
     fw = (r.info[:, 0] > 0).astype(np.uint8)

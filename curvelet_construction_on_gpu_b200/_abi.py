@@ -62,7 +62,8 @@ class CvlServerCfg(C.Structure):
                 ("admit_bytes_per_edge", C.c_size_t), ("max_batch_edges", C.c_int64),
                 ("large_map_edges", C.c_int64), ("host_reserve_bytes", C.c_size_t),
                 ("small_takes_large", C.c_int), ("large_workers", C.c_int), ("large_yield_ms", C.c_int),
-                ("device_reserve_bytes", C.c_size_t)]
+                ("device_reserve_bytes", C.c_size_t), ("max_map_edges", C.c_int64), ("pairs_per_edge", C.c_double),
+                ("curvelets_per_edge", C.c_double)]
 
 
 class CvlServerStats(C.Structure):
@@ -72,7 +73,23 @@ class CvlServerStats(C.Structure):
                 ("p95_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
                 ("upload_ms", C.c_double), ("run_ms", C.c_double), ("device_ms", C.c_double),
                 ("result_ms", C.c_double), ("queue_ms", C.c_double), ("device_grows", C.c_uint64),
-                ("device_grow_ms", C.c_double), ("host_grows", C.c_uint64), ("host_grow_ms", C.c_double)]
+                ("device_grow_ms", C.c_double), ("host_grows", C.c_uint64), ("host_grow_ms", C.c_double),
+                ("reserved_bytes", C.c_size_t)]
+
+
+class CvlRequestTimes(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("edges", C.c_int64), ("queue_ms", C.c_double), ("upload_ms", C.c_double),
+                ("run_ms", C.c_double), ("result_ms", C.c_double), ("total_ms", C.c_double),
+                ("launch_maps", C.c_int32), ("worker", C.c_int32)]
+
+
+class CvlEngineMemory(C.Structure):
+    _fields_ = [("held_bytes", C.c_size_t), ("device_grows", C.c_uint64), ("device_grow_ms", C.c_double)]
+
+
+class CvlWorkspaceShape(C.Structure):
+    _fields_ = [("num_edges", C.c_int64), ("num_pairs", C.c_int64), ("num_curvelets", C.c_int64),
+                ("num_maps", C.c_int32), ("edge_data_sz", C.c_int32)]
 
 
 class CvlTuning(C.Structure):
@@ -124,6 +141,11 @@ SIGNATURES = [
     ("cvl_build_curvelets", C.c_int, [_vp, _vp, C.POINTER(CvlParams), C.POINTER(_vp)]),
     ("cvl_pair_bundles", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), _dp, _dp,
                                    C.POINTER(C.c_uint8), C.POINTER(C.c_int32)]),
+    ("cvl_engine_workspace_bytes", C.c_int, [_vp, C.POINTER(CvlWorkspaceShape), C.POINTER(CvlParams),
+                                            C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    ("cvl_engine_reserve_workspace", C.c_int, [_vp, C.POINTER(CvlWorkspaceShape), C.POINTER(CvlParams)]),
+    ("cvl_engine_memory_get", C.c_int, [_vp, C.POINTER(CvlEngineMemory)]),
+    ("cvl_debug_fail_allocations", C.c_int, [C.c_int64]),
     ("cvl_check_pair_bundles_literal", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), _dp, _dp,
                                                  C.POINTER(C.c_uint8), C.POINTER(C.c_int32)]),
     ("cvl_check_transport_cells", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), _dp, C.POINTER(C.c_int32)]),
@@ -145,6 +167,7 @@ SIGNATURES = [
     ("cvl_server_wait", C.c_int, [_vp, C.c_uint64, C.c_int64, C.POINTER(_vp)]),
     ("cvl_server_next", C.c_int, [_vp, C.c_int64, C.POINTER(C.c_uint64), C.POINTER(_vp)]),
     ("cvl_server_stats_get", C.c_int, [_vp, C.POINTER(CvlServerStats)]),
+    ("cvl_server_request_times", C.c_int64, [_vp, C.POINTER(CvlRequestTimes), C.c_int64]),
     ("cvl_server_latencies", C.c_int64, [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), C.c_int64]),
     ("cvl_server_destroy", None, [_vp]),
     ("cvl_read_edges", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_dp), C.POINTER(C.c_int64)]),

@@ -419,6 +419,30 @@ class Engine:
                  bmax.ctypes.data_as(_abi._dp), valid.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(cells)), name)
         return bmin[:n], bmax[:n], valid[:n].astype(bool)
 
+    def workspace_bytes(self, num_edges: int, num_pairs: int, num_curvelets: int, num_maps: int = 1,
+                        params: CurveletParams | None = None, edge_data_sz: int = 4) -> tuple[int, int]:
+        """cvl_engine_workspace_bytes: (total, per-launch bundle chunk) device bytes of a launch of that shape."""
+        shp = _abi.CvlWorkspaceShape(num_edges, num_pairs, num_curvelets, num_maps, edge_data_sz)
+        p = (params or CurveletParams()).to_c()
+        tot, chunk = C.c_size_t(0), C.c_size_t(0)
+        check(self._lib.cvl_engine_workspace_bytes(self._h, C.byref(shp), C.byref(p), C.byref(tot), C.byref(chunk)),
+              "cvl_engine_workspace_bytes")
+        return int(tot.value), int(chunk.value)
+
+    def reserve_workspace(self, num_edges: int, num_pairs: int, num_curvelets: int, num_maps: int = 1,
+                          params: CurveletParams | None = None, edge_data_sz: int = 4) -> None:
+        """cvl_engine_reserve_workspace: allocate the workspace of that launch shape now."""
+        shp = _abi.CvlWorkspaceShape(num_edges, num_pairs, num_curvelets, num_maps, edge_data_sz)
+        p = (params or CurveletParams()).to_c()
+        check(self._lib.cvl_engine_reserve_workspace(self._h, C.byref(shp), C.byref(p)),
+              "cvl_engine_reserve_workspace")
+
+    def memory(self) -> dict:
+        """cvl_engine_memory_get: held_bytes, device_grows, device_grow_ms."""
+        m = _abi.CvlEngineMemory()
+        check(self._lib.cvl_engine_memory_get(self._h, C.byref(m)), "cvl_engine_memory_get")
+        return {name: getattr(m, name) for name, _ in m._fields_}
+
     def transport_cells(self, ops, params: CurveletParams | None = None, dt_rad: float = 0.0):
         """cvl_check_transport_cells: one orientation column of the transport per row of
         ops [n, 10] = (DX, DY, tt, s_m, s_p, cos_m, sin_m, cos_p, sin_p, branch1).
@@ -584,10 +608,11 @@ class Server:
     out once."""
 
     def __init__(self, params: CurveletParams | None = None, device: int = 0, workers: int = 4,
-                 mem_budget_bytes: int = 40 << 30, admit_bytes_per_edge: int = 2048,
+                 mem_budget_bytes: int = 40 << 30, admit_bytes_per_edge: int = 0,
                  max_batch_edges: int = 2 << 20, large_map_edges: int = 1_000_000,
                  host_reserve_bytes: int = 2 << 30, small_takes_large: bool = False, large_workers: int = 0,
-                 large_yield_ms: int = 10):
+                 large_yield_ms: int = 10, max_map_edges: int = 4 << 20, pairs_per_edge: float = 40.0,
+                 curvelets_per_edge: float = 8.0, device_reserve_bytes: int = 0):
         lib = _abi.load()
         self._lib = lib
         cfg = _abi.CvlServerCfg()
@@ -599,6 +624,8 @@ class Server:
         cfg.small_takes_large = 1 if small_takes_large else 0
         cfg.large_workers = large_workers
         cfg.large_yield_ms = large_yield_ms
+        cfg.max_map_edges, cfg.pairs_per_edge, cfg.curvelets_per_edge = max_map_edges, pairs_per_edge, curvelets_per_edge
+        cfg.device_reserve_bytes = device_reserve_bytes
         self._p = (params or CurveletParams()).to_c()
         h = C.c_void_p()
         check(lib.cvl_server_create(C.byref(cfg), C.byref(self._p), C.byref(h)), "cvl_server_create")
@@ -655,6 +682,19 @@ class Server:
         if k < 0:
             check(int(k), "cvl_server_latencies")
         return (ms[:k], ed[:k], ids[:k]) if with_ids else (ms[:k], ed[:k])
+
+    def request_times(self) -> np.ndarray:
+        """cvl_server_request_times: a structured array (id, edges, queue_ms, upload_ms,
+        run_ms, result_ms, total_ms, launch_maps, worker) per completed request."""
+        n = int(self.stats()["completed"])
+        buf = (_abi.CvlRequestTimes * max(n, 1))()
+        k = self._lib.cvl_server_request_times(self._h, buf, n)
+        if k < 0:
+            check(int(k), "cvl_server_request_times")
+        dt = np.dtype([(name, np.int64 if name == "edges" else np.uint64 if name == "id" else
+                        np.int32 if name in ("launch_maps", "worker") else np.float64)
+                       for name, _ in _abi.CvlRequestTimes._fields_], align=True)
+        return np.frombuffer(bytes(buf), dtype=dt, count=k).copy() if k else np.zeros(0, dt)
 
     def close(self):
         if self._h:

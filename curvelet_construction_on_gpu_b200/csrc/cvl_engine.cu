@@ -20,6 +20,7 @@
 #include <vector>
 
 #include <cuda.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/cvl.h"
 #include "cvl_internal.h"
@@ -72,6 +73,23 @@ inline unsigned next_pow2(unsigned long long v) {
 }  // namespace
 
 int cvl_fail(int code, const std::string &msg) { return fail(code, msg); }
+
+// ---- allocation-failure injector ----------------------------------------------------
+// Allocations left before every device or page-locked allocation of the library
+// fails as if the memory were exhausted; -1: off. Armed by cvl_debug_fail_allocations
+// or, when the library loads, by CVL_FAIL_ALLOC_AFTER=<k> in the environment.
+static std::atomic<int64_t> g_fail_after{[] {
+    const char *v = std::getenv("CVL_FAIL_ALLOC_AFTER");
+    return v ? (int64_t)std::strtoll(v, nullptr, 10) : (int64_t)-1;
+}()};
+
+bool cvl_alloc_fault_injected() {
+    int64_t left = g_fail_after.load();
+    while (left > 0) {
+        if (g_fail_after.compare_exchange_weak(left, left - 1)) return false;
+    }
+    return left == 0;
+}
 
 void cvl_engine_set_yield(cvl_engine *e, cvl_yield_fn fn, void *ctx);
 
@@ -160,7 +178,8 @@ struct cvl_engine {
                                             std::to_string(budget) + " bytes)");
         }
         const auto t_grow = std::chrono::steady_clock::now();
-        cudaError_t e = cudaMallocFromPoolAsync(&b.p, want, pool, stream);
+        cudaError_t e = cvl_alloc_fault_injected() ? cudaErrorMemoryAllocation
+                                                   : cudaMallocFromPoolAsync(&b.p, want, pool, stream);
         dev_grow_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
                            std::chrono::steady_clock::now() - t_grow).count();
         ++dev_grows;
@@ -185,6 +204,7 @@ struct cvl_engine {
         mark_names[nmarks] = name;
         cudaEventRecord(marks[nmarks], stream);
         ++nmarks;
+        nvtxMarkA(name);  // the stage's end on the host timeline (profilers)
     }
 
     int last_launches = 0;
@@ -535,6 +555,11 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
                  RunOut &ro) {
     const int M = (int)map_off_host.size() - 1;
     cudaStream_t s = e->stream;
+    // one NVTX range per run on the host timeline, a mark at each stage's end
+    struct NvtxRun {
+        NvtxRun() { nvtxRangePushA("cvl path"); }
+        ~NvtxRun() { nvtxRangePop(); }
+    } nvtx_run;
     e->nmarks = 0;
     ++e->generation;
     g_launches = 0;
@@ -822,6 +847,88 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     }
 }
 
+// ---- the workspace of a launch, by shape ----------------------------------------
+// The device buffers run_pipeline (mode 0, FP64) takes for a launch of shape s, with
+// the sizes it asks for once the counts are known: the same buffers and the same
+// requests, with each count at the shape's value (a chunk of bundles at its largest).
+// A buffer that already holds a request's size is reused as it is, so a workspace
+// allocated from this plan serves every launch within the shape with no allocation.
+struct WsItem {
+    DBuf cvl_engine::*buf;
+    size_t bytes;
+    bool per_launch;  // the bundle chunk: one per launch, whatever the maps
+};
+
+// tune: the engine's tuning per bucket (it sets the bundle chunk); arena_hint: the
+// record arena a past input needed (0 for a footprint alone)
+std::vector<WsItem> workspace_plan(const cvl_tuning *tune, unsigned long long arena_hint, const Model &md, int cpl,
+                                   const cvl_workspace_shape &s) {
+    const unsigned long long n = (unsigned long long)std::max<int64_t>(s.num_edges, 1);
+    const unsigned long long P = (unsigned long long)std::max<int64_t>(s.num_pairs, 0);
+    const unsigned long long C = (unsigned long long)std::max<int64_t>(s.num_curvelets, 0);
+    const unsigned long long M = (unsigned long long)std::max<int32_t>(s.num_maps, 1);
+    const cvl_tuning &tn = tune[bucket_of((long long)n)];
+    const unsigned long long T = next_pow2(std::max<unsigned long long>(n, 1024ull));
+    const size_t R = sizeof(double);
+    std::vector<WsItem> v;
+    auto add = [&](DBuf cvl_engine::*b, unsigned long long bytes, bool per_launch = false) {
+        v.push_back({b, (size_t)std::max<unsigned long long>(bytes, 16ull), per_launch});
+    };
+    using E = cvl_engine;
+    // the input rows and map offsets (cvl_run's upload; a batch holds its own instead)
+    add(&E::edges, sizeof(double) * n * (unsigned long long)std::max<int32_t>(s.edge_data_sz, 4));
+    add(&E::map_off, 4 * (M + 1));
+    // N-sized (run_pipeline's first block)
+    add(&E::ehash, 4 * n);
+    add(&E::bcount, 4 * (T + 1));
+    add(&E::bstart, 4 * (T + 1));
+    add(&E::bfill, 4 * (T + 1));
+    add(&E::pos_of, 4 * n);
+    for (DBuf E::*b : {&E::bx, &E::by, &E::bth, &E::bsp, &E::bcp, &E::bsm, &E::bcm}) add(b, R * n);
+    add(&E::bcell, 8 * n);
+    add(&E::orig_of, 4 * n);
+    add(&E::bmap, 4 * n);
+    add(&E::ncand, 4 * n);
+    add(&E::deg, 4 * n);
+    add(&E::pair_off, 8 * (n + 1));
+    add(&E::count, 4 * n);
+    add(&E::run_cnt, 8 * n);
+    add(&E::rec_base, 8 * n);
+    add(&E::out_off, 8 * (n + 1));
+    add(&E::stats, sizeof(MapStats) * M);
+    add(&E::err, 16);
+    add(&E::work, 32);
+    add(&E::scan_tmp, (T / SCAN_TILE + 64) * 4 * sizeof(unsigned long long) + 4096);  // the largest scan: T
+    add(&E::chunk_start, 4 * (4096 + 1));
+    // pair-sized (after the count)
+    add(&E::csr_ids, 4 * P);
+    add(&E::pcls, P);
+    add(&E::pflag, P);
+    add(&E::pair_anchor, 4 * P);
+    add(&E::atrig, R * n * (unsigned long long)(2 * md.Q + 2));
+    // one chunk of bundles (max_deg <= max_candidates)
+    const unsigned long long per_chunk = std::max<unsigned long long>((unsigned long long)tn.chunk_pairs, 1024ull);
+    const unsigned long long chunk_cap =
+        std::min<unsigned long long>(P + 1, per_chunk + (unsigned long long)md.max_cand + 1);
+    add(&E::bund, R * 64 * (unsigned long long)cpl * chunk_cap, true);
+    add(&E::pslot, 4 * chunk_cap, true);
+    // the record arena (run_pipeline's cap, with room for C records)
+    const unsigned long long nchunks = std::max<unsigned long long>((P + per_chunk - 1) / per_chunk, 1ull);
+    const unsigned long long cap =
+        std::max<unsigned long long>(std::max<unsigned long long>(arena_hint, C), 4ull * n + 4096ull) + n +
+        (unsigned long long)GROWTH_ARENA_CHUNK * (nchunks + 1);
+    add(&E::rec_ids, 4 * cap * (unsigned long long)md.gms);
+    add(&E::rec_k, 16 * cap);
+    add(&E::rec_meta, 4 * cap);
+    add(&E::crank, 2 * CELLS_MAX);
+    // outputs
+    add(&E::chains, 4 * C * (unsigned long long)(md.gms + 1));
+    add(&E::info, 80 * C);
+    return v;
+}
+
+inline size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+
 template <typename T>
 int upload(cvl_engine *e, const T *edges, int n, int sz, const std::vector<int32_t> &map_off) {
     CVL_TRY(e->alloc(e->edges, sizeof(T) * (size_t)n * sz));
@@ -901,6 +1008,12 @@ void cvl_engine_cfg_default(cvl_engine_cfg *c) {
 }
 
 const char *cvl_last_error(void) { return g_err.c_str(); }
+
+int cvl_debug_fail_allocations(int64_t after) {
+    if (after < -1) return fail(CVL_EINVAL, "after must be >= -1");
+    g_fail_after.store(after);
+    return CVL_OK;
+}
 
 const char *cvl_version(void) { return "cvl 0.1.0 (sm_100a, FP64)"; }
 
@@ -1253,7 +1366,7 @@ int cvl_batch_refill_parts(cvl_batch *b, const double *const *parts, const int32
             b->edges_cap = 0;
         }
         if (e->budget && e->held + want > e->budget) return fail(CVL_ENOMEM, "batch exceeds the device memory budget");
-        if (cudaMallocFromPoolAsync(&b->d_edges, want, e->pool, e->stream) != cudaSuccess) {
+        if (cvl_alloc_fault_injected() || cudaMallocFromPoolAsync(&b->d_edges, want, e->pool, e->stream) != cudaSuccess) {
             cudaGetLastError();
             b->d_edges = nullptr;
             return fail(CVL_ENOMEM, "batch allocation failed");
@@ -1484,12 +1597,95 @@ int cvl_engine_reserve_device(cvl_engine *e, size_t bytes) {
     if (!bytes) return CVL_OK;
     CVL_CUDA(cudaSetDevice(e->device));
     void *p = nullptr;
-    if (cudaMallocFromPoolAsync(&p, bytes, e->pool, e->stream) != cudaSuccess) {
+    if (cvl_alloc_fault_injected() || cudaMallocFromPoolAsync(&p, bytes, e->pool, e->stream) != cudaSuccess) {
         cudaGetLastError();
         return fail(CVL_ENOMEM, "device memory could not be reserved (" + std::to_string(bytes) + " bytes)");
     }
     CVL_CUDA(cudaFreeAsync(p, e->stream));
     CVL_CUDA(cudaStreamSynchronize(e->stream));
+    return CVL_OK;
+}
+
+extern "C" {
+
+int cvl_engine_workspace_bytes(cvl_engine *e, const cvl_workspace_shape *s, const cvl_params *p, size_t *total,
+                               size_t *per_launch) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    return cvl_workspace_bytes_tuned(e->tune, s, p, total, per_launch);
+}
+
+int cvl_engine_reserve_workspace(cvl_engine *e, const cvl_workspace_shape *s, const cvl_params *p) {
+    size_t total = 0;
+    CVL_TRY(cvl_engine_workspace_bytes(e, s, p, &total, nullptr));
+    CVL_CUDA(cudaSetDevice(e->device));
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(e, p, p->nrad, 3u, p->max_candidates, md, cpl));
+    // the record arena of later runs holds at least the shape's curvelets
+    e->arena_hint = std::max<unsigned long long>(e->arena_hint, (unsigned long long)s->num_curvelets);
+    for (const WsItem &w : workspace_plan(e->tune, e->arena_hint, md, cpl, *s)) CVL_TRY(e->alloc(e->*(w.buf), w.bytes));
+    CVL_CUDA(cudaStreamSynchronize(e->stream));
+    return CVL_OK;
+}
+
+int cvl_engine_memory_get(cvl_engine *e, cvl_engine_memory *out) {
+    if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
+    out->held_bytes = e->held;
+    out->device_grows = e->dev_grows.load();
+    out->device_grow_ms = (double)e->dev_grow_ns.load() * 1e-6;
+    return CVL_OK;
+}
+
+}  // extern "C"
+
+int cvl_workspace_bytes_tuned(const cvl_tuning *tune, const cvl_workspace_shape *s, const cvl_params *p,
+                              size_t *total, size_t *per_launch) {
+    if (!tune || !s || !p || !total) return fail(CVL_EINVAL, "tuning/shape/params/total is NULL");
+    if (s->num_edges < 1 || s->num_edges > 0x7fffffffLL || s->num_pairs < 0 || s->num_curvelets < 0 ||
+        s->num_maps < 1 || s->edge_data_sz < 4)
+        return fail(CVL_EINVAL, "workspace shape out of range");
+    Model md;
+    int cpl = 2;
+    CVL_TRY(make_model(nullptr, p, p->nrad, 3u, p->max_candidates, md, cpl));
+    size_t t = 0, c = 0;
+    for (const WsItem &w : workspace_plan(tune, 0, md, cpl, *s)) {
+        t += round256(w.bytes);
+        if (w.per_launch) c += round256(w.bytes);
+    }
+    *total = t;
+    if (per_launch) *per_launch = c;
+    return CVL_OK;
+}
+
+int cvl_batch_create_reserved(cvl_engine *e, int64_t max_edges, int32_t max_maps, int32_t edge_data_sz,
+                              cvl_batch **out) {
+    if (!e || !out || max_edges < 1 || max_maps < 1 || edge_data_sz < 4) return fail(CVL_EINVAL, "invalid batch arguments");
+    *out = nullptr;
+    CVL_CUDA(cudaSetDevice(e->device));
+    cvl_batch *b = new cvl_batch();
+    b->eng = e;
+    const size_t eb = sizeof(double) * (size_t)max_edges * (size_t)edge_data_sz;
+    const size_t mb = sizeof(int) * ((size_t)max_maps + 1);
+    if (e->budget && e->held + eb > e->budget) {
+        delete b;
+        return fail(CVL_ENOMEM, "batch exceeds the device memory budget");
+    }
+    if (cvl_alloc_fault_injected() || cudaMallocFromPoolAsync(&b->d_edges, eb, e->pool, e->stream) != cudaSuccess ||
+        cudaMallocFromPoolAsync(&b->d_map_off, mb, e->pool, e->stream) != cudaSuccess) {
+        cudaGetLastError();
+        if (b->d_edges) cudaFreeAsync(b->d_edges, e->stream);
+        if (b->d_map_off) cudaFreeAsync(b->d_map_off, e->stream);
+        delete b;
+        return fail(CVL_ENOMEM, "batch allocation failed");
+    }
+    e->dev_grows += 2;
+    b->edges_cap = eb;
+    b->map_off_cap = (size_t)max_maps + 1;
+    e->held += eb;
+    b->sz = edge_data_sz;
+    e->batches.push_back(b);
+    CVL_CUDA(cudaStreamSynchronize(e->stream));
+    *out = b;
     return CVL_OK;
 }
 
@@ -1651,8 +1847,6 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[CVL_NOALLOC_SCRATCH_BY
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
-
-inline size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 size_t noalloc_bytes(size_t n, size_t cells) {
     return 256 + round256(48 * n) + 2 * round256(8 * n * cells) + round256(n);

@@ -21,6 +21,10 @@
 #include <unordered_map>
 #include <vector>
 
+// The library's allocation-failure injector (cvl_debug_fail_allocations): true when
+// this allocation is to fail as if the memory were exhausted.
+bool cvl_alloc_fault_injected();
+
 namespace cvl {
 
 class PinnedArena {
@@ -44,6 +48,7 @@ class PinnedArena {
         for (const Chunk &c : chunks_) total += c.size;
         const size_t want = round(std::max({bytes, first_, total}));
         void *base = nullptr;
+        if (cvl_alloc_fault_injected()) return nullptr;
         const auto t0 = std::chrono::steady_clock::now();
         const cudaError_t ce = cudaMallocHost(&base, want);
         grow_ns_ += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(

@@ -43,6 +43,7 @@ struct Request {
     size_t charge = 0;
     int lane = 0;
     Clock::time_point t_submit;
+    cvl_request_times times{};  // filled as the request goes through
     bool done = false;
     int status = CVL_OK;
     std::string err;
@@ -55,10 +56,16 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 }  // namespace
 
+// maps folded into one launch at most (the reserved workspace's per-map statistics)
+constexpr int32_t MAX_MAPS_PER_LAUNCH = 4096;
+
 struct cvl_server {
     cvl_server_cfg cfg{};
     cvl_params params{};
+    cvl_tuning tune[CVL_TUNING_BUCKETS];  // the workers' tuning (the footprint's bundle chunk)
     std::vector<cvl_engine *> engines;
+    std::vector<cvl_batch *> wbatch;  // each worker's device batch, reserved at creation
+    size_t reserved = 0;              // device workspace reserved by the workers
     std::vector<std::thread> threads;
     cvl::PinnedArena host;
 
@@ -79,6 +86,7 @@ struct cvl_server {
     std::vector<double> lat_ms;
     std::vector<int64_t> lat_edges;
     std::vector<uint64_t> lat_ids;
+    std::vector<cvl_request_times> lat_times;
 
     // the lane a worker serves first (the last large_workers workers prefer large maps when there are several)
     int preferred_lane(int w) const { return (cfg.workers >= 2 && w >= cfg.workers - cfg.large_workers) ? 1 : 0; }
@@ -106,15 +114,52 @@ struct cvl_server {
         if (status == CVL_OK) {
             ++completed;
             edges_completed += (uint64_t)r->n;
-            lat_ms.push_back(ms_between(r->t_submit, Clock::now()));
+            const double total = ms_between(r->t_submit, Clock::now());
+            lat_ms.push_back(total);
             lat_edges.push_back(r->n);
             lat_ids.push_back(r->id);
+            r->times.id = r->id;
+            r->times.edges = r->n;
+            r->times.total_ms = total;
+            lat_times.push_back(r->times);
         } else {
             ++failed;
         }
     }
 
     void worker(int w);
+
+    // The launch shape of n edges (sz values each, maps maps) at the configured
+    // pairs and curvelets per edge.
+    cvl_workspace_shape shape_of(int64_t n, int32_t sz, int32_t maps) const {
+        cvl_workspace_shape sh;
+        sh.num_edges = n;
+        sh.num_pairs = (int64_t)std::ceil((double)n * cfg.pairs_per_edge);
+        sh.num_curvelets = (int64_t)std::ceil((double)n * cfg.curvelets_per_edge);
+        sh.num_maps = maps;
+        sh.edge_data_sz = sz;
+        return sh;
+    }
+
+    // A request's admission charge: its workspace footprint (a launch of the map
+    // alone, less the bundle chunk that each worker holds once), or the per-edge charge.
+    size_t charge_of(int64_t n, int32_t sz) const {
+        if (cfg.admit_bytes_per_edge) return (size_t)n * cfg.admit_bytes_per_edge;
+        const cvl_workspace_shape sh = shape_of(n, sz, 1);
+        size_t total = 0, chunk = 0;
+        if (cvl_workspace_bytes_tuned(tune, &sh, &params, &total, &chunk) != CVL_OK) return (size_t)-1;
+        return total - chunk;
+    }
+
+    // The largest map of at most cap edges whose charge fits the budget (0 if none).
+    int64_t largest_admissible(int64_t cap) const {
+        int64_t lo = 0, hi = cap;
+        while (lo < hi) {
+            const int64_t mid = lo + (hi - lo + 1) / 2;
+            if (charge_of(mid, 4) <= cfg.mem_budget_bytes) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+    }
 
     // Engine hook of a worker running a large launch, called between its chunks:
     // while small-lane work is queued or running, hold back (large_yield_ms at most), so
@@ -135,7 +180,7 @@ struct cvl_server {
 void cvl_server::worker(int w) {
     cudaSetDevice(cfg.device);
     cvl_engine *e = engines[w];
-    cvl_batch *batch = nullptr;
+    cvl_batch *batch = wbatch[w];
     std::vector<Request *> take;
     std::vector<int32_t> counts;
     std::vector<const double *> parts;
@@ -152,9 +197,12 @@ void cvl_server::worker(int w) {
             while (!lanes[l].empty()) {
                 Request *r = lanes[l].front();
                 if (!take.empty() && sum + r->n > cfg.max_batch_edges) break;
+                if ((int32_t)take.size() >= MAX_MAPS_PER_LAUNCH) break;
                 if (admitted + r->charge > cfg.mem_budget_bytes) break;
                 lanes[l].pop_front();
-                queue_ms += ms_between(r->t_submit, Clock::now());
+                r->times.queue_ms = ms_between(r->t_submit, Clock::now());
+                r->times.worker = w;
+                queue_ms += r->times.queue_ms;
                 admitted += r->charge;
                 ++in_flight;
                 take.push_back(r);
@@ -206,35 +254,46 @@ void cvl_server::worker(int w) {
             cvl_batch_stats bst;
             if (cvl_batch_result_stats(br, &bst) == CVL_OK) dev_ms = bst.device_ms;
         }
-        std::vector<cvl_result *> outs(take.size(), nullptr);
-        std::vector<int> st(take.size(), rc);
-        std::vector<std::string> errs(take.size(), err);
-        if (rc == CVL_OK) {
-            for (size_t m = 0; m < take.size(); ++m) {
-                st[m] = cvl_batch_result_take_map(br, (int32_t)m, &outs[m]);
-                if (st[m] != CVL_OK) errs[m] = cvl_last_error();
-            }
-        }
-        if (br) cvl_batch_result_free(br);
-        const Clock::time_point t3 = Clock::now();
+        const double t_up = ms_between(t0, t1), t_run = ms_between(t1, t2);
         {
             std::lock_guard<std::mutex> lk(mu);
-            upload_ms += ms_between(t0, t1);
-            run_ms += ms_between(t1, t2);
+            upload_ms += t_up;
+            run_ms += t_run;
             device_ms += dev_ms;
-            result_ms += ms_between(t2, t3);
-            for (size_t m = 0; m < take.size(); ++m) {
-                host.put(take[m]->edges);
-                take[m]->edges = nullptr;
-                finish(take[m], st[m], errs[m], outs[m]);
-            }
-            if (lane_now == 0) --small_running;
         }
+        // each map's rows to its own result; a request is finished as soon as its
+        // rows are copied (not at the end of the launch's copies)
+        for (size_t m = 0; m < take.size(); ++m) {
+            cvl_result *out = nullptr;
+            int stm = rc;
+            std::string errm = err;
+            if (rc == CVL_OK) {
+                stm = cvl_batch_result_take_map(br, (int32_t)m, &out);
+                if (stm != CVL_OK) errm = cvl_last_error();
+            }
+            const Clock::time_point tm = Clock::now();
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                Request *r = take[m];
+                r->times.upload_ms = t_up;
+                r->times.run_ms = t_run;
+                r->times.result_ms = ms_between(t2, tm);
+                r->times.launch_maps = (int32_t)take.size();
+                host.put(r->edges);
+                r->edges = nullptr;
+                finish(r, stm, errm, out);
+                if (m + 1 == take.size()) {
+                    result_ms += ms_between(t2, tm);
+                    if (lane_now == 0) --small_running;
+                }
+            }
+            cv_done.notify_all();
+        }
+        if (br) cvl_batch_result_free(br);
         cv_done.notify_all();
         cv_work.notify_all();  // budget freed
         cv_yield.notify_all();
     }
-    if (batch) cvl_batch_free(batch);
 }
 
 extern "C" {
@@ -244,7 +303,6 @@ void cvl_server_cfg_default(cvl_server_cfg *c) {
     c->device = 0;
     c->workers = 4;
     c->mem_budget_bytes = (size_t)40 << 30;
-    c->admit_bytes_per_edge = 2048;
     c->max_batch_edges = 2 << 20;
     c->large_map_edges = 1000000;
     c->host_reserve_bytes = (size_t)2 << 30;
@@ -252,6 +310,10 @@ void cvl_server_cfg_default(cvl_server_cfg *c) {
     c->large_workers = 0;
     c->large_yield_ms = 10;
     c->device_reserve_bytes = 0;
+    c->admit_bytes_per_edge = 0;
+    c->max_map_edges = 4 << 20;
+    c->pairs_per_edge = 40.0;
+    c->curvelets_per_edge = 8.0;
 }
 
 int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server **out) {
@@ -265,8 +327,11 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
     if (c.large_workers == 0) c.large_workers = std::max(1, c.workers / 2);
     if (c.workers >= 2 && c.large_workers >= c.workers) c.large_workers = c.workers - 1;
     if (c.large_workers < 1) return cvl_fail(CVL_EINVAL, "large_workers must be 0 (automatic) or in [1, workers - 1]");
-    if (c.mem_budget_bytes == 0 || c.admit_bytes_per_edge == 0 || c.max_batch_edges <= 0 || c.large_map_edges <= 0)
-        return cvl_fail(CVL_EINVAL, "budget, admission charge and batch sizes must be > 0");
+    if (c.mem_budget_bytes == 0 || c.max_batch_edges <= 0 || c.large_map_edges <= 0 || c.max_map_edges <= 0)
+        return cvl_fail(CVL_EINVAL, "budget, batch sizes and max_map_edges must be > 0");
+    if (!(c.pairs_per_edge >= 0.0 && c.pairs_per_edge <= 1024.0) ||
+        !(c.curvelets_per_edge >= 0.0 && c.curvelets_per_edge <= 1024.0))
+        return cvl_fail(CVL_EINVAL, "pairs_per_edge and curvelets_per_edge must be in [0, 1024]");
     cvl_server *s = new cvl_server();
     s->cfg = c;
     s->params = *p;
@@ -286,13 +351,25 @@ int cvl_server_create(const cvl_server_cfg *cfg, const cvl_params *p, cvl_server
             return cvl_fail(rc, msg);
         }
         s->engines.push_back(e);
-        // device memory for the largest launch the worker will fold (admission's model of
-        // the footprint), mapped now so that the stream never waits on a memory mapping
-        size_t dev_reserve = c.device_reserve_bytes;
-        if (!dev_reserve)
-            dev_reserve = std::min((size_t)c.max_batch_edges * c.admit_bytes_per_edge,
-                                   c.mem_budget_bytes / (size_t)c.workers);
-        int rr = cvl_engine_reserve_device(e, dev_reserve);
+        if (w == 0) {
+            for (int b = 0; b < CVL_TUNING_BUCKETS; ++b) cvl_engine_get_tuning(e, b, &s->tune[b]);
+        }
+        // The workspace of the largest launch the worker's lane takes, allocated now, so
+        // that the stream never waits on a memory mapping: max_batch_edges folded maps
+        // for a small-lane worker, the largest map for a large-lane one (which also takes
+        // small maps when its lane is empty); no more than the budget admits.
+        const bool takes_large = !small_lane || c.workers < 2 || c.small_takes_large;
+        const int64_t lane_edges = takes_large ? std::max(c.max_map_edges, c.max_batch_edges) : c.max_batch_edges;
+        const int64_t n_res = std::max<int64_t>(s->largest_admissible(std::min<int64_t>(lane_edges, 0x7fffffffLL)), 1);
+        const cvl_workspace_shape sh = s->shape_of(n_res, 4, MAX_MAPS_PER_LAUNCH);
+        size_t ws_total = 0;
+        int rr = cvl_engine_workspace_bytes(e, &sh, p, &ws_total, nullptr);
+        if (rr == CVL_OK) rr = cvl_engine_reserve_workspace(e, &sh, p);
+        cvl_batch *wb = nullptr;
+        if (rr == CVL_OK) rr = cvl_batch_create_reserved(e, n_res, MAX_MAPS_PER_LAUNCH, 4, &wb);
+        s->wbatch.push_back(wb);
+        s->reserved += ws_total;
+        if (rr == CVL_OK && c.device_reserve_bytes) rr = cvl_engine_reserve_device(e, c.device_reserve_bytes);
         if (rr == CVL_OK) rr = cvl_engine_reserve_host(e, c.host_reserve_bytes);
         if (rr != CVL_OK) {
             const std::string msg = cvl_last_error();
@@ -315,7 +392,10 @@ int cvl_server_submit(cvl_server *s, const double *edges, int32_t num_edges, int
     const Clock::time_point t_call = Clock::now();  // latency counts the copy below
     if (!s || !edges || !id) return cvl_fail(CVL_EINVAL, "server/edges/id is NULL");
     if (num_edges <= 0 || edge_data_sz < 4) return cvl_fail(CVL_EINVAL, "num_edges <= 0 or edge_data_sz < 4");
-    const size_t charge = (size_t)num_edges * s->cfg.admit_bytes_per_edge;
+    if (num_edges > s->cfg.max_map_edges)
+        return cvl_fail(CVL_ENOMEM, "a map of " + std::to_string(num_edges) + " edges is larger than max_map_edges (" +
+                                        std::to_string(s->cfg.max_map_edges) + ")");
+    const size_t charge = s->charge_of(num_edges, edge_data_sz);
     if (charge > s->cfg.mem_budget_bytes)
         return cvl_fail(CVL_ENOMEM, "a map of " + std::to_string(num_edges) + " edges needs " + std::to_string(charge) +
                                         " bytes of admission budget; the budget is " +
@@ -428,6 +508,7 @@ int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out) {
         st.device_ms = s->device_ms;
         st.result_ms = s->result_ms;
         st.queue_ms = s->queue_ms;
+        st.reserved_bytes = s->reserved;
         l = s->lat_ms;
     }
     st.host_grows = s->host.grows();
@@ -468,6 +549,14 @@ int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, uint64_t
     return n;
 }
 
+int64_t cvl_server_request_times(cvl_server *s, cvl_request_times *out, int64_t cap) {
+    if (!s || cap < 0 || (cap > 0 && !out)) return cvl_fail(CVL_EINVAL, "invalid arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int64_t n = std::min<int64_t>(cap, (int64_t)s->lat_times.size());
+    for (int64_t k = 0; k < n; ++k) out[k] = s->lat_times[k];
+    return n;
+}
+
 void cvl_server_destroy(cvl_server *s) {
     if (!s) return;
     {
@@ -493,7 +582,7 @@ void cvl_server_destroy(cvl_server *s) {
         if (kv.second->res) cvl_result_free(kv.second->res);
         delete kv.second;
     }
-    for (cvl_engine *e : s->engines) cvl_engine_destroy(e);
+    for (cvl_engine *e : s->engines) cvl_engine_destroy(e);  // frees each engine's batches too
     delete s;
 }
 

@@ -190,6 +190,16 @@ int cvl_build_curvelets(cvl_engine *e, const cvl_graph *g, const cvl_params *p, 
 int cvl_pair_bundles(cvl_engine *e, const double *pairs, int32_t n, const cvl_params *p,
                      double *bmin, double *bmax, uint8_t *valid, int32_t *cells);
 
+/* ---- failure injection (tests) ----------------------------------------
+ * No reference counterpart (the reference only prints errors,
+ * cpu_curvelet/data_io.hpp:27-76). From this call on, `after` more device or
+ * page-locked allocations of the library succeed, then every one fails as if
+ * the memory were exhausted (the call that needed it returns CVL_ENOMEM), until
+ * the next call; -1 turns it off. Host side only: nothing on the GPU fails.
+ * CVL_FAIL_ALLOC_AFTER=<after> in the environment arms it when the library
+ * loads. */
+int cvl_debug_fail_allocations(int64_t after);
+
 /* ---- checking entry points ------------------------------------------- */
 /* No reference counterpart: they exist so that tests can reach the device code of
  * the transport at chosen operands.
@@ -324,16 +334,27 @@ int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *counts, int3
  * A request's edges are copied at submit into page-locked memory that the
  * server reuses, and go from there to the device.
  *
- * Admission: a request holds admit_bytes_per_edge × its edges of the budget
- * from upload to result. A request that can never fit is refused at submit
- * with CVL_ENOMEM. One server serves one cvl_params. */
+ * Admission: a request holds its footprint of the budget from upload to result.
+ * The footprint is the device workspace of a launch of that map alone
+ * (cvl_engine_workspace_bytes), at pairs_per_edge and curvelets_per_edge, less the
+ * bundle chunk, which each worker holds once. With admit_bytes_per_edge set, the
+ * footprint is admit_bytes_per_edge x the map's edges instead. A request that can
+ * never fit (or has more than max_map_edges edges) is refused at submit with
+ * CVL_ENOMEM. One server serves one cvl_params.
+ *
+ * Memory: each worker reserves at creation the workspace of the largest launch
+ * its lane takes (cvl_engine_reserve_workspace): max_batch_edges edges for a
+ * small-lane worker, max_map_edges for a large-lane one, each at pairs_per_edge
+ * and curvelets_per_edge, never more than the budget admits. A launch within that
+ * shape allocates no device memory, so the stream never waits on a memory
+ * mapping; a launch beyond it grows the worker's workspace (device_grows). */
 typedef struct cvl_server cvl_server;
 typedef struct cvl_server_cfg {
     int device;                    /* CUDA device ordinal (0) */
     int workers;                   /* engines working concurrently (4) */
     size_t mem_budget_bytes;       /* device bytes that admitted requests may hold at once (40 GiB) */
-    size_t admit_bytes_per_edge;   /* admission charge per edge (2048: about twice the path's measured
-                                      footprint per edge, edges + hash + neighbour pairs + curvelets) */
+    size_t admit_bytes_per_edge;   /* 0: a request's footprint by the workspace formula above; else this
+                                      many bytes per edge (0) */
     int64_t max_batch_edges;       /* edges folded into one launch at most; a larger map runs alone (2 Mi) */
     int64_t large_map_edges;       /* maps with at least this many edges use the large lane (1,000,000) */
     size_t host_reserve_bytes;     /* page-locked host memory set aside at creation for each worker's results
@@ -347,10 +368,12 @@ typedef struct cvl_server_cfg {
                                       keep the small maps' within 22-38 ms) */
     int large_yield_ms;            /* a large-lane launch holds back between its chunks while small-lane
                                       work is queued or running, for at most this long each time; 0 = never (10) */
-    size_t device_reserve_bytes;   /* device memory each worker's engine maps ahead of time (its memory pool
-                                      keeps it), so that a launch larger than any before it grows its workspace
-                                      without mapping new memory mid-stream; 0 = max_batch_edges x
-                                      admit_bytes_per_edge, at most mem_budget_bytes / workers (0) */
+    size_t device_reserve_bytes;   /* extra device memory each worker's engine maps into its memory pool at
+                                      creation, for launches beyond the reserved workspace (0) */
+    int64_t max_map_edges;         /* largest map accepted, and the large-lane workspace's edges (4 Mi) */
+    double pairs_per_edge;         /* neighbour pairs per edge the footprint and the reservations assume (40;
+                                      the synthetic workloads average 16) */
+    double curvelets_per_edge;     /* curvelets per edge they assume (8; the synthetic workloads average 3) */
 } cvl_server_cfg;
 
 typedef struct cvl_server_stats {
@@ -374,6 +397,7 @@ typedef struct cvl_server_stats {
     double device_grow_ms;         /* host time of those calls */
     uint64_t host_grows;           /* page-locked chunks pinned: request staging and results */
     double host_grow_ms;           /* host time of those cudaMallocHost calls */
+    size_t reserved_bytes;         /* device workspace the workers reserved at creation */
 } cvl_server_stats;
 
 void cvl_server_cfg_default(cvl_server_cfg *cfg);
@@ -397,6 +421,19 @@ int cvl_server_stats_get(cvl_server *s, cvl_server_stats *out);
  * request, in completion order; returns how many were written (<= cap). ids
  * may be NULL. */
 int64_t cvl_server_latencies(cvl_server *s, double *ms, int64_t *edges, uint64_t *ids, int64_t cap);
+/* Where each completed request's time went, in completion order (host wall
+ * clock, ms): waiting to be taken into a launch; its launch's upload and run
+ * (cvl_batch_run, the path on the device); from the end of the run until its own
+ * rows were copied to its result. total_ms is submit -> result ready. Returns how
+ * many were written (<= cap). */
+typedef struct cvl_request_times {
+    uint64_t id;
+    int64_t edges;
+    double queue_ms, upload_ms, run_ms, result_ms, total_ms;
+    int32_t launch_maps;  /* maps folded into its launch */
+    int32_t worker;       /* the worker that ran it */
+} cvl_request_times;
+int64_t cvl_server_request_times(cvl_server *s, cvl_request_times *out, int64_t cap);
 /* Finishes the requests already admitted, drops the queued ones, stops the
  * workers and releases everything. */
 void cvl_server_destroy(cvl_server *s);
@@ -445,6 +482,39 @@ int cvl_engine_set_tuning(cvl_engine *e, int bucket, const cvl_tuning *t);
  * and its time to *best_ms. The batch's results are not kept. */
 int cvl_engine_autotune(cvl_engine *e, const cvl_batch *b, const cvl_params *p, int passes, cvl_tuning *best,
                         double *best_ms);
+
+/* ---- workspace by shape ------------------------------------------------
+ * No reference counterpart (the reference allocates its worst case,
+ * N (max_degree + 1) 2 output rows, per run: cpu_curvelet.hpp:59-67). The
+ * engine sizes its device workspace to each launch: buffers grow when a launch
+ * needs more than any before it, and are kept. The shape of a launch is what
+ * decides the sizes: */
+typedef struct cvl_workspace_shape {
+    int64_t num_edges;      /* edges of the launch, all maps together */
+    int64_t num_pairs;      /* neighbour pairs (total_neighbor_pairs) */
+    int64_t num_curvelets;  /* curvelets written (at most num_pairs: each seed grows at most one) */
+    int32_t num_maps;       /* maps folded into the launch */
+    int32_t edge_data_sz;   /* values per edge row (4) */
+} cvl_workspace_shape;
+/* Device bytes of the workspace a launch of that shape takes on this engine (its
+ * tuning sets the bundle chunk), the launch's input rows included, in *total; of
+ * that, the one bundle chunk a launch holds whatever its maps, in *per_launch
+ * (may be NULL). */
+int cvl_engine_workspace_bytes(cvl_engine *e, const cvl_workspace_shape *s, const cvl_params *p, size_t *total,
+                               size_t *per_launch);
+/* Allocates the workspace of that shape now, so that later runs within it (edges,
+ * pairs, curvelets and maps at most the shape's) allocate no device memory: cvl_run
+ * and cvl_batch_run (a batch holds its own rows: cvl_batch_refill reuses a buffer
+ * large enough). */
+int cvl_engine_reserve_workspace(cvl_engine *e, const cvl_workspace_shape *s, const cvl_params *p);
+/* The engine's device memory: bytes its workspace and batches hold, and the
+ * allocations made so far with their host time. */
+typedef struct cvl_engine_memory {
+    size_t held_bytes;
+    uint64_t device_grows;
+    double device_grow_ms;
+} cvl_engine_memory;
+int cvl_engine_memory_get(cvl_engine *e, cvl_engine_memory *out);
 
 /* Writes a buffer larger than the L2 cache on the engine's stream and waits
  * (timing hygiene between benchmark iterations). */

@@ -23,7 +23,13 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_DIR = "/root/reference/test_files"
+# the reference project's sample inputs: $CVL_REFERENCE_DIR/test_files
+REF_DIR = os.path.join(os.environ.get("CVL_REFERENCE_DIR", ""), "test_files")
+
+
+def _need_reference() -> None:
+    if not os.path.isdir(REF_DIR) or not os.environ.get("CVL_REFERENCE_DIR"):
+        raise SystemExit("set CVL_REFERENCE_DIR to the reference project's root (it holds test_files/)")
 REF_CLI = os.path.join(ROOT, "oracle", "_ref", "CURVELET")
 FILES = {"TO_edges_digit1": "full", "TO_edges_ABC_0006_thresh1": "full", "TO_edges": "digest"}
 
@@ -45,6 +51,7 @@ def run_reference(name: str, work: str, scalar: str = "--double") -> tuple[bytes
 
 
 def main() -> None:
+    _need_reference()
     if not os.path.exists(REF_CLI):
         sys.exit("oracle/_ref/CURVELET is not built (make -C oracle)")
     out = {}

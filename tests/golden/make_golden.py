@@ -32,7 +32,13 @@ sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
 REF_FILES = ["TO_edges_digit1.txt", "TO_edges_ABC_0006_thresh1.txt", "TO_edges.txt"]
-REF_DIR = "/root/reference/test_files"
+# the reference project's sample inputs: $CVL_REFERENCE_DIR/test_files
+REF_DIR = os.path.join(os.environ.get("CVL_REFERENCE_DIR", ""), "test_files")
+
+
+def _need_reference() -> None:
+    if not os.path.isdir(REF_DIR) or not os.environ.get("CVL_REFERENCE_DIR"):
+        raise SystemExit("set CVL_REFERENCE_DIR to the reference project's root (it holds test_files/)")
 
 
 def digest(a: np.ndarray) -> str:
@@ -79,6 +85,7 @@ def kat_maps() -> dict[str, tuple[np.ndarray, dict]]:
 
 
 def main() -> None:
+    _need_reference()
     O.build()
     if not O.ref_available():
         raise SystemExit("reference harness not built (needs the reference sources)")

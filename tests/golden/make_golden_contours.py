@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
 from curvelet_construction_on_gpu_b200 import synth  # noqa: E402
-from make_golden import REF_DIR, REF_FILES  # noqa: E402
+from make_golden import REF_DIR, REF_FILES, _need_reference  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
 FILE_PARAMS = [(4, 1.5), (2, 1.5), (3, 2.0), (4, 1.0)]
@@ -56,6 +56,7 @@ def put(out: dict, key: str, c, full: bool) -> None:
 
 
 def main() -> None:
+    _need_reference()
     O.build()
     if not (O.ref_available() and O.orig_available()):
         raise SystemExit("reference harnesses not built (make -C oracle; needs the reference sources)")

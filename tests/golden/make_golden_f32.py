@@ -26,11 +26,12 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from make_golden import REF_DIR, REF_FILES, digest, kat_maps  # noqa: E402
+from make_golden import REF_DIR, REF_FILES, _need_reference, digest, kat_maps  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
 
 def main() -> None:
+    _need_reference()
     O.build()
     if not O.ref_available():
         raise SystemExit("reference harness not built (needs the reference sources)")

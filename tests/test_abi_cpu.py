@@ -95,9 +95,11 @@ def test_server_defaults_and_argument_checks():
     cfg = _abi.CvlServerCfg()
     lib.cvl_server_cfg_default(C.byref(cfg))
     assert (cfg.device, cfg.workers, cfg.mem_budget_bytes) == (0, 4, 40 << 30)
-    assert (cfg.admit_bytes_per_edge, cfg.max_batch_edges, cfg.large_map_edges) == (2048, 2 << 20, 1_000_000)
+    # admission by the workspace formula (admit_bytes_per_edge 0)
+    assert (cfg.admit_bytes_per_edge, cfg.max_batch_edges, cfg.large_map_edges) == (0, 2 << 20, 1_000_000)
     assert cfg.host_reserve_bytes == 2 << 30 and cfg.small_takes_large == 0 and cfg.large_workers == 0
     assert cfg.large_yield_ms == 10 and cfg.device_reserve_bytes == 0
+    assert (cfg.max_map_edges, cfg.pairs_per_edge, cfg.curvelets_per_edge) == (4 << 20, 40.0, 8.0)
     ec = _abi.CvlEngineCfg()
     lib.cvl_engine_cfg_default(C.byref(ec))
     assert ec.stream_priority == 0
@@ -108,6 +110,13 @@ def test_server_defaults_and_argument_checks():
     lib.cvl_server_cfg_default(C.byref(bad))
     bad.workers = 0
     assert lib.cvl_server_create(C.byref(bad), C.byref(p), C.byref(h)) == _abi.CVL_EINVAL
+    lib.cvl_server_cfg_default(C.byref(bad))
+    bad.pairs_per_edge = -1.0
+    assert lib.cvl_server_create(C.byref(bad), C.byref(p), C.byref(h)) == _abi.CVL_EINVAL
+    shp = _abi.CvlWorkspaceShape(1000, 16000, 3000, 1, 4)
+    tot = C.c_size_t(0)
+    assert lib.cvl_engine_workspace_bytes(None, C.byref(shp), C.byref(p), C.byref(tot), None) == _abi.CVL_EINVAL
+    assert lib.cvl_engine_reserve_workspace(None, C.byref(shp), C.byref(p)) == _abi.CVL_EINVAL
     rid = C.c_uint64(0)
     assert lib.cvl_server_submit(None, None, 1, 4, C.byref(rid)) == _abi.CVL_EINVAL
     assert lib.cvl_server_wait(None, 1, 0, C.byref(h)) == _abi.CVL_EINVAL
@@ -127,3 +136,11 @@ def test_tuning_buckets():
     t = _abi.CvlTuning()
     assert lib.cvl_engine_set_tuning(None, 0, C.byref(t)) == _abi.CVL_EINVAL
     assert lib.cvl_engine_get_tuning(None, 0, C.byref(t)) == _abi.CVL_EINVAL
+
+
+def test_allocation_injector_arms_and_disarms():
+    """The injector is host state: arming and disarming need no device."""
+    lib = _abi.load()
+    assert lib.cvl_debug_fail_allocations(5) == _abi.CVL_OK
+    assert lib.cvl_debug_fail_allocations(-1) == _abi.CVL_OK
+    assert lib.cvl_debug_fail_allocations(-2) == _abi.CVL_EINVAL

@@ -106,3 +106,48 @@ def test_server_next_hands_out_in_completion_order(engine):
     assert sorted(seen) == sorted(ids)
     for rid, m in zip(ids, maps):
         _same(engine.run(m), seen[rid])
+
+
+def test_engine_reserved_workspace_runs_without_allocation():
+    """cvl_engine_reserve_workspace: runs within the reserved shape allocate no
+    device memory, and give the same results as an engine that grew on demand."""
+    maps = [synth.plain_small(0), synth.plain_hd(1000), synth.mixed_map(2004), synth.plain_small(3)]
+    n = max(m.shape[0] for m in maps)
+    with cvl.Engine() as grown, cvl.Engine() as eng:
+        tot, chunk = eng.workspace_bytes(n, 40 * n, 8 * n)
+        eng.reserve_workspace(n, 40 * n, 8 * n)
+        m0 = eng.memory()
+        assert m0["held_bytes"] >= tot - (1 << 20), (m0, tot)
+        for m in maps:
+            _same(grown.run(m), eng.run(m))
+        m1 = eng.memory()
+    assert m1["device_grows"] == m0["device_grows"], (m0, m1)
+    print(f"[reserve] {n} edges: workspace {tot / 2**30:.2f} GiB (bundle chunk {chunk / 2**30:.2f} GiB), "
+          f"{len(maps)} runs, no allocation")
+
+
+def test_server_stream_allocates_no_device_memory(engine):
+    """The default server reserves each worker's workspace at creation: a Poisson
+    stream over every size class, a 3.79M-edge map included, then runs with no
+    device allocation (device_grows unchanged after creation), and its results
+    equal the maps run alone."""
+    import time
+    big = synth.mixed_map(2038)  # 3,791,782 edges: the largest map of the 64-map batch
+    small = [synth.plain_small(s) for s in range(6)]
+    mid = [synth.mixed_map(s) for s in (2000, 2004, 2005)] + [synth.plain_hd(1000)]
+    maps = small + mid + [synth.dense_4k(4000), big] + small[:3]
+    rng = np.random.default_rng(3)
+    with cvl.Server() as srv:
+        st0 = srv.stats()
+        ids = []
+        for k in rng.permutation(len(maps)):
+            ids.append((k, srv.submit(maps[k])))
+            time.sleep(float(rng.exponential(0.02)))
+        got = {k: srv.wait(i, timeout_s=300.0) for k, i in ids}
+        st = srv.stats()
+    assert st["completed"] == len(maps) and st["failed"] == 0
+    assert st["device_grows"] == st0["device_grows"], (st0["device_grows"], st["device_grows"])
+    for k in range(len(small) + len(mid)):
+        _same(engine.run(maps[k]), got[k])
+    print(f"[server] reserved {st['reserved_bytes'] / 2**30:.1f} GiB at creation; {len(maps)} maps, "
+          f"{st['launches']} launches, device allocations in the stream: {st['device_grows'] - st0['device_grows']}")
