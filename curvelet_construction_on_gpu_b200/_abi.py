@@ -83,6 +83,11 @@ class CvlRequestTimes(C.Structure):
                 ("launch_maps", C.c_int32), ("worker", C.c_int32)]
 
 
+class CvlEngineGraphs(C.Structure):
+    _fields_ = [("enabled", C.c_int32), ("graphs", C.c_int32), ("captures", C.c_uint64), ("replays", C.c_uint64),
+                ("fallbacks", C.c_uint64)]
+
+
 class CvlEngineMemory(C.Structure):
     _fields_ = [("held_bytes", C.c_size_t), ("device_grows", C.c_uint64), ("device_grow_ms", C.c_double)]
 
@@ -145,6 +150,8 @@ SIGNATURES = [
                                             C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("cvl_engine_reserve_workspace", C.c_int, [_vp, C.POINTER(CvlWorkspaceShape), C.POINTER(CvlParams)]),
     ("cvl_engine_memory_get", C.c_int, [_vp, C.POINTER(CvlEngineMemory)]),
+    ("cvl_engine_set_graphs", C.c_int, [_vp, C.c_int]),
+    ("cvl_engine_graph_stats", C.c_int, [_vp, C.POINTER(CvlEngineGraphs)]),
     ("cvl_debug_fail_allocations", C.c_int, [C.c_int64]),
     ("cvl_check_pair_bundles_literal", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), _dp, _dp,
                                                  C.POINTER(C.c_uint8), C.POINTER(C.c_int32)]),

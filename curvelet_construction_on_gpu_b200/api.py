@@ -437,6 +437,16 @@ class Engine:
         check(self._lib.cvl_engine_reserve_workspace(self._h, C.byref(shp), C.byref(p)),
               "cvl_engine_reserve_workspace")
 
+    def set_graphs(self, enable: bool) -> None:
+        """cvl_engine_set_graphs: replay a CUDA graph per size bucket (default) or launch kernel by kernel."""
+        check(self._lib.cvl_engine_set_graphs(self._h, 1 if enable else 0), "cvl_engine_set_graphs")
+
+    def graph_stats(self) -> dict:
+        """cvl_engine_graph_stats: enabled, graphs, captures, replays, fallbacks."""
+        g = _abi.CvlEngineGraphs()
+        check(self._lib.cvl_engine_graph_stats(self._h, C.byref(g)), "cvl_engine_graph_stats")
+        return {name: getattr(g, name) for name, _ in g._fields_}
+
     def memory(self) -> dict:
         """cvl_engine_memory_get: held_bytes, device_grows, device_grow_ms."""
         m = _abi.CvlEngineMemory()

@@ -153,6 +153,22 @@ struct cvl_engine {
         }
     } cw;
 
+    // CUDA graphs of the path for the small size buckets: each captured once for a
+    // key (parameters, buffers, input pointers) and replayed for every run whose sizes
+    // fit the bucket's capacities (the kernels read the run's sizes on the device)
+    struct GraphSlot {
+        std::string key;
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;
+        uint64_t last_use = 0;
+    };
+    std::vector<GraphSlot> graphs;
+    bool graphs_on = std::getenv("CVL_NO_GRAPHS") == nullptr;
+    uint64_t ws_epoch = 0;                         // workspace (re)allocations so far
+    uint64_t graph_replays = 0, graph_fallbacks = 0, graph_captures = 0, graph_clock = 0;
+    DBuf gdims, gchunks, gread;
+    unsigned char *gread_host = nullptr;           // page-locked: the runs' sizes and the readback
+
     // per-kernel timing of the last run
     std::vector<const char *> mark_names;
     std::vector<cudaEvent_t> marks;
@@ -191,6 +207,7 @@ struct cvl_engine {
         }
         b.bytes = want;
         held += want;
+        ++ws_epoch;
         return CVL_OK;
     }
 
@@ -230,7 +247,7 @@ struct cvl_engine {
                        &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
                        &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
                        &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &pslot, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
-                       &pb_max, &pb_valid, &chains_alt, &info_alt};
+                       &pb_max, &pb_valid, &chains_alt, &info_alt, &gdims, &gchunks, &gread};
         for (DBuf *b : all) {
             if (b->p) cudaFreeAsync(b->p, stream);
             b->p = nullptr;
@@ -489,8 +506,10 @@ int launch_bundles(cvl_engine *e, BundleArgsT<T> &a, int blocks) {
     // higher-priority stream's blocks get SMs as soon as any block ends
     constexpr int pair_bytes = 2 * 32 * CPL * (int)sizeof(T);
     const long long ppb = bundles_pairs_per_block(a.md.Q, pair_bytes);
-    const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
-    blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
+    if (!a.cd) {  // a graph run (device-side range) keeps the given grid, which strides over the pairs
+        const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
+        blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
+    }
     k_bundles<T, CPL, MINB><<<blocks, BUNDLE_THREADS, (size_t)ppb * pair_bytes, e->stream>>>(a);
     return check_launch("k_bundles");
 }
@@ -498,11 +517,13 @@ int launch_bundles(cvl_engine *e, BundleArgsT<T> &a, int blocks) {
 template <typename T, int CPL, int K, int MINB>
 int launch_growth(cvl_engine *e, GrowthArgsT<T> &a, size_t smem, int blocks) {
     CVL_CUDA(cudaFuncSetAttribute(k_growth<T, CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    // a warp per anchor and anchors_per_warp anchors per warp: short blocks (a
-    // higher-priority stream's blocks get SMs as soon as any block ends)
-    const long long per_block = (GROWTH_THREADS / 32) * (long long)a.anchors_per_warp;
-    blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + per_block - 1) / per_block,
-                                                    0x7fffffffLL));
+    if (!a.cd) {  // a graph run (device-side range) keeps the given grid, which strides over the anchors
+        // a warp per anchor and anchors_per_warp anchors per warp: short blocks (a
+        // higher-priority stream's blocks get SMs as soon as any block ends)
+        const long long per_block = (GROWTH_THREADS / 32) * (long long)a.anchors_per_warp;
+        blocks = (int)std::max(1LL, std::min<long long>(((long long)a.a_end - a.a_begin + per_block - 1) / per_block,
+                                                        0x7fffffffLL));
+    }
     k_growth<T, CPL, K, MINB><<<blocks, GROWTH_THREADS, smem, e->stream>>>(a);
     return check_launch("k_growth");
 }
@@ -550,7 +571,7 @@ void pick_kernels(int cpl, const cvl_tuning &t, bundles_fn<double> &bf, growth_f
 
 // mode: 0 = full run, 1 = count valid pairs only, 2 = neighbour graph only
 template <typename R>
-int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_map_off,
+int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_map_off,
                  const std::vector<int32_t> &map_off_host, ModelT<R> md, int cpl, int mode, bool want_d2,
                  RunOut &ro) {
     const int M = (int)map_off_host.size() - 1;
@@ -621,11 +642,12 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     // ---- (a) binning
     const int gb = short_grid(n, 256);
     k_bin_keys<<<gb, 256, 0, s>>>(d_edges, sz, n, d_map_off, M, md, (unsigned *)e->ehash.p, (unsigned *)e->bcount.p,
-                                  err);
+                                  err, nullptr);
     CVL_TRY(check_launch("k_bin_keys"));
     CVL_TRY((scan<unsigned, unsigned>(e, (const unsigned *)e->bcount.p, T, (unsigned *)e->bstart.p)));
     k_bin_scatter<<<gb, 256, 0, s>>>(d_edges, sz, n, d_map_off, M, md, (const unsigned *)e->ehash.p,
-                                     (const unsigned *)e->bstart.p, (unsigned *)e->bfill.p, B, (int *)e->pos_of.p);
+                                     (const unsigned *)e->bstart.p, (unsigned *)e->bfill.p, B, (int *)e->pos_of.p,
+                                     nullptr);
     CVL_TRY(check_launch("k_bin_scatter"));
     e->mark("bin");
 
@@ -647,7 +669,7 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     na.err = err;
     k_nb<R, NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
     CVL_TRY(check_launch("k_nb<COUNT>"));
-    k_deg_from_ncand<<<gb, 256, 0, s>>>(n, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p);
+    k_deg_from_ncand<<<gb, 256, 0, s>>>(n, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p, nullptr);
     CVL_TRY(check_launch("k_deg_from_ncand"));
     CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->deg.p, n,
                                                 (unsigned long long *)e->pair_off.p)));
@@ -657,7 +679,7 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
     CVL_TRY(e->alloc(e->chunk_start, sizeof(int) * (max_chunks + 1)));
     CVL_CUDA(cudaMemsetAsync(e->chunk_start.p, 0, sizeof(int) * (max_chunks + 1), s));
     k_chunk_starts<<<gb, 256, 0, s>>>(n, (const unsigned long long *)e->pair_off.p + 1, per_chunk, max_chunks,
-                                     (int *)e->chunk_start.p);
+                                     (int *)e->chunk_start.p, nullptr);
     CVL_TRY(check_launch("k_chunk_starts"));
     e->mark("neighbors_count");
 
@@ -840,7 +862,7 @@ int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_ma
         CVL_TRY(e->alloc(e->info, sizeof(double) * C * 10));
         k_finalize<R><<<gb, 256, 0, s>>>(md, d_edges, sz, n, d_map_off, M, rec, (const unsigned *)e->rec_base.p,
                                       (const unsigned *)e->run_cnt.p, (const unsigned long long *)e->out_off.p, C,
-                                      (unsigned *)e->chains.p, (double *)e->info.p);
+                                      (unsigned *)e->chains.p, (double *)e->info.p, nullptr);
         CVL_TRY(check_launch("k_finalize"));
         e->mark("finalize");
         return CVL_OK;
@@ -928,6 +950,334 @@ std::vector<WsItem> workspace_plan(const cvl_tuning *tune, unsigned long long ar
 }
 
 inline size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// ---- the path as a CUDA graph, one per size bucket ---------------------------------
+// Runs of up to 64 Ki edges (bucket 0) and 512 Ki edges (bucket 1) replay a graph
+// captured for the bucket's capacities: every kernel is launched for the bucket's
+// edges, maps and bundle chunks and reads the run's own sizes (RunDims) and chunk
+// ranges (ChunkDims, computed on the device) from device memory, so that one graph
+// serves every run of the bucket, with one host synchronisation at its end instead
+// of the direct path's three. A run that exceeds a capacity (more pairs than the
+// bucket's chunks hold, more curvelets than its outputs, a record-arena overflow)
+// is flagged on the device and run again by the direct path, with the same results.
+struct GraphCaps {
+    int N;  // edges
+    int M;  // maps
+    int K;  // bundle chunks
+    int curvelets_per_edge;
+};
+constexpr GraphCaps GRAPH_CAPS[2] = {{64 << 10, 4096, 2, 8}, {512 << 10, 4096, 8, 8}};
+constexpr size_t GRAPH_SLOTS = 6;  // captured graphs kept per engine (least recently used goes)
+
+size_t graph_readback_bytes() {
+    // totals + per-map curvelet offsets, per-map statistics, error bits
+    return (size_t)(2 + GRAPH_CAPS[1].M + 1) * 8 + sizeof(MapStats) * (size_t)GRAPH_CAPS[1].M + 16;
+}
+
+// CVL_OK with ro filled; CVL_EAGAIN when the run is not for a graph or did not fit
+// (the caller runs the direct path); another status on a real error.
+int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, const int *d_map_off,
+                       const std::vector<int32_t> &map_off_host, Model md, int cpl, RunOut &ro) {
+    const int M = (int)map_off_host.size() - 1;
+    const int b = bucket_of(n);
+    if (!e->graphs_on || g_sync_check || b > 1) return CVL_EAGAIN;
+    const GraphCaps cap = GRAPH_CAPS[b];
+    if (n > cap.N || M > cap.M) return CVL_EAGAIN;
+    cudaStream_t s = e->stream;
+    const cvl_tuning &tn = e->tune[b];
+    md.sbits = tn.cell_size == 2 ? 1 : (tn.cell_size == 8 ? 3 : 2);
+    const unsigned T = next_pow2(std::max<unsigned long long>((unsigned long long)cap.N, 1024ull));
+    md.hash_mask = T - 1;
+    const unsigned long long per_chunk = std::max<unsigned long long>((unsigned long long)tn.chunk_pairs, 1024ull);
+
+    // the workspace at the bucket's capacities (no-ops once it is there)
+    cvl_workspace_shape sh;
+    sh.num_edges = cap.N;
+    sh.num_pairs = (int64_t)(per_chunk * (unsigned long long)cap.K);
+    sh.num_curvelets = (int64_t)cap.N * cap.curvelets_per_edge;
+    sh.num_maps = cap.M;
+    sh.edge_data_sz = sz;
+    // (the input rows and map offsets are the caller's, already in place: they are
+    // not reallocated here)
+    for (const WsItem &w : workspace_plan(e->tune, e->arena_hint, md, cpl, sh)) {
+        if (w.buf == &cvl_engine::edges || w.buf == &cvl_engine::map_off) continue;
+        CVL_TRY(e->alloc(e->*(w.buf), w.bytes));
+    }
+    CVL_TRY(e->alloc(e->gdims, sizeof(RunDims)));
+    CVL_TRY(e->alloc(e->gchunks, sizeof(ChunkDims) * (size_t)cap.K));
+    CVL_TRY(e->alloc(e->gread, (size_t)(2 + cap.M + 1) * 8));
+    if (!e->gread_host) {
+        void *h = nullptr;
+        if (cvl_alloc_fault_injected() || cudaMallocHost(&h, graph_readback_bytes() + sizeof(RunDims) + 64) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CVL_ENOMEM, "page-locked graph readback could not be allocated");
+        }
+        e->gread_host = (unsigned char *)h;
+    }
+    const unsigned long long C_cap = (unsigned long long)sh.num_curvelets;
+    const unsigned long long nchunks_cap = (unsigned long long)cap.K;
+    const unsigned long long arena_cap =
+        std::max<unsigned long long>(std::max<unsigned long long>(e->arena_hint, C_cap), 4ull * cap.N + 4096ull) +
+        (unsigned long long)cap.N + (unsigned long long)GROWTH_ARENA_CHUNK * (nchunks_cap + 1);
+    unsigned long long *rb_h = (unsigned long long *)e->gread_host;
+    MapStats *stats_h = (MapStats *)(e->gread_host + (size_t)(2 + cap.M + 1) * 8);
+    unsigned *err_h = (unsigned *)((unsigned char *)stats_h + sizeof(MapStats) * (size_t)cap.M);
+    RunDims *dims_h = (RunDims *)(e->gread_host + graph_readback_bytes() + 32);
+
+    // what the graph is captured for
+    std::string key((const char *)&md, sizeof(md));
+    const void *ptrs[] = {d_edges, d_map_off, e->chains.p, e->info.p};
+    key.append((const char *)ptrs, sizeof(ptrs));
+    const unsigned long long nums[] = {(unsigned long long)b, (unsigned long long)sz, (unsigned long long)cpl,
+                                       e->ws_epoch, arena_cap, per_chunk};
+    key.append((const char *)nums, sizeof(nums));
+    key.append((const char *)&tn, sizeof(tn));
+    cvl_engine::GraphSlot *slot = nullptr;
+    for (auto &g : e->graphs)
+        if (g.key == key) slot = &g;
+
+    e->nmarks = 0;
+    ++e->generation;
+    g_launches = 0;
+    if (!slot) {
+        bundles_fn<double> bf;
+        growth_fn<double> gf;
+        pick_kernels(cpl, tn, bf, gf);
+        const int nb_wpb = 8;
+        const size_t nb_smem = (size_t)nb_wpb * nbr_smem_per_warp(md.max_cand);
+        CVL_CUDA(cudaFuncSetAttribute(k_nb<double, NB_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
+        CVL_CUDA(cudaFuncSetAttribute(k_nb<double, NB_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nb_smem));
+        const size_t gsmem = (size_t)(GROWTH_THREADS / 32) * growth_smem_per_warp(md.max_cand, md.gms);
+        BinnedT<double> B;
+        B.x = (double *)e->bx.p;
+        B.y = (double *)e->by.p;
+        B.th = (double *)e->bth.p;
+        B.sp = (double *)e->bsp.p;
+        B.cp = (double *)e->bcp.p;
+        B.sm = (double *)e->bsm.p;
+        B.cm = (double *)e->bcm.p;
+        B.cell = (int2 *)e->bcell.p;
+        B.orig = (int *)e->orig_of.p;
+        B.map = (int *)e->bmap.p;
+        unsigned *err = (unsigned *)e->err.p;
+        MapStats *stats = (MapStats *)e->stats.p;
+        unsigned long long *arena_ctr = (unsigned long long *)e->work.p;
+        unsigned *slot_ctr = (unsigned *)((unsigned long long *)e->work.p + 2);
+        const RunDims *dd = (const RunDims *)e->gdims.p;
+        ChunkDims *cdp = (ChunkDims *)e->gchunks.p;
+        const int sms = e->prop.multiProcessorCount;
+        const int N = cap.N;
+        CVL_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        auto enqueue = [&]() -> int {
+            CVL_CUDA(cudaMemsetAsync(e->bcount.p, 0, sizeof(unsigned) * (T + 1), s));
+            CVL_CUDA(cudaMemsetAsync(e->bfill.p, 0, sizeof(unsigned) * (T + 1), s));
+            CVL_CUDA(cudaMemsetAsync(e->stats.p, 0, sizeof(MapStats) * cap.M, s));
+            CVL_CUDA(cudaMemsetAsync(e->err.p, 0, 16, s));
+            CVL_CUDA(cudaMemsetAsync(e->work.p, 0, 32, s));
+            CVL_CUDA(cudaMemsetAsync(e->count.p, 0, sizeof(unsigned) * N, s));
+            CVL_CUDA(cudaMemsetAsync(e->chunk_start.p, 0, sizeof(int) * (cap.K + 1), s));
+            const int gb = short_grid(N, 256);
+            k_bin_keys<<<gb, 256, 0, s>>>(d_edges, sz, N, d_map_off, cap.M, md, (unsigned *)e->ehash.p,
+                                          (unsigned *)e->bcount.p, err, dd);
+            CVL_TRY(check_launch("k_bin_keys"));
+            CVL_TRY((scan<unsigned, unsigned>(e, (const unsigned *)e->bcount.p, T, (unsigned *)e->bstart.p)));
+            k_bin_scatter<<<gb, 256, 0, s>>>(d_edges, sz, N, d_map_off, cap.M, md, (const unsigned *)e->ehash.p,
+                                             (const unsigned *)e->bstart.p, (unsigned *)e->bfill.p, B,
+                                             (int *)e->pos_of.p, dd);
+            CVL_TRY(check_launch("k_bin_scatter"));
+            NbArgsT<double> na{};
+            na.md = md;
+            na.B = B;
+            na.bstart = (const unsigned *)e->bstart.p;
+            na.N = N;
+            na.M = cap.M;
+            na.ncand = (unsigned *)e->ncand.p;
+            na.stats = stats;
+            na.pair_off = (const unsigned long long *)e->pair_off.p;
+            na.err = err;
+            na.dims = dd;
+            na.pair_cap = (unsigned long long)sh.num_pairs;
+            const int gn = std::min(short_grid(N, (long long)nb_wpb * 4), sms * 8);
+            k_nb<double, NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+            CVL_TRY(check_launch("k_nb<COUNT>"));
+            k_deg_from_ncand<<<gb, 256, 0, s>>>(N, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p, dd);
+            CVL_TRY(check_launch("k_deg_from_ncand"));
+            CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->deg.p, N,
+                                                        (unsigned long long *)e->pair_off.p)));
+            k_chunk_starts<<<gb, 256, 0, s>>>(N, (const unsigned long long *)e->pair_off.p + 1, per_chunk, cap.K,
+                                             (int *)e->chunk_start.p, dd);
+            CVL_TRY(check_launch("k_chunk_starts"));
+            k_chunk_dims<<<1, 32, 0, s>>>(dd, (const unsigned long long *)e->pair_off.p, (const int *)e->chunk_start.p,
+                                          per_chunk, cap.K, cdp, err);
+            CVL_TRY(check_launch("k_chunk_dims"));
+            na.csr_ids = (int *)e->csr_ids.p;
+            na.csr_d2 = nullptr;
+            na.pcls = (unsigned char *)e->pcls.p;
+            na.pair_anchor = (int *)e->pair_anchor.p;
+            na.atrig = (double *)e->atrig.p;
+            k_nb<double, NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+            CVL_TRY(check_launch("k_nb<FILL>"));
+            k_cell_ranks<double><<<1, 128, 0, s>>>(md, (unsigned short *)e->crank.p);
+            CVL_TRY(check_launch("k_cell_ranks"));
+            Records rec;
+            rec.ids = (unsigned *)e->rec_ids.p;
+            rec.k = (double *)e->rec_k.p;
+            rec.meta = (unsigned *)e->rec_meta.p;
+            for (int c = 0; c < cap.K; ++c) {
+                CVL_CUDA(cudaMemsetAsync(slot_ctr, 0, sizeof(unsigned), s));
+                BundleArgsT<double> ba{};
+                ba.md = md;
+                ba.B = B;
+                ba.csr_ids = (const int *)e->csr_ids.p;
+                ba.pair_anchor = (const int *)e->pair_anchor.p;
+                ba.pcls = (const unsigned char *)e->pcls.p;
+                ba.atrig = (const double *)e->atrig.p;
+                ba.bund = (double *)e->bund.p;
+                ba.pslot = (unsigned *)e->pslot.p;
+                ba.slot_ctr = slot_ctr;
+                ba.pflag = (unsigned char *)e->pflag.p;
+                ba.cd = cdp + c;
+                CVL_TRY(bf(e, ba, sms * 16));
+                GrowthArgsT<double> ga{};
+                ga.md = md;
+                ga.B = B;
+                ga.M = cap.M;
+                ga.pair_off = (const unsigned long long *)e->pair_off.p;
+                ga.csr_ids = (const int *)e->csr_ids.p;
+                ga.pcls = (const unsigned char *)e->pcls.p;
+                ga.pflag = (const unsigned char *)e->pflag.p;
+                ga.bund = (const double *)e->bund.p;
+                ga.pslot = (const unsigned *)e->pslot.p;
+                ga.rec = rec;
+                ga.arena_cap = arena_cap;
+                ga.arena_ctr = arena_ctr;
+                ga.rec_base = (unsigned *)e->rec_base.p;
+                ga.run_cnt = (unsigned *)e->run_cnt.p;
+                ga.count = (unsigned *)e->count.p;
+                ga.stats = stats;
+                ga.count_only = 0;
+                ga.err = err;
+                ga.cell_rank = (const unsigned short *)e->crank.p;
+                // one arena record per curvelet, no chunk tails: the strided warps take
+                // few anchors each
+                ga.anchors_per_warp = 1;
+                ga.cd = cdp + c;
+                CVL_TRY(gf(e, ga, gsmem, sms * 24));
+            }
+            CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->count.p, N,
+                                                        (unsigned long long *)e->out_off.p)));
+            k_finalize<double><<<gb, 256, 0, s>>>(md, d_edges, sz, N, d_map_off, cap.M, rec,
+                                                  (const unsigned *)e->rec_base.p, (const unsigned *)e->run_cnt.p,
+                                                  (const unsigned long long *)e->out_off.p, C_cap,
+                                                  (unsigned *)e->chains.p, (double *)e->info.p, dd);
+            CVL_TRY(check_launch("k_finalize"));
+            k_graph_readback<<<(cap.M + 1 + 255) / 256, 256, 0, s>>>(dd, (const unsigned long long *)e->pair_off.p,
+                                                                     (const unsigned long long *)e->out_off.p,
+                                                                     d_map_off, (unsigned long long *)e->gread.p);
+            CVL_TRY(check_launch("k_graph_readback"));
+            CVL_CUDA(cudaMemcpyAsync(rb_h, e->gread.p, (size_t)(2 + cap.M + 1) * 8, cudaMemcpyDeviceToHost, s));
+            CVL_CUDA(cudaMemcpyAsync(stats_h, e->stats.p, sizeof(MapStats) * cap.M, cudaMemcpyDeviceToHost, s));
+            CVL_CUDA(cudaMemcpyAsync(err_h, e->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            return CVL_OK;
+        };
+        const int rc = enqueue();
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        if (rc != CVL_OK || ce != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            if (rc != CVL_OK) return rc;
+            return fail(CVL_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        }
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CVL_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        }
+        if (e->graphs.size() >= GRAPH_SLOTS) {
+            auto lru = std::min_element(e->graphs.begin(), e->graphs.end(),
+                                        [](const auto &a, const auto &b2) { return a.last_use < b2.last_use; });
+            cudaGraphExecDestroy(lru->exec);
+            e->graphs.erase(lru);
+        }
+        e->graphs.push_back({key, exec, g_launches, 0});
+        slot = &e->graphs.back();
+        ++e->graph_captures;
+    }
+    slot->last_use = ++e->graph_clock;
+
+    // the run: its sizes to the device, then the graph
+    dims_h->N = n;
+    dims_h->M = M;
+    e->mark("start");
+    CVL_CUDA(cudaMemcpyAsync(e->gdims.p, dims_h, sizeof(RunDims), cudaMemcpyHostToDevice, s));
+    CVL_CUDA(cudaGraphLaunch(slot->exec, s));
+    e->mark("graph");
+    CVL_CUDA(cudaStreamSynchronize(s));
+    g_launches = slot->launches;
+    ++e->graph_replays;
+    const unsigned h_err = *err_h;
+    if (h_err & ERR_NONFINITE) return fail(CVL_EINVAL, "non-finite or out-of-range (|v| >= 1e9) edge coordinate");
+    const unsigned long long P = rb_h[0], C = rb_h[1];
+    if ((h_err & (ERR_CAPACITY | ERR_ARENA)) || C > C_cap) {
+        ++e->graph_fallbacks;
+        return CVL_EAGAIN;
+    }
+    if (h_err) return fail(CVL_EOVERFLOW, "kernel reported error bits " + std::to_string(h_err));
+    ro.stats.assign(stats_h, stats_h + M);
+    ro.max_deg = 0;
+    for (const MapStats &st : ro.stats) ro.max_deg = std::max(ro.max_deg, st.max_deg);
+    ro.total_pairs = P;
+    ro.cv_off.assign(rb_h + 2, rb_h + 2 + M + 1);
+    ro.total_curvelets = C;
+    return CVL_OK;
+}
+
+// The workspace of a shape for an engine that replays graphs: each buffer at the
+// larger of its size for the shape and its size for the graphs of the buckets that
+// runs within the shape can use (buckets 0 and 1 up to the shape's edges), and the
+// graphs' own small buffers.
+std::vector<WsItem> workspace_plan_with_graphs(const cvl_tuning *tune, unsigned long long arena_hint, const Model &md,
+                                               int cpl, const cvl_workspace_shape &s, bool graphs) {
+    std::vector<WsItem> v = workspace_plan(tune, arena_hint, md, cpl, s);
+    if (!graphs) return v;
+    const int top = std::min(bucket_of((long long)s.num_edges), 1);
+    for (int b = 0; b <= top; ++b) {
+        const GraphCaps cap = GRAPH_CAPS[b];
+        const unsigned long long per_chunk = std::max<unsigned long long>((unsigned long long)tune[b].chunk_pairs, 1024ull);
+        cvl_workspace_shape g;
+        g.num_edges = cap.N;
+        g.num_pairs = (int64_t)(per_chunk * (unsigned long long)cap.K);
+        g.num_curvelets = (int64_t)cap.N * cap.curvelets_per_edge;
+        g.num_maps = cap.M;
+        g.edge_data_sz = s.edge_data_sz;
+        for (const WsItem &w : workspace_plan(tune, arena_hint, md, cpl, g)) {
+            if (w.buf == &cvl_engine::edges || w.buf == &cvl_engine::map_off) continue;  // the caller's input
+            for (WsItem &x : v)
+                if (x.buf == w.buf) x.bytes = std::max(x.bytes, w.bytes);
+        }
+        v.push_back({&cvl_engine::gdims, sizeof(RunDims), false});
+        v.push_back({&cvl_engine::gchunks, sizeof(ChunkDims) * (size_t)cap.K, false});
+        v.push_back({&cvl_engine::gread, (size_t)(2 + cap.M + 1) * 8, false});
+    }
+    return v;
+}
+
+// The path: a bucket's graph where the run fits one, else the kernels launched one by one.
+template <typename R>
+int run_pipeline(cvl_engine *e, const R *d_edges, int n, int sz, const int *d_map_off,
+                 const std::vector<int32_t> &map_off_host, ModelT<R> md, int cpl, int mode, bool want_d2,
+                 RunOut &ro) {
+    if constexpr (std::is_same<R, double>::value) {
+        if (mode == 0 && !want_d2) {
+            const int rc = run_pipeline_graph(e, d_edges, n, sz, d_map_off, map_off_host, md, cpl, ro);
+            if (rc != CVL_EAGAIN) return rc;
+        }
+    }
+    return run_pipeline_direct(e, d_edges, n, sz, d_map_off, map_off_host, md, cpl, mode, want_d2, ro);
+}
 
 template <typename T>
 int upload(cvl_engine *e, const T *edges, int n, int sz, const std::vector<int32_t> &map_off) {
@@ -1092,6 +1442,9 @@ void cvl_engine_destroy(cvl_engine *e) {
     e->release_all();
     cudaStreamSynchronize(e->stream);
     for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
+    for (auto &g : e->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (e->gread_host) cudaFreeHost(e->gread_host);
     if (e->chunk_done) cudaEventDestroy(e->chunk_done);
     if (e->dev_done) cudaEventDestroy(e->dev_done);
     if (e->copy_stream) {
@@ -1606,12 +1959,15 @@ int cvl_engine_reserve_device(cvl_engine *e, size_t bytes) {
     return CVL_OK;
 }
 
+static int workspace_bytes_impl(const cvl_tuning *tune, bool graphs, const cvl_workspace_shape *s,
+                                const cvl_params *p, size_t *total, size_t *per_launch);
+
 extern "C" {
 
 int cvl_engine_workspace_bytes(cvl_engine *e, const cvl_workspace_shape *s, const cvl_params *p, size_t *total,
                                size_t *per_launch) {
     if (!e) return fail(CVL_EINVAL, "engine is NULL");
-    return cvl_workspace_bytes_tuned(e->tune, s, p, total, per_launch);
+    return workspace_bytes_impl(e->tune, e->graphs_on, s, p, total, per_launch);
 }
 
 int cvl_engine_reserve_workspace(cvl_engine *e, const cvl_workspace_shape *s, const cvl_params *p) {
@@ -1623,8 +1979,33 @@ int cvl_engine_reserve_workspace(cvl_engine *e, const cvl_workspace_shape *s, co
     CVL_TRY(make_model(e, p, p->nrad, 3u, p->max_candidates, md, cpl));
     // the record arena of later runs holds at least the shape's curvelets
     e->arena_hint = std::max<unsigned long long>(e->arena_hint, (unsigned long long)s->num_curvelets);
-    for (const WsItem &w : workspace_plan(e->tune, e->arena_hint, md, cpl, *s)) CVL_TRY(e->alloc(e->*(w.buf), w.bytes));
+    for (const WsItem &w : workspace_plan_with_graphs(e->tune, e->arena_hint, md, cpl, *s, e->graphs_on))
+        CVL_TRY(e->alloc(e->*(w.buf), w.bytes));
+    if (e->graphs_on && !e->gread_host) {  // the graphs' page-locked readback
+        void *h = nullptr;
+        if (cvl_alloc_fault_injected() || cudaMallocHost(&h, graph_readback_bytes() + sizeof(RunDims) + 64) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CVL_ENOMEM, "page-locked graph readback could not be allocated");
+        }
+        e->gread_host = (unsigned char *)h;
+    }
     CVL_CUDA(cudaStreamSynchronize(e->stream));
+    return CVL_OK;
+}
+
+int cvl_engine_set_graphs(cvl_engine *e, int enable) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    e->graphs_on = enable != 0;
+    return CVL_OK;
+}
+
+int cvl_engine_graph_stats(cvl_engine *e, cvl_engine_graphs *out) {
+    if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
+    out->enabled = e->graphs_on ? 1 : 0;
+    out->graphs = (int32_t)e->graphs.size();
+    out->captures = e->graph_captures;
+    out->replays = e->graph_replays;
+    out->fallbacks = e->graph_fallbacks;
     return CVL_OK;
 }
 
@@ -1640,6 +2021,11 @@ int cvl_engine_memory_get(cvl_engine *e, cvl_engine_memory *out) {
 
 int cvl_workspace_bytes_tuned(const cvl_tuning *tune, const cvl_workspace_shape *s, const cvl_params *p,
                               size_t *total, size_t *per_launch) {
+    return workspace_bytes_impl(tune, false, s, p, total, per_launch);
+}
+
+static int workspace_bytes_impl(const cvl_tuning *tune, bool graphs, const cvl_workspace_shape *s,
+                                const cvl_params *p, size_t *total, size_t *per_launch) {
     if (!tune || !s || !p || !total) return fail(CVL_EINVAL, "tuning/shape/params/total is NULL");
     if (s->num_edges < 1 || s->num_edges > 0x7fffffffLL || s->num_pairs < 0 || s->num_curvelets < 0 ||
         s->num_maps < 1 || s->edge_data_sz < 4)
@@ -1648,7 +2034,7 @@ int cvl_workspace_bytes_tuned(const cvl_tuning *tune, const cvl_workspace_shape 
     int cpl = 2;
     CVL_TRY(make_model(nullptr, p, p->nrad, 3u, p->max_candidates, md, cpl));
     size_t t = 0, c = 0;
-    for (const WsItem &w : workspace_plan(tune, 0, md, cpl, *s)) {
+    for (const WsItem &w : workspace_plan_with_graphs(tune, 0, md, cpl, *s, graphs)) {
         t += round256(w.bytes);
         if (w.per_launch) c += round256(w.bytes);
     }

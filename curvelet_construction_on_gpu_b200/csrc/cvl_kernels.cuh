@@ -70,6 +70,22 @@ struct BinnedT {
     int *map;                   // map of the edge
 };
 
+// The sizes of a run that a captured graph replays (one graph per size bucket
+// serves every run within the bucket): the kernels launched for the bucket's
+// capacity read the run's own sizes from device memory at their start. nullptr
+// outside graphs, where the launch's arguments are the run's sizes.
+struct RunDims {
+    int N;  // edges of the run (all maps)
+    int M;  // maps
+};
+
+// One chunk of a graph run's bundle/growth stages, computed on the device
+// (k_chunk_dims): its anchors [a_begin, a_end) and their pairs [p_begin, p_end).
+struct ChunkDims {
+    int a_begin, a_end;
+    unsigned long long p_begin, p_end;
+};
+
 struct MapStats {
     unsigned long long pairs;  // total_neighbor_pairs
     unsigned max_deg;          // max_num_of_neighbors
@@ -210,7 +226,11 @@ __device__ __forceinline__ int map_of(const int *map_off, int M, int e) {
 template <typename T>
 __global__ void k_bin_keys(const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off, int M,
                            ModelT<T> md, unsigned *__restrict__ ehash, unsigned *__restrict__ bcount,
-                           unsigned *__restrict__ err) {
+                           unsigned *__restrict__ err, const RunDims *__restrict__ dims) {
+    if (dims) {
+        N = dims->N;
+        M = dims->M;
+    }
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N; e += gridDim.x * blockDim.x) {
         const T x = edges[(size_t)e * sz + 0];
         const T y = edges[(size_t)e * sz + 1];
@@ -234,7 +254,11 @@ template <typename T>
 __global__ void k_bin_scatter(const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
                               int M, ModelT<T> md, const unsigned *__restrict__ ehash,
                               const unsigned *__restrict__ bstart, unsigned *__restrict__ bfill, BinnedT<T> B,
-                              int *__restrict__ pos_of) {
+                              int *__restrict__ pos_of, const RunDims *__restrict__ dims) {
+    if (dims) {
+        N = dims->N;
+        M = dims->M;
+    }
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N; e += gridDim.x * blockDim.x) {
         const unsigned h = ehash[e];
         const unsigned pos = bstart[h] + atomicAdd(&bfill[h], 1u);
@@ -430,6 +454,8 @@ struct NbArgsT {
     int *pair_anchor;                    // FILL (optional): internal anchor of each pair
     T *atrig;                            // FILL (optional): [N][2Q + 2] sin/cos(T2 + delta_t2_j), cos/sin(T2)
     unsigned *err;
+    const RunDims *dims;                 // graph runs: N and M from device memory
+    unsigned long long pair_cap;         // graph runs: pairs the CSR buffers hold (0: sized to the run)
 };
 
 // COUNT: ncand[i], per-map pairs / max degree / truncated anchors.
@@ -469,8 +495,10 @@ __global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
+    const int N = a.dims ? a.dims->N : a.N;
+    const int M = a.dims ? a.dims->M : a.M;
     if (MODE == NB_COUNT) {
-        block_stats_init(bstats, a.M);
+        block_stats_init(bstats, M);
         __syncthreads();
     }
     NbrSmemT<T> S;
@@ -481,7 +509,7 @@ __global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a
         S.idx = (int *)(p + (size_t)md.max_cand * 16);
     }
     const unsigned lt_mask = (1u << lane) - 1u;
-    for (int i = blockIdx.x * wpb + wib; i < a.N; i += gridDim.x * wpb) {
+    for (int i = blockIdx.x * wpb + wib; i < N; i += gridDim.x * wpb) {
         const int m = a.B.map[i];
         const int2 ac = a.B.cell[i];
         const T ax = a.B.x[i], ay = a.B.y[i];
@@ -494,7 +522,7 @@ __global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a
             if (lane == 0) {
                 a.ncand[i] = cnt;
                 const unsigned deg = cnt < (unsigned)md.max_cand ? cnt : (unsigned)md.max_cand;
-                stats_add(bstats, a.stats, a.M, m, deg, deg, deg >= (unsigned)md.max_cand ? 1u : 0u, 0u);
+                stats_add(bstats, a.stats, M, m, deg, deg, deg >= (unsigned)md.max_cand ? 1u : 0u, 0u);
             }
             continue;
         }
@@ -523,6 +551,11 @@ __global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a
         const unsigned long long off = a.pair_off[i];
         if (a.pair_off[i + 1] - off != n) {  // the two passes must agree
             if (lane == 0) atomicOr(a.err, ERR_INTERNAL);
+            __syncwarp();
+            continue;
+        }
+        if (a.pair_cap && a.pair_off[i + 1] > a.pair_cap) {  // a graph run beyond its pair buffers
+            if (lane == 0) atomicOr(a.err, ERR_CAPACITY);
             __syncwarp();
             continue;
         }
@@ -569,13 +602,18 @@ __global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a
     }
     if (MODE == NB_COUNT) {
         __syncthreads();
-        block_stats_flush(bstats, a.stats, a.M);
+        block_stats_flush(bstats, a.stats, M);
     }
 }
 
-__global__ void k_deg_from_ncand(int N, int max_cand, const unsigned *__restrict__ ncand, unsigned *__restrict__ deg) {
+// deg[i] for i < N; with dims (a graph run launched for its bucket's N), deg of the
+// run's anchors and 0 for the rest of the N entries, so that the scan over all N
+// gives the run's pair offsets and, at [N], its total.
+__global__ void k_deg_from_ncand(int N, int max_cand, const unsigned *__restrict__ ncand, unsigned *__restrict__ deg,
+                                 const RunDims *__restrict__ dims) {
+    const int n_run = dims ? dims->N : N;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const unsigned c = ncand[i];
+        const unsigned c = i < n_run ? ncand[i] : 0u;
         deg[i] = c < (unsigned)max_cand ? c : (unsigned)max_cand;
     }
 }
@@ -584,13 +622,43 @@ __global__ void k_deg_from_ncand(int N, int max_cand, const unsigned *__restrict
 // anchor whose pair offset is >= k * per_chunk (anchor-aligned, <= per_chunk +
 // max_deg pairs each). chunk_start[k] for k in [1, nchunks); [0] = 0.
 __global__ void k_chunk_starts(int N, const unsigned long long *__restrict__ pair_off, unsigned long long per_chunk,
-                               int nchunks, int *__restrict__ chunk_start) {
+                               int nchunks, int *__restrict__ chunk_start, const RunDims *__restrict__ dims) {
+    if (dims) N = dims->N;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const unsigned long long lo = (i == 0) ? 0ull : pair_off[i - 1];
         const unsigned long long hi = pair_off[i];
         // chunk boundaries k with lo < k * per_chunk <= hi start at anchor i
         for (unsigned long long k = lo / per_chunk + 1; k * per_chunk <= hi && k < (unsigned long long)nchunks; ++k)
             chunk_start[k] = i;
+    }
+}
+
+// A graph run's chunks (ChunkDims[K]) from k_chunk_starts' boundaries: the run has
+// ceil(P / per_chunk) chunks (at least one); chunks beyond those are empty. A run
+// with more than K chunks does not fit the graph: ERR_CAPACITY (the host runs it
+// without the graph). One thread.
+__global__ void k_chunk_dims(const RunDims *__restrict__ dims, const unsigned long long *__restrict__ pair_off,
+                             const int *__restrict__ chunk_start, unsigned long long per_chunk, int K,
+                             ChunkDims *__restrict__ cd, unsigned *__restrict__ err) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int N = dims->N;
+    const unsigned long long P = pair_off[N];
+    unsigned long long nch = (P + per_chunk - 1) / per_chunk;
+    if (nch < 1) nch = 1;
+    // more chunks than the graph holds: every chunk stays empty (the host runs the
+    // map again kernel by kernel)
+    const bool over = nch > (unsigned long long)K;
+    if (over) atomicOr(err, ERR_CAPACITY);
+    for (int c = 0; c < K; ++c) {
+        int a0 = N, a1 = N;
+        if (!over && (unsigned long long)c < nch) {
+            a0 = c == 0 ? 0 : chunk_start[c];
+            a1 = ((unsigned long long)c + 1 < nch && c + 1 < K) ? chunk_start[c + 1] : N;
+        }
+        cd[c].a_begin = a0;
+        cd[c].a_end = a1;
+        cd[c].p_begin = pair_off[a0];
+        cd[c].p_end = pair_off[a1];
     }
 }
 

@@ -217,6 +217,7 @@ struct BundleArgsT {
     unsigned *pslot;                    // [p_end - p_begin]: bund slot of each valid non-close pair
     unsigned *slot_ctr;                 // slots taken in this chunk (zero before the launch)
     unsigned char *pflag;               // [P]: bit 0 valid, bit 1 close
+    const ChunkDims *cd;                // graph runs: the pair range from device memory
 };
 
 constexpr int BUNDLE_THREADS = 128;
@@ -259,11 +260,12 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
     const bool lane_on = pl < PPB;
     const T delta_t2 = grid_offset(md.st, jl, md.Q);  // :698
     const int A2 = 2 * md.Q + 2;
-    const unsigned long long np = a.p_end - a.p_begin;
+    const unsigned long long p_begin = a.cd ? a.cd->p_begin : a.p_begin;
+    const unsigned long long np = (a.cd ? a.cd->p_end : a.p_end) - p_begin;
     for (unsigned long long g = (unsigned long long)blockIdx.x * PPB; g < np; g += (unsigned long long)gridDim.x * PPB) {
         const unsigned long long q = g + pl;
         if (lane_on && q < np) {
-            const unsigned long long p = a.p_begin + q;
+            const unsigned long long p = p_begin + q;
             if (!(a.pcls[p] & 4u)) {
                 const int ia = a.pair_anchor[p];
                 const int nn = a.csr_ids[p];
@@ -330,7 +332,7 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                 const unsigned long long qq = g + k;
                 bool need = false;
                 if (k < PPB && qq < np) {
-                    const unsigned long long p = a.p_begin + qq;
+                    const unsigned long long p = p_begin + qq;
                     const bool closep = (a.pcls[p] & 4u) != 0;
                     const bool valid = closep || s_open[k] != 0;
                     a.pflag[p] = (unsigned char)((valid ? 1u : 0u) | (closep ? 2u : 0u));
@@ -400,6 +402,7 @@ struct GrowthArgsT {
     unsigned *err;
     const unsigned short *cell_rank;    // [CELLS_MAX] best-cell rank of each cell (k_cell_ranks)
     int anchors_per_warp;               // sets the grid: ceil((a_end - a_begin) / (warps per block * this))
+    const ChunkDims *cd;                // graph runs: the chunk's anchors and first pair from device memory
 };
 
 // The best-cell ranks of fill_curvelet_info (:202-219), once per run.
@@ -463,7 +466,10 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
     // The grid has one warp per anchors_per_warp anchors, and a warp strides over
     // the chunk: its anchors lie far apart, so the work of dense regions is shared
     // out across warps (measured 8% faster than contiguous runs per warp).
-    for (int i = a.a_begin + blockIdx.x * wpb + wib; i < a.a_end; i += gridDim.x * wpb) {
+    const int a_begin = a.cd ? a.cd->a_begin : a.a_begin;
+    const int a_end = a.cd ? a.cd->a_end : a.a_end;
+    const unsigned long long p_begin = a.cd ? a.cd->p_begin : a.p_begin;
+    for (int i = a_begin + blockIdx.x * wpb + wib; i < a_end; i += gridDim.x * wpb) {
         const int m = a.B.map[i];
         const int orig = a.B.orig[i];
         const unsigned long long off = a.pair_off[i];
@@ -491,7 +497,7 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
                 const int slot = t0 ? ns_run0 + __popc(b0 & lt_mask) : md.max_cand - 1 - (ns_run1 + __popc(b1 & lt_mask));
                 // a valid non-close pair's bundle is at its compacted slot; a close pair
                 // keeps the default bundle and reads none
-                seed_q[slot] = (fl & 2u) ? CLOSE_BIT : a.pslot[off + k - a.p_begin];
+                seed_q[slot] = (fl & 2u) ? CLOSE_BIT : a.pslot[off + k - p_begin];
                 seed_orig[slot] = a.B.orig[a.csr_ids[off + k]];
             }
             ns_run0 += __popc(b0);
@@ -741,7 +747,12 @@ template <typename T>
 __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
                            int M, Records rec, const unsigned *__restrict__ rec_base,
                            const unsigned *__restrict__ run_cnt, const unsigned long long *__restrict__ out_off,
-                           unsigned long long out_cap, unsigned *__restrict__ chains, double *__restrict__ info) {
+                           unsigned long long out_cap, unsigned *__restrict__ chains, double *__restrict__ info,
+                           const RunDims *__restrict__ dims) {
+    if (dims) {
+        N = dims->N;
+        M = dims->M;
+    }
     const int W = md.gms + 1;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < N; a += gridDim.x * blockDim.x) {
         const unsigned c0 = run_cnt[2 * a], c1 = run_cnt[2 * a + 1];
@@ -915,6 +926,23 @@ __global__ void k_transport_cells(Model md, const double *__restrict__ ops, int 
 // ---------------------------------------------------------------------------
 // Utility kernels
 // ---------------------------------------------------------------------------
+// The end of a graph run: its pair and curvelet totals and each map's curvelet
+// offset, for the host to read in one copy: out[0] = P, out[1] = C,
+// out[2 + m] = out_off[map_off[m]] for m <= M. out_off is the scan over the
+// bucket's N, with zero counts past the run.
+__global__ void k_graph_readback(const RunDims *__restrict__ dims, const unsigned long long *__restrict__ pair_off,
+                                 const unsigned long long *__restrict__ out_off, const int *__restrict__ map_off,
+                                 unsigned long long *__restrict__ out) {
+    const int N = dims->N, M = dims->M;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m <= M; m += gridDim.x * blockDim.x) {
+        if (m == 0) {
+            out[0] = pair_off[N];
+            out[1] = out_off[N];
+        }
+        if (m <= M) out[2 + m] = out_off[map_off[m]];
+    }
+}
+
 // CSR in the reference's layout (anchor = input order, neighbour ids = input
 // indices local to the map) from the internal CSR.
 __global__ void k_graph_degrees(int N, const int *__restrict__ orig_of, const unsigned long long *__restrict__ pair_off,

@@ -516,6 +516,27 @@ typedef struct cvl_engine_memory {
 } cvl_engine_memory;
 int cvl_engine_memory_get(cvl_engine *e, cvl_engine_memory *out);
 
+/* ---- CUDA graphs of the path ------------------------------------------
+ * No reference counterpart. A run (cvl_run, cvl_batch_run, ...) of up to 64 Ki
+ * edges (tuning bucket 0) or 512 Ki edges (bucket 1), in double, replays a CUDA
+ * graph of the whole path captured for the bucket's capacities (edges, 4,096
+ * maps, 2 or 8 bundle chunks, 8 curvelets per edge): the kernels read the run's
+ * sizes from device memory, so one graph serves every run of its bucket, with
+ * one host synchronisation where the kernel-by-kernel path has three. A graph is
+ * captured on a bucket's first run and again when the parameters, the tuning or
+ * the buffers change (up to 6 kept per engine). A run beyond a capacity is
+ * flagged on the device and run again kernel by kernel; the results are the same
+ * either way. CVL_NO_GRAPHS in the environment turns graphs off for new engines. */
+int cvl_engine_set_graphs(cvl_engine *e, int enable);
+typedef struct cvl_engine_graphs {
+    int32_t enabled;
+    int32_t graphs;      /* captured graphs held */
+    uint64_t captures;   /* graphs captured so far */
+    uint64_t replays;    /* runs that replayed a graph */
+    uint64_t fallbacks;  /* of those, runs beyond a capacity, run again kernel by kernel */
+} cvl_engine_graphs;
+int cvl_engine_graph_stats(cvl_engine *e, cvl_engine_graphs *out);
+
 /* Writes a buffer larger than the L2 cache on the engine's stream and waits
  * (timing hygiene between benchmark iterations). */
 int cvl_engine_flush_l2(cvl_engine *e);
