@@ -555,6 +555,15 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
                             for (int u = 0; u < CPL; ++u) cmin[q][u] = cmax[q][u] = T(0);
                         }
                     }
+                    // open cells of each seed's running bundle, this lane's (bit q * CPL + u):
+                    // the intersection test below needs them, and they change only when
+                    // a seed takes a bundle
+                    unsigned copen = 0;
+#pragma unroll
+                    for (int q = 0; q < K; ++q)
+#pragma unroll
+                        for (int u = 0; u < CPL; ++u)
+                            copen |= (on_l[u] && cmax[q][u] > cmin[q][u]) ? 1u << (q * CPL + u) : 0u;
                     // the walk's bundles, one ahead: r + 1 loads while r is intersected
                     T nmin[CPL], nmax[CPL];
                     load_bundle(0, nmin, nmax);
@@ -566,17 +575,21 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
                             rmax[u] = nmax[u];
                         }
                         if (r + 1 < ns) load_bundle(r + 1, nmin, nmax);
+                        // bundle_intersection + bundle_intersection_valid_check (:832-854): a
+                        // cell of the intersection is open when min(cmax, rmax) > max(cmin,
+                        // rmin), that is when cmax > cmin, rmax > rmin, cmax > rmin and rmax >
+                        // cmin (bundle bounds are never NaN: a NaN bound never wins a clamp)
+                        bool ropen[CPL];
+#pragma unroll
+                        for (int u = 0; u < CPL; ++u) ropen[u] = rmax[u] > rmin[u];
                         unsigned bits = 0;
 #pragma unroll
                         for (int q = 0; q < K; ++q) {
                             bool lv = false;
 #pragma unroll
-                            for (int u = 0; u < CPL; ++u) {
-                                // bundle_intersection (:832-843)
-                                const T lo = (cmin[q][u] < rmin[u]) ? rmin[u] : cmin[q][u];
-                                const T hi = (cmax[q][u] > rmax[u]) ? rmax[u] : cmax[q][u];
-                                lv = lv || (on_l[u] && hi > lo);
-                            }
+                            for (int u = 0; u < CPL; ++u)
+                                lv |= ((copen >> (q * CPL + u)) & 1u) & ropen[u] & (cmax[q][u] > rmin[u]) &
+                                      (rmax[u] > cmin[q][u]);
                             bits |= lv ? (1u << q) : 0u;
                         }
                         bits = __reduce_or_sync(FULL, bits);  // bundle_intersection_valid_check (:845-854)
@@ -599,6 +612,8 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
                                 for (int u = 0; u < CPL; ++u) {
                                     cmin[q][u] = (cmin[q][u] < rmin[u]) ? rmin[u] : cmin[q][u];
                                     cmax[q][u] = (cmax[q][u] > rmax[u]) ? rmax[u] : cmax[q][u];
+                                    const unsigned bit = 1u << (q * CPL + u);
+                                    copen = (on_l[u] && cmax[q][u] > cmin[q][u]) ? (copen | bit) : (copen & ~bit);
                                 }
                             }
                             if (len[q] >= (unsigned)md.gms) done |= 1u << q;
