@@ -337,7 +337,9 @@ cvl_tuning default_tuning(int cell_size, int seeds_per_group) {
     cvl_tuning t;
     t.cell_size = cell_size;
     t.bundle_blocks_per_sm = 4;
-    t.growth_blocks_per_sm = 6;  // measured: growth -11% against 4 (80 registers, 24 warps per SM)
+    // measured on the 64-map batch: 8 (63 registers, 32 one-warp blocks per SM) 174.8 ms,
+    // 6 (72 registers) 187.3 ms, 4 slower still; grids other than the default take 6 for 8
+    t.growth_blocks_per_sm = 8;
     t.seeds_per_group = seeds_per_group;
     t.anchors_per_warp = 8;
     t.chunk_pairs = (int64_t)CHUNK_PAIRS_DEFAULT;
@@ -349,8 +351,8 @@ int check_tuning(const cvl_tuning &t) {
         return fail(CVL_EINVAL, "tuning: cell_size must be 2, 4 or 8");
     if (t.bundle_blocks_per_sm != 3 && t.bundle_blocks_per_sm != 4)
         return fail(CVL_EINVAL, "tuning: bundle_blocks_per_sm must be 3 or 4");
-    if (t.growth_blocks_per_sm != 4 && t.growth_blocks_per_sm != 6)
-        return fail(CVL_EINVAL, "tuning: growth_blocks_per_sm must be 4 or 6");
+    if (t.growth_blocks_per_sm != 4 && t.growth_blocks_per_sm != 6 && t.growth_blocks_per_sm != 8)
+        return fail(CVL_EINVAL, "tuning: growth_blocks_per_sm must be 4, 6 or 8");
     if (t.seeds_per_group != 4 && t.seeds_per_group != 8) return fail(CVL_EINVAL, "tuning: seeds_per_group must be 4 or 8");
     if (t.anchors_per_warp < 1 || t.anchors_per_warp > 32) return fail(CVL_EINVAL, "tuning: anchors_per_warp in [1, 32]");
     if (t.chunk_pairs < (1 << 16) || t.chunk_pairs > (1LL << 30))
@@ -548,6 +550,7 @@ void pick_kernels(int cpl, const cvl_tuning &, bundles_fn<float> &bf, growth_fn<
 void pick_kernels(int cpl, const cvl_tuning &t, bundles_fn<double> &bf, growth_fn<double> &gf) {
     const bool b3 = t.bundle_blocks_per_sm == 3;
     const bool g6 = t.growth_blocks_per_sm == 6;
+    const bool g8 = t.growth_blocks_per_sm == 8;  // 64 registers: 32 one-warp blocks per SM
     const bool k8 = t.seeds_per_group == 8 && cpl <= 2;
     switch (cpl) {
         case 1:
@@ -564,7 +567,9 @@ void pick_kernels(int cpl, const cvl_tuning &t, bundles_fn<double> &bf, growth_f
             break;
         default:
             bf = b3 ? launch_bundles<double, 2, 3> : launch_bundles<double, 2, 4>;
-            gf = k8 ? launch_growth<double, 2, 8, 4> : (g6 ? launch_growth<double, 2, 4, 6> : launch_growth<double, 2, 4, 4>);
+            gf = k8 ? launch_growth<double, 2, 8, 4>
+                    : (g8 ? launch_growth<double, 2, 4, 8>
+                          : (g6 ? launch_growth<double, 2, 4, 6> : launch_growth<double, 2, 4, 4>));
             break;
     }
 }
@@ -1162,7 +1167,7 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
                 // few anchors each
                 ga.anchors_per_warp = 1;
                 ga.cd = cdp + c;
-                CVL_TRY(gf(e, ga, gsmem, sms * 24));
+                CVL_TRY(gf(e, ga, gsmem, sms * 4 * tn.growth_blocks_per_sm));
             }
             CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->count.p, N,
                                                         (unsigned long long *)e->out_off.p)));
@@ -2124,7 +2129,7 @@ int cvl_engine_autotune(cvl_engine *e, const cvl_batch *b, const cvl_params *p, 
     const int64_t chunks[] = {1LL << 20, 4LL << 20, 16LL << 20};
     const int apws[] = {1, 2, 4, 8, 16};
     const int cells[] = {2, 4, 8};
-    const int growth[][2] = {{4, 4}, {4, 6}, {8, 4}};  // (seeds_per_group, blocks per SM)
+    const int growth[][2] = {{4, 4}, {4, 6}, {4, 8}, {8, 4}};  // (seeds_per_group, blocks per SM)
     for (int pass = 0; pass < passes; ++pass) {
         auto consider = [&](const cvl_tuning &t) -> int {
             if (std::memcmp(&t, &cur, sizeof(t)) == 0) return CVL_OK;

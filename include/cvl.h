@@ -465,7 +465,8 @@ int cvl_write_edges_binary(const char *path, const double *edges, int64_t num_ed
 typedef struct cvl_tuning {
     int cell_size;                    /* spatial-hash block edge in pixel cells: 2, 4 or 8 (4; 8 above 512 Ki edges) */
     int bundle_blocks_per_sm;         /* bundle kernel's register budget: 3 or 4 resident blocks per SM (4) */
-    int growth_blocks_per_sm;         /* growth kernel's register budget: 4 or 6 resident blocks of 4 warps per SM (6) */
+    int growth_blocks_per_sm;         /* growth kernel's register budget: 4, 6 or 8 resident blocks of 4 warps per SM
+                                         (8: 63 registers; grids other than the default 63-cell one take 6 for 8) */
     int seeds_per_group;              /* chain-growth seeds walked together per warp: 4 or 8 (4) */
     int anchors_per_warp;             /* chain-growth anchors per warp: 1..32 (8) */
     int64_t chunk_pairs;              /* neighbour pairs whose bundles are held in HBM at once (4 Mi) */
