@@ -88,10 +88,16 @@ def test_server_admission_budget(engine):
             srv.submit(synth.plain_hd(1000))
         assert ei.value.code == _abi.CVL_ENOMEM
         ms, ed = srv.latencies()
+        rt = srv.request_times()
     for m, g in zip(maps, got):
         _same(engine.run(m), g)
     assert st["completed"] == 6 and st["launches"] == 6 and st["admitted_bytes"] == 0
     assert len(ms) == 6 and sorted(ed.tolist()) == sorted(m.shape[0] for m in maps)
+    # the per-request breakdown: one entry per request, its parts within its total
+    assert len(rt) == 6 and sorted(rt["edges"].tolist()) == sorted(m.shape[0] for m in maps)
+    assert np.all(rt["launch_maps"] == 1)
+    parts = rt["queue_ms"] + rt["upload_ms"] + rt["run_ms"] + rt["result_ms"]
+    assert np.all(parts <= rt["total_ms"] + 0.5) and np.all(rt["run_ms"] > 0)
 
 
 def test_server_next_hands_out_in_completion_order(engine):
