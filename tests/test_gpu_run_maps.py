@@ -40,3 +40,20 @@ def test_run_maps_params_and_errors(engine):
     with pytest.raises(cvl.CvlError):
         engine.run_maps(np.concatenate(maps), counts=[maps[0].shape[0], 0, maps[1].shape[0] + maps[2].shape[0]])
     assert _same(engine.run_maps(maps[:1])[0], engine.run(maps[0]))
+
+
+def test_run_maps_gated_copies_on_large_groups(engine):
+    """Groups above the graph buckets (512 Ki edges) run kernel by kernel in chunks,
+    and each group's result copies are released during the next group's growth
+    kernels: the results still equal the maps run alone, bit for bit."""
+    # 598k, 621k, 1.25M and 1.31M edges, and two small maps folded with the large ones
+    maps = [synth.mixed_map(s) for s in (2037, 2041, 2010, 2009)] + [synth.plain_small(3), synth.plain_small(4)]
+    singles = [engine.run(m) for m in maps]
+    with cvl.Engine() as eng:
+        for b in range(4):
+            eng.set_tuning(b, chunk_pairs=1 << 18)  # more chunks: more gated releases
+        # group_edges 1: one map per group (four groups above the graph buckets);
+        # 2 Mi: groups of several maps
+        for group_edges in (1, 2 << 20):
+            got = eng.run_maps(maps, group_edges=group_edges)
+            assert all(_same(a, b) for a, b in zip(got, singles)), group_edges
