@@ -126,11 +126,6 @@ struct cvl_engine {
     cvl_tuning tune[CVL_TUNING_BUCKETS];                   // per size bucket of the batch
     cvl_yield_fn yield_fn = nullptr;                       // called between chunks (serving)
     void *yield_ctx = nullptr;
-    // called around each chunk's growth launch: phase 0 after the chunk's bundles were
-    // launched (ev: recorded after them), phase 1 after its growth was launched
-    void (*chunk_hook)(void *ctx, int phase, unsigned long long pairs, cudaEvent_t ev) = nullptr;
-    void *chunk_ctx = nullptr;
-    cudaEvent_t hook_ev = nullptr;
     cudaEvent_t chunk_done = nullptr;
     std::vector<cvl_batch *> batches;                      // live batches, freed with the engine
     unsigned long long arena_hint = 0;  // record arena size that the last input needed
@@ -145,7 +140,6 @@ struct cvl_engine {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t computed[2] = {nullptr, nullptr};
     cudaEvent_t copied[2] = {nullptr, nullptr};
-    cudaEvent_t copy_piece_done = nullptr;
     // downstream stage (link graph, contour fragments)
     struct ContourBufs {
         DBuf chains_in, cnt, off, cursor, bucket, outdeg, indeg, child, parent, succ, pred, flags, linked, firsts,
@@ -439,7 +433,7 @@ int check_launch(const char *what) {
 // Host<->device copies in pieces of at most 32 MiB: the copy engines take
 // commands in turn across streams, so a large map's transfer does not hold up
 // a small map's for the whole of its length.
-inline cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
     constexpr size_t PIECE = (size_t)32 << 20;
     for (size_t o = 0; o < bytes; o += PIECE) {
         const cudaError_t ce =
@@ -447,6 +441,27 @@ inline cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMem
         if (ce != cudaSuccess) return ce;
     }
     return cudaSuccess;
+}
+
+// Device -> page-locked host copy of results. RESULT_COPY_SM (the default) copies with a
+// small kernel (RESULT_COPY_BLOCKS blocks), which slows concurrent path kernels far less
+// than a copy-engine transfer does; CVL_RESULT_COPY=ce in the environment selects the
+// copy engine (cudaMemcpyAsync in pieces). Sizes are multiples of 4 bytes.
+constexpr int RESULT_COPY_BLOCKS = 16;
+const bool g_result_copy_sm = [] {
+    const char *v = std::getenv("CVL_RESULT_COPY");
+    return !(v && std::strcmp(v, "ce") == 0);
+}();
+
+cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
+
+inline cudaError_t copy_result_to_host(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (!bytes) return cudaSuccess;
+    if (!g_result_copy_sm || (bytes & 3) || (((uintptr_t)src | (uintptr_t)dst) & 3))
+        return copy_pieces(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+    const int wide = ((((uintptr_t)src | (uintptr_t)dst) | bytes) & 15) == 0 ? 1 : 0;
+    k_copy_to_host<<<RESULT_COPY_BLOCKS, 256, 0, s>>>(src, dst, bytes, wide);
+    return cudaGetLastError();
 }
 
 // Grids of short blocks: `per_block` work items per block and no cap, so a
@@ -806,11 +821,6 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
                 CVL_TRY(bf(e, ba, bblocks));
             }
             e->mark("bundles");
-            if (e->chunk_hook) {
-                if (!e->hook_ev) CVL_CUDA(cudaEventCreateWithFlags(&e->hook_ev, cudaEventDisableTiming));
-                CVL_CUDA(cudaEventRecord(e->hook_ev, s));
-                e->chunk_hook(e->chunk_ctx, 0, ba.p_end - ba.p_begin, e->hook_ev);
-            }
             GrowthArgsT<R> ga{};
             ga.md = md;
             ga.B = B;
@@ -836,7 +846,6 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
             ga.cell_rank = (const unsigned short *)e->crank.p;
             ga.anchors_per_warp = tn.anchors_per_warp;
             CVL_TRY(gf(e, ga, gsmem, gblocks));
-            if (e->chunk_hook) e->chunk_hook(e->chunk_ctx, 1, ba.p_end - ba.p_begin, nullptr);
             e->mark("growth");
         }
 
@@ -1460,7 +1469,6 @@ void cvl_engine_destroy(cvl_engine *e) {
     e->release_all();
     cudaStreamSynchronize(e->stream);
     for (cudaEvent_t ev : e->marks) cudaEventDestroy(ev);
-    if (e->hook_ev) cudaEventDestroy(e->hook_ev);
     for (auto &g : e->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (e->gread_host) cudaFreeHost(e->gread_host);
@@ -1472,7 +1480,6 @@ void cvl_engine_destroy(cvl_engine *e) {
             cudaEventDestroy(e->computed[k]);
             cudaEventDestroy(e->copied[k]);
         }
-        if (e->copy_piece_done) cudaEventDestroy(e->copy_piece_done);
         cudaStreamDestroy(e->copy_stream);
     }
     cudaStreamDestroy(e->stream);
@@ -1907,11 +1914,11 @@ int cvl_batch_result_take_map(cvl_batch_result *r, int32_t m, cvl_result **out) 
             std::memcpy(res->chains_p, r->chains + c0 * r->width, sizeof(unsigned) * C * r->width);
             std::memcpy(res->info_p, r->info + c0 * 10, sizeof(double) * C * 10);
         } else {
-            cudaError_t ce = copy_pieces(res->chains_p, (const unsigned *)e->chains.p + c0 * r->width,
-                                         sizeof(unsigned) * C * r->width, cudaMemcpyDeviceToHost, e->stream);
+            cudaError_t ce = copy_result_to_host(res->chains_p, (const unsigned *)e->chains.p + c0 * r->width,
+                                                 sizeof(unsigned) * C * r->width, e->stream);
             if (ce == cudaSuccess)
-                ce = copy_pieces(res->info_p, (const double *)e->info.p + c0 * 10, sizeof(double) * C * 10,
-                                 cudaMemcpyDeviceToHost, e->stream);
+                ce = copy_result_to_host(res->info_p, (const double *)e->info.p + c0 * 10, sizeof(double) * C * 10,
+                                         e->stream);
             if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
             if (ce != cudaSuccess) {
                 delete res;
@@ -2765,88 +2772,9 @@ void cvl_contours_free(cvl_contours *c) { delete c; }
 
 
 // =============================================================================
-// Many maps, host to host, with the result copies behind the compute
+// Many maps, host to host, with the result copies behind the compute (by SM threads:
+// copy_result_to_host)
 // =============================================================================
-namespace {
-
-// Device-to-host copies slow the path's write-heavy kernels when they run beside
-// them: measured on the 64-map batch with a copy stream busy at 53 GB/s, k_bundles
-// 240 -> 752 ms and k_finalize 12 -> 559 ms, while k_growth (which writes little)
-// went 174 -> 177 ms, and host-to-device or device-to-device copies changed little.
-// So cvl_run_maps queues a group's result copies and releases them only while the
-// next group's growth kernels run: after each chunk's bundles, about as many bytes
-// as the chunk's growth takes time to copy, and the next chunk's bundles wait for
-// them. What does not fit is copied at the end of that group.
-struct CopyGate {
-    struct Piece {
-        void *dst;
-        const void *src;
-        size_t bytes;
-        int group;
-        bool last;  // the group's last piece: its copied event follows
-    };
-    std::deque<Piece> q;
-    cudaStream_t cs = nullptr, s = nullptr;
-    cudaEvent_t piece_done = nullptr;
-    cudaEvent_t *copied = nullptr;  // [2], by group parity
-    double bytes_per_pair = 16.0;   // growth time per pair at the host link's rate
-    bool issued = false;
-    cudaError_t err = cudaSuccess;
-
-    void issue(const Piece &p) {
-        const cudaError_t e1 = cudaMemcpyAsync(p.dst, p.src, p.bytes, cudaMemcpyDeviceToHost, cs);
-        if (e1 != cudaSuccess) err = e1;
-        if (p.last) {
-            const cudaError_t e2 = cudaEventRecord(copied[p.group & 1], cs);
-            if (e2 != cudaSuccess) err = e2;
-        }
-    }
-    void release(size_t budget) {
-        while (budget > 0 && !q.empty()) {
-            Piece &p = q.front();
-            if (p.bytes <= budget) {
-                budget -= p.bytes;
-                const Piece x = p;
-                q.pop_front();
-                issue(x);
-            } else {
-                Piece x = p;
-                x.bytes = budget;
-                x.last = false;
-                issue(x);
-                p.dst = (char *)p.dst + budget;
-                p.src = (const char *)p.src + budget;
-                p.bytes -= budget;
-                budget = 0;
-            }
-        }
-    }
-    void flush(int up_to_group) {
-        while (!q.empty() && q.front().group <= up_to_group) {
-            const Piece x = q.front();
-            q.pop_front();
-            issue(x);
-        }
-    }
-    static void hook(void *ctx, int phase, unsigned long long pairs, cudaEvent_t ev) {
-        CopyGate *g = (CopyGate *)ctx;
-        if (phase == 0) {
-            if (g->q.empty()) return;
-            cudaError_t e1 = cudaStreamWaitEvent(g->cs, ev, 0);  // after the chunk's bundles
-            if (e1 != cudaSuccess) g->err = e1;
-            g->release((size_t)((double)pairs * g->bytes_per_pair) + 1);
-            e1 = cudaEventRecord(g->piece_done, g->cs);
-            if (e1 != cudaSuccess) g->err = e1;
-            g->issued = true;
-        } else if (g->issued) {
-            const cudaError_t e1 = cudaStreamWaitEvent(g->s, g->piece_done, 0);  // the next bundles wait
-            if (e1 != cudaSuccess) g->err = e1;
-            g->issued = false;
-        }
-    }
-};
-
-}  // namespace
 
 extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps,
                             int32_t edge_data_sz, const cvl_params *p, int64_t group_edges, cvl_result **out) {
@@ -2866,27 +2794,8 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
             CVL_CUDA(cudaEventCreateWithFlags(&e->computed[k], cudaEventDisableTiming));
             CVL_CUDA(cudaEventCreateWithFlags(&e->copied[k], cudaEventDisableTiming));
         }
-        CVL_CUDA(cudaEventCreateWithFlags(&e->copy_piece_done, cudaEventDisableTiming));
     }
-    CopyGate gate;
-    gate.cs = e->copy_stream;
-    gate.s = e->stream;
-    gate.piece_done = e->copy_piece_done;
-    gate.copied = e->copied;
-    if (const char *v = std::getenv("CVL_COPY_BYTES_PER_PAIR")) gate.bytes_per_pair = std::atof(v);
-    // the gate is the engine's chunk hook for this call (a server's yield hook, if any,
-    // is left as it is: cvl_run_maps is not called by the server)
-    struct HookScope {
-        cvl_engine *e;
-        HookScope(cvl_engine *e_, CopyGate *g) : e(e_) {
-            e->chunk_hook = &CopyGate::hook;
-            e->chunk_ctx = g;
-        }
-        ~HookScope() {
-            e->chunk_hook = nullptr;
-            e->chunk_ctx = nullptr;
-        }
-    } hook_scope(e, &gate);
+
     Model md;
     int cpl = 2;
     CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
@@ -2903,7 +2812,6 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
 
     std::vector<cvl_result *> res(num_maps, nullptr);
     auto cleanup = [&](int rc) {
-        gate.flush(1 << 30);
         cudaStreamSynchronize(e->copy_stream);
         for (cvl_result *r : res) delete r;
         return rc;
@@ -2919,8 +2827,6 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
             std::swap(e->chains, e->chains_alt);
             std::swap(e->info, e->info_alt);
         }
-        // the group before last's copies are all issued by now (flushed at the end of
-        // the last group); this group's outputs wait for them
         if (copy_pending[buf]) CVL_CUDA(cudaStreamWaitEvent(e->stream, e->copied[buf], 0));
         std::vector<int32_t> mo(M + 1, 0);
         for (int k = 0; k < M; ++k) mo[k + 1] = mo[k] + counts[m0 + k];
@@ -2933,9 +2839,6 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
         if (rc != CVL_OK) return cleanup(rc);
         e->collect_marks();
         device_ms += e->last_device_ms;
-        // what the group before did not get copied during this group's growth goes now
-        gate.flush(g - 1);
-        if (gate.err != cudaSuccess) return cleanup(fail(CVL_ECUDA, std::string("result copy: ") + cudaGetErrorString(gate.err)));
         if (cudaEventRecord(e->computed[buf], e->stream) != cudaSuccess ||
             cudaStreamWaitEvent(e->copy_stream, e->computed[buf], 0) != cudaSuccess)
             return cleanup(fail(CVL_ECUDA, "event record/wait failed"));
@@ -2948,10 +2851,13 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
             r->info_p = e->pinned->get(sizeof(double) * (C ? C : 1) * 10);
             if (!r->chains_p || !r->info_p)
                 return cleanup(fail(CVL_ENOMEM, "page-locked result buffers could not be allocated"));
-            if (C) {  // queued: released during the next group's growth (CopyGate)
-                gate.q.push_back({r->chains_p, (const unsigned *)e->chains.p + c0 * W, sizeof(unsigned) * C * W, g,
-                                  false});
-                gate.q.push_back({r->info_p, (const double *)e->info.p + c0 * 10, sizeof(double) * C * 10, g, false});
+            if (C) {  // by SM threads beside the next group's compute (copy_result_to_host)
+                cudaError_t ce = copy_result_to_host(r->chains_p, (const unsigned *)e->chains.p + c0 * W,
+                                                     sizeof(unsigned) * C * W, e->copy_stream);
+                if (ce == cudaSuccess)
+                    ce = copy_result_to_host(r->info_p, (const double *)e->info.p + c0 * 10,
+                                             sizeof(double) * C * 10, e->copy_stream);
+                if (ce != cudaSuccess) return cleanup(fail(CVL_ECUDA, std::string("result copy: ") + cudaGetErrorString(ce)));
             }
             const MapStats &st = ro.stats[k];
             cvl_result_view &v = r->v;
@@ -2966,16 +2872,10 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
             v.num_edges = (uint32_t)counts[m0 + k];
             v.flags = v.truncated_anchors ? CVL_FLAG_TRUNCATED : 0u;
         }
-        // the group's copied event follows its last piece (a group with no rows: now)
-        if (!gate.q.empty() && gate.q.back().group == g) {
-            gate.q.back().last = true;
-        } else if (cudaEventRecord(e->copied[buf], e->copy_stream) != cudaSuccess) {
+        if (cudaEventRecord(e->copied[buf], e->copy_stream) != cudaSuccess)
             return cleanup(fail(CVL_ECUDA, "event record failed"));
-        }
         copy_pending[buf] = true;
     }
-    gate.flush(1 << 30);  // the last group's rows: the compute is over
-    if (gate.err != cudaSuccess) return cleanup(fail(CVL_ECUDA, std::string("result copy: ") + cudaGetErrorString(gate.err)));
     CVL_CUDA(cudaStreamSynchronize(e->copy_stream));
     for (int32_t m = 0; m < num_maps; ++m) {
         res[m]->v.device_ms = device_ms;

@@ -997,6 +997,25 @@ __global__ void k_fp64_peak(double *out, int iters, double seed) {
     if (s == 12345.678) out[0] = s;  // keeps the chains live
 }
 
+// Device -> page-locked host copy by SM threads (the destination is host memory the
+// device addresses directly). Beside the path's write-heavy kernels a copy-engine
+// transfer to the host slows them several times over, and this one far less.
+// 16-byte words when both addresses and the size allow, else 4-byte words.
+__global__ void k_copy_to_host(const void *__restrict__ src, void *__restrict__ dst, size_t bytes, int wide) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    if (wide) {
+        const uint4 *s4 = (const uint4 *)src;
+        uint4 *d4 = (uint4 *)dst;
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < bytes / 16; i += stride)
+            __stcs(d4 + i, __ldcs(s4 + i));
+    } else {
+        const unsigned *s1 = (const unsigned *)src;
+        unsigned *d1 = (unsigned *)dst;
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < bytes / 4; i += stride)
+            __stcs(d1 + i, __ldcs(s1 + i));
+    }
+}
+
 // Writes a buffer larger than L2 (timing hygiene).
 __global__ void k_flush(unsigned *buf, size_t n, unsigned v) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
