@@ -18,6 +18,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cuda.h>
@@ -534,12 +535,26 @@ int launch_bundles(cvl_engine *e, BundleArgsT<T> &a, int blocks) {
         const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
         blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
     }
+    if constexpr (std::is_same<T, double>::value) {
+        if (a.queue) {  // a graph run: the queue-pulling variant
+            k_bundles<T, CPL, MINB, true><<<blocks, BUNDLE_THREADS, (size_t)ppb * pair_bytes, e->stream>>>(a);
+            return check_launch("k_bundles");
+        }
+    }
     k_bundles<T, CPL, MINB><<<blocks, BUNDLE_THREADS, (size_t)ppb * pair_bytes, e->stream>>>(a);
     return check_launch("k_bundles");
 }
 
 template <typename T, int CPL, int K, int MINB>
 int launch_growth(cvl_engine *e, GrowthArgsT<T> &a, size_t smem, int blocks) {
+    if constexpr (std::is_same<T, double>::value) {
+        if (a.queue) {  // a graph run: the queue-pulling variant on the given persistent grid
+            CVL_CUDA(cudaFuncSetAttribute(k_growth<T, CPL, K, MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            k_growth<T, CPL, K, MINB, true><<<blocks, GROWTH_THREADS, smem, e->stream>>>(a);
+            return check_launch("k_growth");
+        }
+    }
     CVL_CUDA(cudaFuncSetAttribute(k_growth<T, CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (!a.cd) {  // a graph run (device-side range) keeps the given grid, which strides over the anchors
         // a warp per anchor and anchors_per_warp anchors per warp: short blocks (a
@@ -1150,8 +1165,11 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
             rec.ids = (unsigned *)e->rec_ids.p;
             rec.k = (double *)e->rec_k.p;
             rec.meta = (unsigned *)e->rec_meta.p;
+            // the chunks' work queues (bundle pair tiles, growth anchors)
+            unsigned *queues = (unsigned *)((unsigned long long *)e->work.p + 3);
             for (int c = 0; c < cap.K; ++c) {
                 CVL_CUDA(cudaMemsetAsync(slot_ctr, 0, sizeof(unsigned), s));
+                CVL_CUDA(cudaMemsetAsync(queues, 0, 2 * sizeof(unsigned), s));
                 BundleArgsT<double> ba{};
                 ba.md = md;
                 ba.B = B;
@@ -1164,6 +1182,9 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
                 ba.slot_ctr = slot_ctr;
                 ba.pflag = (unsigned char *)e->pflag.p;
                 ba.cd = cdp + c;
+                // bucket 1 pulls work from the queues (measured: the 242k-edge map 2.79 ->
+                // 2.52 ms); bucket 0's runs are too small for the atomics to pay
+                ba.queue = b == 1 ? queues : nullptr;
                 CVL_TRY(bf(e, ba, sms * 16));
                 GrowthArgsT<double> ga{};
                 ga.md = md;
@@ -1189,6 +1210,7 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
                 // few anchors each
                 ga.anchors_per_warp = 1;
                 ga.cd = cdp + c;
+                ga.queue = b == 1 ? queues + 1 : nullptr;
                 CVL_TRY(gf(e, ga, gsmem, sms * 4 * tn.growth_blocks_per_sm));
             }
             CVL_TRY((scan<unsigned, unsigned long long>(e, (const unsigned *)e->count.p, N,

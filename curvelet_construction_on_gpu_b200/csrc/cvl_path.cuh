@@ -218,6 +218,7 @@ struct BundleArgsT {
     unsigned *slot_ctr;                 // slots taken in this chunk (zero before the launch)
     unsigned char *pflag;               // [P]: bit 0 valid, bit 1 close
     const ChunkDims *cd;                // graph runs: the pair range from device memory
+    unsigned *queue;                    // graph runs: the work queue blocks take pair tiles from (0 at start)
 };
 
 constexpr int BUNDLE_THREADS = 128;
@@ -235,7 +236,8 @@ __host__ __device__ inline int bundles_pairs_per_block(int Q, int pair_bytes) {
 // MINB: the resident 256-thread blocks per SM the register allocation is capped for
 // (3 or 4; with 128-thread blocks, twice as many of those). 128 threads measured 1%
 // faster than 256 at the same registers, and shorter blocks free SMs sooner.
-template <typename T, int CPL, int MINB>
+// QUEUE: a graph run's variant, whose persistent grid pulls tiles from a.queue.
+template <typename T, int CPL, int MINB, bool QUEUE = false>
 __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS)) k_bundles(BundleArgsT<T> a) {
     const ModelT<T> &md = a.md;
     constexpr int BW = 2 * 32 * CPL;
@@ -262,7 +264,16 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
     const int A2 = 2 * md.Q + 2;
     const unsigned long long p_begin = a.cd ? a.cd->p_begin : a.p_begin;
     const unsigned long long np = (a.cd ? a.cd->p_end : a.p_end) - p_begin;
-    for (unsigned long long g = (unsigned long long)blockIdx.x * PPB; g < np; g += (unsigned long long)gridDim.x * PPB) {
+    // A graph run's persistent grid pulls tiles of PPB pairs from a device queue; a
+    // direct run's short blocks take their tile by index (and stride, for any grid).
+    __shared__ unsigned s_tile;
+    unsigned tile = blockIdx.x;
+    if constexpr (QUEUE) {
+        if (t == 0) s_tile = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        tile = s_tile;
+    }
+    for (unsigned long long g = (unsigned long long)tile * PPB; g < np;) {
         const unsigned long long q = g + pl;
         if (lane_on && q < np) {
             const unsigned long long p = p_begin + q;
@@ -368,6 +379,13 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
             }
         }
         __syncthreads();
+        if constexpr (QUEUE) {  // the next tile from the queue (every thread has read s_tile above)
+            if (t == 0) s_tile = atomicAdd(a.queue, 1u);
+            __syncthreads();
+            g = (unsigned long long)s_tile * PPB;
+        } else {
+            g += (unsigned long long)gridDim.x * PPB;
+        }
     }
 }
 
@@ -403,6 +421,7 @@ struct GrowthArgsT {
     const unsigned short *cell_rank;    // [CELLS_MAX] best-cell rank of each cell (k_cell_ranks)
     int anchors_per_warp;               // sets the grid: ceil((a_end - a_begin) / (warps per block * this))
     const ChunkDims *cd;                // graph runs: the chunk's anchors and first pair from device memory
+    unsigned *queue;                    // graph runs: the work queue warps take anchors from (0 at start)
 };
 
 // The best-cell ranks of fill_curvelet_info (:202-219), once per run.
@@ -430,7 +449,8 @@ __host__ __device__ inline size_t growth_smem_per_warp(int max_cand, int gms) {
 constexpr int GROWTH_THREADS = 32;
 // records a growth warp reserves in the arena at a time (at most its anchors per warp)
 constexpr int GROWTH_ARENA_CHUNK = 8;
-template <typename T, int CPL, int K, int MINB>
+// QUEUE: a graph run's variant, whose warps pull anchors from a.queue.
+template <typename T, int CPL, int K, int MINB, bool QUEUE = false>
 __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT<T> a) {
     extern __shared__ __align__(16) unsigned char gr_smem[];
     const ModelT<T> &md = a.md;
@@ -469,7 +489,17 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
     const int a_begin = a.cd ? a.cd->a_begin : a.a_begin;
     const int a_end = a.cd ? a.cd->a_end : a.a_end;
     const unsigned long long p_begin = a.cd ? a.cd->p_begin : a.p_begin;
-    for (int i = a_begin + blockIdx.x * wpb + wib; i < a_end; i += gridDim.x * wpb) {
+    // A graph run's persistent grid: each warp pulls its next anchor from a device
+    // queue (dense regions are shared out as they come); a direct run's warps stride.
+    auto next_anchor = [&](int cur) -> int {
+        if constexpr (!QUEUE) return cur + gridDim.x * wpb;
+        unsigned q = 0;
+        if (lane == 0) q = atomicAdd(a.queue, 1u);
+        q = __shfl_sync(FULL, q, 0);
+        return (q < (unsigned)(a_end - a_begin)) ? a_begin + (int)q : a_end;
+    };
+    const int i0 = QUEUE ? next_anchor(0) : a_begin + blockIdx.x * wpb + wib;
+    for (int i = i0; i < a_end; i = next_anchor(i)) {
         const int m = a.B.map[i];
         const int orig = a.B.orig[i];
         const unsigned long long off = a.pair_off[i];
