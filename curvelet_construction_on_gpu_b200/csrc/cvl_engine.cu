@@ -166,6 +166,8 @@ struct cvl_engine {
     };
     std::vector<GraphSlot> graphs;
     bool graphs_on = std::getenv("CVL_NO_GRAPHS") == nullptr;
+    // direct runs on queue-pulling persistent grids (CVL_NO_PERSIST: short blocks)
+    bool persist_on = std::getenv("CVL_NO_PERSIST") == nullptr;
     uint64_t ws_epoch = 0;                         // workspace (re)allocations so far
     uint64_t graph_replays = 0, graph_fallbacks = 0, graph_captures = 0, graph_clock = 0;
     DBuf gdims, gchunks, gread;
@@ -531,7 +533,7 @@ int launch_bundles(cvl_engine *e, BundleArgsT<T> &a, int blocks) {
     // higher-priority stream's blocks get SMs as soon as any block ends
     constexpr int pair_bytes = 2 * 32 * CPL * (int)sizeof(T);
     const long long ppb = bundles_pairs_per_block(a.md.Q, pair_bytes);
-    if (!a.cd) {  // a graph run (device-side range) keeps the given grid, which strides over the pairs
+    if (!a.cd && !a.queue) {  // a graph run or a queue-pulling grid keeps the given grid
         const long long need = ((long long)(a.p_end - a.p_begin) + ppb - 1) / ppb;
         blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
     }
@@ -556,7 +558,7 @@ int launch_growth(cvl_engine *e, GrowthArgsT<T> &a, size_t smem, int blocks) {
         }
     }
     CVL_CUDA(cudaFuncSetAttribute(k_growth<T, CPL, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (!a.cd) {  // a graph run (device-side range) keeps the given grid, which strides over the anchors
+    if (!a.cd && !a.queue) {  // a graph run or a queue-pulling grid keeps the given grid
         // a warp per anchor and anchors_per_warp anchors per warp: short blocks (a
         // higher-priority stream's blocks get SMs as soon as any block ends)
         const long long per_block = (GROWTH_THREADS / 32) * (long long)a.anchors_per_warp;
@@ -610,6 +612,14 @@ void pick_kernels(int cpl, const cvl_tuning &t, bundles_fn<double> &bf, growth_f
             break;
     }
 }
+
+// Whether a direct run of n edges on this engine runs its chunks on persistent grids.
+inline bool persistent_chunks(const cvl_engine *e, long long n) {
+    return e->persist_on && !e->yield_fn && n > (64 << 10);
+}
+// growth warps of a persistent grid at most (SMs x 4 x the largest register budget), for
+// the record arena's chunk tails in the workspace formula
+constexpr unsigned long long PERSIST_GROWTH_WARPS_MAX = 160ull * 4 * 8;
 
 // mode: 0 = full run, 1 = count valid pairs only, 2 = neighbour graph only
 template <typename R>
@@ -782,12 +792,22 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
     const int bblocks = e->prop.multiProcessorCount * 8;
     const int gblocks = e->prop.multiProcessorCount * 8;
 
+    // Without a yield hook (no higher-priority work to make room for), the chunks run on
+    // persistent grids that pull their work from device queues (measured on the 64-map
+    // batch: 509.2 -> 492.1 ms; bundles -3.7%, growth -4.7%). A launch that yields keeps
+    // short blocks, so that a higher-priority stream takes SMs as soon as any block ends.
+    // Runs above 64 Ki edges (smaller ones replay a graph).
+    const int persist_warps = e->prop.multiProcessorCount * 4 * tn.growth_blocks_per_sm;
+    const bool persist = persistent_chunks(e, n) && std::is_same<R, double>::value &&
+                         (unsigned long long)persist_warps <= PERSIST_GROWTH_WARPS_MAX;
     for (int attempt = 0;; ++attempt) {
         // the growth warps reserve the arena in chunks of at most GROWTH_ARENA_CHUNK
         // records, no more than their anchors (anchors_per_warp): the chunk tails they
-        // leave unused are at most one record per anchor plus one chunk per launch
+        // leave unused are at most one record per anchor plus one chunk per launch; a
+        // persistent grid's warp, whatever its anchors, leaves at most one chunk per launch
         unsigned long long cap = std::max<unsigned long long>(e->arena_hint, 4ull * (unsigned long long)n + 4096ull) +
-                                 (unsigned long long)n + (unsigned long long)GROWTH_ARENA_CHUNK * (nchunks + 1);
+                                 (unsigned long long)n + (unsigned long long)GROWTH_ARENA_CHUNK * (nchunks + 1) +
+                                 (persist ? (unsigned long long)GROWTH_ARENA_CHUNK * persist_warps * nchunks : 0ull);
         if (mode == 0) {
             CVL_TRY(e->alloc(e->rec_ids, sizeof(unsigned) * cap * md.gms));
             CVL_TRY(e->alloc(e->rec_k, sizeof(double) * cap * 2));
@@ -807,6 +827,7 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
             CVL_CUDA(cudaMemcpyAsync(&h_poff[c], (unsigned long long *)e->pair_off.p + cstart[c],
                                      sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         CVL_CUDA(cudaStreamSynchronize(s));
+        unsigned *queues = (unsigned *)((unsigned long long *)e->work.p + 3);
         for (int c = 0; c < nchunks; ++c) {
             const int a0 = cstart[c], a1 = cstart[c + 1];
             if (a1 <= a0) continue;
@@ -831,9 +852,13 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
             ba.pslot = (unsigned *)e->pslot.p;
             ba.slot_ctr = slot_ctr;
             ba.pflag = (unsigned char *)e->pflag.p;
+            if (persist) {
+                CVL_CUDA(cudaMemsetAsync(queues, 0, 2 * sizeof(unsigned), s));
+                ba.queue = queues;
+            }
             if (ba.p_end > ba.p_begin) {
                 CVL_CUDA(cudaMemsetAsync(slot_ctr, 0, sizeof(unsigned), s));
-                CVL_TRY(bf(e, ba, bblocks));
+                CVL_TRY(bf(e, ba, persist ? e->prop.multiProcessorCount * 16 : bblocks));
             }
             e->mark("bundles");
             GrowthArgsT<R> ga{};
@@ -860,7 +885,8 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
             ga.err = err;
             ga.cell_rank = (const unsigned short *)e->crank.p;
             ga.anchors_per_warp = tn.anchors_per_warp;
-            CVL_TRY(gf(e, ga, gsmem, gblocks));
+            if (persist) ga.queue = queues + 1;
+            CVL_TRY(gf(e, ga, gsmem, persist ? persist_warps : gblocks));
             e->mark("growth");
         }
 
@@ -980,7 +1006,8 @@ std::vector<WsItem> workspace_plan(const cvl_tuning *tune, unsigned long long ar
     const unsigned long long nchunks = std::max<unsigned long long>((P + per_chunk - 1) / per_chunk, 1ull);
     const unsigned long long cap =
         std::max<unsigned long long>(std::max<unsigned long long>(arena_hint, C), 4ull * n + 4096ull) + n +
-        (unsigned long long)GROWTH_ARENA_CHUNK * (nchunks + 1);
+        (unsigned long long)GROWTH_ARENA_CHUNK * (nchunks + 1) +
+        (n > (64 << 10) ? (unsigned long long)GROWTH_ARENA_CHUNK * PERSIST_GROWTH_WARPS_MAX * nchunks : 0ull);
     add(&E::rec_ids, 4 * cap * (unsigned long long)md.gms);
     add(&E::rec_k, 16 * cap);
     add(&E::rec_meta, 4 * cap);
