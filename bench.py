@@ -76,8 +76,8 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-map-per-launch comparison")
-    ap.add_argument("--no-sweep", action="store_true", help="skip the served rate sweep (configs[3])")
-    ap.add_argument("--no-stress", action="store_true", help="skip the stress stream (configs[4])")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the served rate sweep (20 to 400 maps/s)")
+    ap.add_argument("--no-stress", action="store_true", help="skip the stress stream (dense 4K maps among small ones)")
     ap.add_argument("--no-small", action="store_true", help="skip batched vs plain on the 1,024 small maps")
     ap.add_argument("--rate", type=float, default=50.0, help="served stream: offered maps/s")
     ap.add_argument("--rates", default="20,50,100,200,400", help="served workload: rates to sweep")

@@ -158,8 +158,8 @@ int read_text(const std::string &path, int per_edge, int nthreads, std::vector<T
     // a file that ends in '\n' has no empty last line for getline
     const char *b = buf.data(), *e = buf.data() + buf.size();
     const char *body_end = (e[-1] == '\n') ? e - 1 : e;
-    // an empty body, or one that still ends in '\n' (an empty last line), is the
-    // exact reader's to judge
+    // an empty body, or one that still ends in '\n' (an empty last line), goes to the
+    // exact reader
     if (body_end == b || body_end[-1] == '\n') return read_stream(path, per_edge, out);
     const int NT = std::max(1, std::min(nthreads, (int)((body_end - b) >> 16) + 1));
     std::vector<const char *> cut(NT + 1);
