@@ -123,7 +123,7 @@ struct cvl_engine {
     DBuf bx, by, bth, bsp, bcp, bsm, bcm, bcell, bmap;
     DBuf ncand, deg, pair_off, csr_ids, csr_d2, rec_ids, rec_k, rec_meta, count, out_off;
     DBuf chains, info, stats, err, work, scratch, scratch_chain, scratch_res, scan_tmp, flush, deg_orig, off_orig,
-        gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, pslot, chunk_start, crank;
+        gids, gd2, run_cnt, rec_base, pcls, pflag, pair_anchor, atrig, bund, chunk_start, crank;
     cvl_tuning tune[CVL_TUNING_BUCKETS];                   // per size bucket of the batch
     cvl_yield_fn yield_fn = nullptr;                       // called between chunks (serving)
     void *yield_ctx = nullptr;
@@ -250,7 +250,7 @@ struct cvl_engine {
         DBuf *all[] = {&edges, &map_off, &ehash, &bcount, &bstart, &bfill, &pos_of, &orig_of, &bx, &by, &bth, &bsp,
                        &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
                        &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
-                       &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &pslot, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
+                       &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
                        &pb_max, &pb_valid, &chains_alt, &info_alt, &gdims, &gchunks, &gread};
         for (DBuf *b : all) {
             if (b->p) cudaFreeAsync(b->p, stream);
@@ -668,7 +668,7 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
     CVL_TRY(e->alloc(e->out_off, sizeof(unsigned long long) * (n + 1)));
     CVL_TRY(e->alloc(e->stats, sizeof(MapStats) * M));
     CVL_TRY(e->alloc(e->err, sizeof(unsigned) * 4));
-    CVL_TRY(e->alloc(e->work, sizeof(unsigned long long) * 4));  // arena counter, bundle slot counter
+    CVL_TRY(e->alloc(e->work, sizeof(unsigned long long) * 4));  // arena counter, -, work queues
 
     BinnedT<R> B;
     B.x = (R *)e->bx.p;
@@ -787,8 +787,6 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
     const unsigned long long max_chunk_pairs = per_chunk + (unsigned long long)ro.max_deg + 1;
     const unsigned long long chunk_cap = std::min<unsigned long long>(P + 1, max_chunk_pairs);
     CVL_TRY(e->alloc(e->bund, sizeof(R) * 64 * (size_t)cpl * chunk_cap));
-    CVL_TRY(e->alloc(e->pslot, sizeof(unsigned) * chunk_cap));
-    unsigned *slot_ctr = (unsigned *)((unsigned long long *)e->work.p + 2);
     const int bblocks = e->prop.multiProcessorCount * 8;
     const int gblocks = e->prop.multiProcessorCount * 8;
 
@@ -849,15 +847,12 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
             ba.pcls = (const unsigned char *)e->pcls.p;
             ba.atrig = (const R *)e->atrig.p;
             ba.bund = (R *)e->bund.p;
-            ba.pslot = (unsigned *)e->pslot.p;
-            ba.slot_ctr = slot_ctr;
             ba.pflag = (unsigned char *)e->pflag.p;
             if (persist) {
                 CVL_CUDA(cudaMemsetAsync(queues, 0, 2 * sizeof(unsigned), s));
                 ba.queue = queues;
             }
             if (ba.p_end > ba.p_begin) {
-                CVL_CUDA(cudaMemsetAsync(slot_ctr, 0, sizeof(unsigned), s));
                 CVL_TRY(bf(e, ba, persist ? e->prop.multiProcessorCount * 16 : bblocks));
             }
             e->mark("bundles");
@@ -873,7 +868,6 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
             ga.pcls = (const unsigned char *)e->pcls.p;
             ga.pflag = (const unsigned char *)e->pflag.p;
             ga.bund = (const R *)e->bund.p;
-            ga.pslot = (const unsigned *)e->pslot.p;
             ga.rec = rec;
             ga.arena_cap = cap;
             ga.arena_ctr = arena_ctr;
@@ -1001,7 +995,6 @@ std::vector<WsItem> workspace_plan(const cvl_tuning *tune, unsigned long long ar
     const unsigned long long chunk_cap =
         std::min<unsigned long long>(P + 1, per_chunk + (unsigned long long)md.max_cand + 1);
     add(&E::bund, R * 64 * (unsigned long long)cpl * chunk_cap, true);
-    add(&E::pslot, 4 * chunk_cap, true);
     // the record arena (run_pipeline's cap, with room for C records)
     const unsigned long long nchunks = std::max<unsigned long long>((P + per_chunk - 1) / per_chunk, 1ull);
     const unsigned long long cap =
@@ -1131,7 +1124,6 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
         unsigned *err = (unsigned *)e->err.p;
         MapStats *stats = (MapStats *)e->stats.p;
         unsigned long long *arena_ctr = (unsigned long long *)e->work.p;
-        unsigned *slot_ctr = (unsigned *)((unsigned long long *)e->work.p + 2);
         const RunDims *dd = (const RunDims *)e->gdims.p;
         ChunkDims *cdp = (ChunkDims *)e->gchunks.p;
         const int sms = e->prop.multiProcessorCount;
@@ -1195,7 +1187,6 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
             // the chunks' work queues (bundle pair tiles, growth anchors)
             unsigned *queues = (unsigned *)((unsigned long long *)e->work.p + 3);
             for (int c = 0; c < cap.K; ++c) {
-                CVL_CUDA(cudaMemsetAsync(slot_ctr, 0, sizeof(unsigned), s));
                 CVL_CUDA(cudaMemsetAsync(queues, 0, 2 * sizeof(unsigned), s));
                 BundleArgsT<double> ba{};
                 ba.md = md;
@@ -1205,8 +1196,6 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
                 ba.pcls = (const unsigned char *)e->pcls.p;
                 ba.atrig = (const double *)e->atrig.p;
                 ba.bund = (double *)e->bund.p;
-                ba.pslot = (unsigned *)e->pslot.p;
-                ba.slot_ctr = slot_ctr;
                 ba.pflag = (unsigned char *)e->pflag.p;
                 ba.cd = cdp + c;
                 // bucket 1 pulls work from the queues (measured: the 242k-edge map 2.79 ->
@@ -1222,7 +1211,6 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
                 ga.pcls = (const unsigned char *)e->pcls.p;
                 ga.pflag = (const unsigned char *)e->pflag.p;
                 ga.bund = (const double *)e->bund.p;
-                ga.pslot = (const unsigned *)e->pslot.p;
                 ga.rec = rec;
                 ga.arena_cap = arena_cap;
                 ga.arena_ctr = arena_ctr;

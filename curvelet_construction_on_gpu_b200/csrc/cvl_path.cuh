@@ -96,6 +96,12 @@ __device__ __forceinline__ void bundle_cell_tt(const Model &md, double DX2, doub
 // dx2sq[i] = dx2[i]^2 are the per-i constants; store(i, bmin, bmax) takes each
 // cell. Returns whether any cell of the column is open (bmax > bmin).
 // k_bundles and k_pair_bundles (form 0) both run this function.
+#ifndef CVL_BUNDLE_UNROLL
+#define CVL_BUNDLE_UNROLL 1
+#endif
+#define CVL_PRAGMA_(x) _Pragma(#x)
+#define CVL_UNROLL_(n) CVL_PRAGMA_(unroll n)
+#define CVL_BUNDLE_UNROLL_PRAGMA CVL_UNROLL_(CVL_BUNDLE_UNROLL)
 template <class Store>
 __device__ __forceinline__ bool bundle_column_fp64(const Model &md, const double *dx2, const double *dx2_2,
                                                    const double *dx2sq, const PairGeom &g2, double tt, double s_m,
@@ -111,7 +117,7 @@ __device__ __forceinline__ bool bundle_column_fp64(const Model &md, const double
     const double n_lo = g2.branch1 ? g2.sin_m_DY : g2.sin_p_DY;
     const double n_hi = g2.branch1 ? g2.sin_p_DY : g2.sin_m_DY;
     bool open = false;
-#pragma unroll 1  // (measured: unrolling by 2 spills under the 64-register cap and is 2.6% slower)
+CVL_BUNDLE_UNROLL_PRAGMA  // (measured: unrolling by 2 spills under the 64-register cap and is 2.6% slower)
     for (int i = 0; i < md.P; ++i) {
         const double delta_x2 = dx2[i], d2_2 = dx2_2[i];
         const double ttmdx2_2 = tt2 - d2_2;                          // 2 ttmdx2
@@ -213,9 +219,7 @@ struct BundleArgsT {
     const int *pair_anchor;
     const unsigned char *pcls;
     const T *atrig;                     // [N][2Q+2]: sin(T2t_j), cos(T2t_j), cos(T2), sin(T2)
-    T *bund;                            // [slots][2][32 * CPL]: valid non-close pairs only, compacted
-    unsigned *pslot;                    // [p_end - p_begin]: bund slot of each valid non-close pair
-    unsigned *slot_ctr;                 // slots taken in this chunk (zero before the launch)
+    T *bund;                            // [chunk pairs][2][32 * CPL]: written for valid non-close pairs only
     unsigned char *pflag;               // [P]: bit 0 valid, bit 1 close
     const ChunkDims *cd;                // graph runs: the pair range from device memory
     unsigned *queue;                    // graph runs: the work queue blocks take pair tiles from (0 at start)
@@ -244,17 +248,16 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
     extern __shared__ __align__(16) unsigned char bn_smem[];
     T *s_b = (T *)bn_smem;  // [PPB][BW]: the block's bundles until their validity is known
     __shared__ T s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
-    __shared__ unsigned char s_open[BUNDLE_THREADS];
-    __shared__ unsigned char s_src[BUNDLE_THREADS];  // staged pair of each compacted slot of the block
-    __shared__ unsigned s_rel[BUNDLE_THREADS];       // slot of each staged pair in the block's run (~0: none)
-    __shared__ unsigned s_nv, s_base;
+    // each staged pair's flags (bit 0 open, bit 1 close), two sets used in turn by
+    // successive tiles: a tile clears the other set after its first barrier
+    __shared__ unsigned char s_flag[2][BUNDLE_THREADS];
     for (int i = threadIdx.x; i < md.P; i += blockDim.x) {
         const T d = grid_offset(md.sx, i, md.P);  // delta_x2 (:697)
         s_dx2[i] = d;
         s_dx2_2[i] = T(2) * d;
         s_dx2sq[i] = d * d;
     }
-    for (int t = threadIdx.x; t < BUNDLE_THREADS; t += blockDim.x) s_open[t] = 0;
+    for (int t = threadIdx.x; t < BUNDLE_THREADS; t += blockDim.x) s_flag[0][t] = s_flag[1][t] = 0;
     __syncthreads();
     const int t = threadIdx.x;
     const int PPB = bundles_pairs_per_block(md.Q, BW * (int)sizeof(T));
@@ -273,11 +276,14 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
         __syncthreads();
         tile = s_tile;
     }
+    int par = 0;  // the flag set of this tile
     for (unsigned long long g = (unsigned long long)tile * PPB; g < np;) {
         const unsigned long long q = g + pl;
         if (lane_on && q < np) {
             const unsigned long long p = p_begin + q;
-            if (!(a.pcls[p] & 4u)) {
+            if (a.pcls[p] & 4u) {
+                if (jl == 0) s_flag[par][pl] = 2u;  // close: valid, keeps the default bundle, not written
+            } else {
                 const int ia = a.pair_anchor[p];
                 const int nn = a.csr_ids[p];
                 const T *at = a.atrig + (size_t)ia * A2;
@@ -330,62 +336,42 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                                                   dst[32 * CPL + i * md.Q + jl] = hi;
                                               });
                 }
-                if (open) s_open[pl] = 1;
+                if (open) s_flag[par][pl] = 1u;
             }
         }
         __syncthreads();
-        // warp 0: each pair's flags; the valid non-close pairs take consecutive
-        // slots of the chunk's compacted bundle buffer (one atomic per block)
-        if (t < 32) {
-            unsigned nv = 0;
-            for (int k0 = 0; k0 < PPB; k0 += 32) {
-                const int k = k0 + t;
-                const unsigned long long qq = g + k;
-                bool need = false;
-                if (k < PPB && qq < np) {
-                    const unsigned long long p = p_begin + qq;
-                    const bool closep = (a.pcls[p] & 4u) != 0;
-                    const bool valid = closep || s_open[k] != 0;
-                    a.pflag[p] = (unsigned char)((valid ? 1u : 0u) | (closep ? 2u : 0u));
-                    need = valid && !closep;
-                }
-                const unsigned bal = __ballot_sync(FULL, need);
-                if (k < PPB) {
-                    s_open[k] = 0;
-                    s_rel[k] = need ? nv + __popc(bal & ((1u << t) - 1u)) : ~0u;
-                    if (need) s_src[s_rel[k]] = (unsigned char)k;
-                }
-                nv += __popc(bal);
+        // Each pair's flags, and the valid non-close pairs' bundles to their pairs'
+        // slots of the chunk's bundle buffer (a slot per pair of the chunk; only the
+        // valid non-close ones are written), a warp per pair at a time, 16-byte stores.
+        for (int k = t; k < PPB; k += BUNDLE_THREADS) {
+            if (g + k < np) {
+                const unsigned f = s_flag[par][k];
+                a.pflag[p_begin + g + k] = (unsigned char)((f ? 1u : 0u) | (f & 2u));
             }
-            unsigned base = 0;
-            if (t == 0 && nv) base = atomicAdd(a.slot_ctr, nv);
-            base = __shfl_sync(FULL, base, 0);
-            if (t == 0) {
-                s_nv = nv;
-                s_base = base;
-            }
-            for (int k = t; k < PPB; k += 32)
-                if (s_rel[k] != ~0u) a.pslot[g + k] = base + s_rel[k];
+            s_flag[par ^ 1][k] = 0;  // the next tile's set (last read before the previous barrier)
         }
-        __syncthreads();
-        // the valid pairs' bundles to their slots: one contiguous run per block, 16-byte stores
         {
             constexpr int VP = BW * (int)sizeof(T) / 16;  // 16-byte words per pair
-            const int nv = (int)s_nv;
-            uint4 *gdst = (uint4 *)(a.bund + (size_t)s_base * BW);
-            for (int v = t; v < nv * VP; v += BUNDLE_THREADS) {
-                const int r = v / VP, w = v - r * VP;
-                gdst[v] = ((const uint4 *)(s_b + (size_t)s_src[r] * BW))[w];
+            const int w = t >> 5, lane = t & 31;
+            for (int k = w; k < PPB; k += BUNDLE_THREADS / 32) {
+                if (g + k < np && s_flag[par][k] == 1u) {
+                    uint4 *gdst = (uint4 *)(a.bund + (size_t)(g + k) * BW);
+                    const uint4 *src = (const uint4 *)(s_b + (size_t)k * BW);
+                    for (int v = lane; v < VP; v += 32) gdst[v] = src[v];
+                }
             }
         }
-        __syncthreads();
-        if constexpr (QUEUE) {  // the next tile from the queue (every thread has read s_tile above)
+        // the next tile (from the queue: every thread read s_tile before the barrier above)
+        if constexpr (QUEUE) {
             if (t == 0) s_tile = atomicAdd(a.queue, 1u);
-            __syncthreads();
+        }
+        __syncthreads();  // s_b, s_flag[par] and s_tile are free again
+        if constexpr (QUEUE) {
             g = (unsigned long long)s_tile * PPB;
         } else {
             g += (unsigned long long)gridDim.x * PPB;
         }
+        par ^= 1;
     }
 }
 
@@ -407,8 +393,7 @@ struct GrowthArgsT {
     const int *csr_ids;
     const unsigned char *pcls;
     const unsigned char *pflag;
-    const T *bund;                      // the chunk's compacted bundles (k_bundles)
-    const unsigned *pslot;              // [chunk pairs]: bund slot of each valid non-close pair
+    const T *bund;                      // the chunk's bundles (k_bundles), by chunk-local pair index
     Records rec;                        // record arena
     unsigned long long arena_cap;
     unsigned long long *arena_ctr;
@@ -525,9 +510,9 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
             const unsigned b1 = __ballot_sync(FULL, t1);
             if (t0 || t1) {
                 const int slot = t0 ? ns_run0 + __popc(b0 & lt_mask) : md.max_cand - 1 - (ns_run1 + __popc(b1 & lt_mask));
-                // a valid non-close pair's bundle is at its compacted slot; a close pair
-                // keeps the default bundle and reads none
-                seed_q[slot] = (fl & 2u) ? CLOSE_BIT : a.pslot[off + k - p_begin];
+                // a valid non-close pair's bundle is at its chunk-local pair index (below
+                // 2^30); a close pair keeps the default bundle and reads none
+                seed_q[slot] = (fl & 2u) ? CLOSE_BIT : (unsigned)(off + k - p_begin);
                 seed_orig[slot] = a.B.orig[a.csr_ids[off + k]];
             }
             ns_run0 += __popc(b0);
