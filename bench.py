@@ -52,16 +52,17 @@ METRIC = "edges/s"
 # per computed (non-close) pair: 63 cells x 20 FP64 flops, divisions counted as 1
 FLOPS_PER_PAIR_CELL = 20
 # DRAM bytes of k_bundles per computed pair, from one ncu capture of the kernel
-# (--set full) on the 242k-edge 1920x1080 map: dram__bytes_read.sum 0.334940 GB +
-# dram__bytes_write.sum 2.183544 GB over 2,176,780 non-close pairs. The traffic is
-# the bundle write (1,008 B per pair) plus the pair/anchor reads, so it scales with
-# the pairs a launch processes.
-BUNDLE_DRAM_BYTES_PER_PAIR = (0.334940e9 + 2.183544e9) / 2_176_780
+# (--set full, profiles/k_bundles_k_growth_persistent_hd.md) on the 242k-edge
+# 1920x1080 map: dram__bytes_read.sum 0.153845 GB + dram__bytes_write.sum 1.428184 GB
+# over 2,176,780 non-close pairs. The traffic is the valid pairs' bundle writes
+# (1,008 B each, about half of the computed pairs) plus the pair/anchor reads, so it
+# scales with the pairs a launch processes.
+BUNDLE_DRAM_BYTES_PER_PAIR = (0.153845e9 + 1.428184e9) / 2_176_780
 # FP64-pipe instructions of k_bundles per cell, from the same capture: the pipe was
-# active 48.72% of 0.952480 ms on 148 SMs (each issues 2 FP64 warp-instructions a
-# cycle at 1.965 GHz), 30.57 active lanes per warp-instruction, 2,176,780 x 63 cells.
-# A division costs about 10 of them, which the algorithmic count above takes as 1 flop.
-BUNDLE_FP64_INSTR_PER_CELL = 0.4872 * 0.952480e-3 * 148 * 2 * 1.965e9 * 30.57 / (2_176_780 * 63)
+# active 51.154% of 1,852,462 active cycles per SM on 148 SMs (each issues 2 FP64
+# warp-instructions a cycle), 30.72 active lanes per warp-instruction, 2,176,780 x 63
+# cells. A division costs about 10 of them, which the algorithmic count takes as 1 flop.
+BUNDLE_FP64_INSTR_PER_CELL = 0.51154 * 1_852_462 * 148 * 2 * 30.72 / (2_176_780 * 63)
 
 
 def _args():
@@ -654,6 +655,7 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
     stats = last.stats()
     n_curv = int(stats["num_curvelets"])
     nonclose = int(stats["total_pairs"]) - int(stats["close_pairs"])
+    valid_nonclose = int(stats["valid_pairs"]) - int(stats["close_pairs"])
     last.close()
 
     plain = None
@@ -757,7 +759,9 @@ def run_ours(args, maps, cfg, world, rank, local, pg):
                      "traffic_unit": "bytes per launch",
                      "traffic_source": "ncu dram bytes of k_bundles on the 242k-edge map, per non-close pair, "
                                        "times this workload's pairs per launch",
-                     "algorithmic_bytes": 1008.0 * nonclose / launches_b,
+                     "algorithmic_bytes": (1008.0 * valid_nonclose + 10.0 * nonclose) / launches_b,
+                     "algorithmic_bytes_note": "1,008 B of bundle per valid non-close pair written, 10 B per "
+                                               "computed pair of ids and flags",
                      "fp64_pipe": {
                          "instr_per_cell": BUNDLE_FP64_INSTR_PER_CELL,
                          "frac": (BUNDLE_FP64_INSTR_PER_CELL * 63 * nonclose / (curv_ms / 1e3)

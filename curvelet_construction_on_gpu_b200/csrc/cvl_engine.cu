@@ -449,7 +449,8 @@ cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind
 // Device -> page-locked host copy of results. RESULT_COPY_SM (the default) copies with a
 // small kernel (RESULT_COPY_BLOCKS blocks), which slows concurrent path kernels far less
 // than a copy-engine transfer does; CVL_RESULT_COPY=ce in the environment selects the
-// copy engine (cudaMemcpyAsync in pieces). Sizes are multiples of 4 bytes.
+// copy engine (cudaMemcpyAsync in pieces). A copy that no path kernel runs beside
+// (alone) takes the copy engine, which is faster (53 against 38 GB/s measured).
 constexpr int RESULT_COPY_BLOCKS = 16;
 const bool g_result_copy_sm = [] {
     const char *v = std::getenv("CVL_RESULT_COPY");
@@ -458,9 +459,9 @@ const bool g_result_copy_sm = [] {
 
 cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
 
-inline cudaError_t copy_result_to_host(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+inline cudaError_t copy_result_to_host(void *dst, const void *src, size_t bytes, cudaStream_t s, bool alone = false) {
     if (!bytes) return cudaSuccess;
-    if (!g_result_copy_sm || (bytes & 3) || (((uintptr_t)src | (uintptr_t)dst) & 3))
+    if (alone || !g_result_copy_sm || (bytes & 3) || (((uintptr_t)src | (uintptr_t)dst) & 3))
         return copy_pieces(dst, src, bytes, cudaMemcpyDeviceToHost, s);
     const int wide = ((((uintptr_t)src | (uintptr_t)dst) | bytes) & 15) == 0 ? 1 : 0;
     k_copy_to_host<<<RESULT_COPY_BLOCKS, 256, 0, s>>>(src, dst, bytes, wide);
@@ -2888,12 +2889,13 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
             r->info_p = e->pinned->get(sizeof(double) * (C ? C : 1) * 10);
             if (!r->chains_p || !r->info_p)
                 return cleanup(fail(CVL_ENOMEM, "page-locked result buffers could not be allocated"));
-            if (C) {  // by SM threads beside the next group's compute (copy_result_to_host)
+            if (C) {  // by SM threads beside the next group's compute; the last group's alone
+                const bool alone = g == G - 1;
                 cudaError_t ce = copy_result_to_host(r->chains_p, (const unsigned *)e->chains.p + c0 * W,
-                                                     sizeof(unsigned) * C * W, e->copy_stream);
+                                                     sizeof(unsigned) * C * W, e->copy_stream, alone);
                 if (ce == cudaSuccess)
                     ce = copy_result_to_host(r->info_p, (const double *)e->info.p + c0 * 10,
-                                             sizeof(double) * C * 10, e->copy_stream);
+                                             sizeof(double) * C * 10, e->copy_stream, alone);
                 if (ce != cudaSuccess) return cleanup(fail(CVL_ECUDA, std::string("result copy: ") + cudaGetErrorString(ce)));
             }
             const MapStats &st = ro.stats[k];
