@@ -137,8 +137,10 @@ struct cvl_engine {
     unsigned long long dev_generation = ~0ull;
     cudaEvent_t dev_done = nullptr;
     // cvl_run_maps: the other group's outputs, a copy stream and its events
-    DBuf chains_alt, info_alt;
+    DBuf chains_alt, info_alt, edges_alt;
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t upload_stream = nullptr;  // cvl_run_maps: the next group's edges
+    cudaEvent_t uploaded[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
     cudaEvent_t computed[2] = {nullptr, nullptr};
     cudaEvent_t copied[2] = {nullptr, nullptr};
     // downstream stage (link graph, contour fragments)
@@ -251,7 +253,7 @@ struct cvl_engine {
                        &bcp, &bsm, &bcm, &bcell, &bmap, &ncand, &deg, &pair_off, &csr_ids, &csr_d2, &rec_ids,
                        &rec_k, &rec_meta, &count, &out_off, &chains, &info, &stats, &err, &work, &scratch,
                        &scratch_chain, &scratch_res, &run_cnt, &rec_base, &pcls, &pflag, &pair_anchor, &atrig, &bund, &chunk_start, &crank, &scan_tmp, &flush, &deg_orig, &off_orig, &gids, &gd2, &pairs_in, &pb_min,
-                       &pb_max, &pb_valid, &chains_alt, &info_alt, &gdims, &gchunks, &gread};
+                       &pb_max, &pb_valid, &chains_alt, &info_alt, &edges_alt, &gdims, &gchunks, &gread};
         for (DBuf *b : all) {
             if (b->p) cudaFreeAsync(b->p, stream);
             b->p = nullptr;
@@ -1514,11 +1516,15 @@ void cvl_engine_destroy(cvl_engine *e) {
     if (e->dev_done) cudaEventDestroy(e->dev_done);
     if (e->copy_stream) {
         cudaStreamSynchronize(e->copy_stream);
+        cudaStreamSynchronize(e->upload_stream);
         for (int k = 0; k < 2; ++k) {
             cudaEventDestroy(e->computed[k]);
             cudaEventDestroy(e->copied[k]);
+            cudaEventDestroy(e->uploaded[k]);
+            cudaEventDestroy(e->consumed[k]);
         }
         cudaStreamDestroy(e->copy_stream);
+        cudaStreamDestroy(e->upload_stream);
     }
     cudaStreamDestroy(e->stream);
     if (e->pool) cudaMemPoolDestroy(e->pool);
@@ -2828,9 +2834,12 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
     CVL_CUDA(cudaSetDevice(e->device));
     if (!e->copy_stream) {
         CVL_CUDA(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+        CVL_CUDA(cudaStreamCreateWithFlags(&e->upload_stream, cudaStreamNonBlocking));
         for (int k = 0; k < 2; ++k) {
             CVL_CUDA(cudaEventCreateWithFlags(&e->computed[k], cudaEventDisableTiming));
             CVL_CUDA(cudaEventCreateWithFlags(&e->copied[k], cudaEventDisableTiming));
+            CVL_CUDA(cudaEventCreateWithFlags(&e->uploaded[k], cudaEventDisableTiming));
+            CVL_CUDA(cudaEventCreateWithFlags(&e->consumed[k], cudaEventDisableTiming));
         }
     }
 
@@ -2839,26 +2848,95 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
     CVL_TRY(make_model(e, p, p ? p->nrad : 0.0, 3u, p ? p->max_candidates : 0u, md, cpl));
     const int W = md.gms + 1;
     const long long total = off[num_maps];
-    if (group_edges <= 0) group_edges = std::min<long long>(std::max<long long>(total / 6, 1LL << 20), 8LL << 20);
+    const bool default_groups = group_edges <= 0;
+    if (default_groups) group_edges = std::min<long long>(std::max<long long>(total / 6, 1LL << 20), 8LL << 20);
 
-    // groups of whole maps, about group_edges edges each
-    std::vector<int32_t> gstart = {0};
+    // The maps in the order they run: by default the smallest maps, about a sixteenth
+    // of the edges (at least 256 Ki), are held back for a last group of their own, so
+    // that the result copies left after the last compute are short.
+    std::vector<int32_t> order;
+    order.reserve(num_maps);
+    std::vector<char> tail(num_maps, 0);
+    if (default_groups && total > group_edges && num_maps > 1) {
+        std::vector<int32_t> by_size(num_maps);
+        for (int32_t m = 0; m < num_maps; ++m) by_size[m] = m;
+        std::stable_sort(by_size.begin(), by_size.end(), [&](int32_t a, int32_t b) { return counts[a] < counts[b]; });
+        const long long want = std::max<long long>(total / 16, 256LL << 10);
+        long long got = 0;
+        for (int32_t k = 0; k + 1 < num_maps && got < want; ++k) {
+            tail[by_size[k]] = 1;
+            got += counts[by_size[k]];
+        }
+    }
     for (int32_t m = 0; m < num_maps; ++m)
-        if (m + 1 < num_maps && off[m + 1] - off[gstart.back()] >= group_edges) gstart.push_back(m + 1);
+        if (!tail[m]) order.push_back(m);
+    const size_t body = order.size();
+    for (int32_t m = 0; m < num_maps; ++m)
+        if (tail[m]) order.push_back(m);
+
+    // groups of whole maps (positions in order), about group_edges edges each; the held
+    // back maps form the last group
+    std::vector<int32_t> gstart = {0};
+    long long acc = 0;
+    for (size_t k = 0; k < order.size(); ++k) {
+        acc += counts[order[k]];
+        const bool cut = (k + 1 == body) || (k + 1 < order.size() && acc >= group_edges && k + 1 < body);
+        if (k + 1 < order.size() && cut) {
+            gstart.push_back((int32_t)(k + 1));
+            acc = 0;
+        }
+    }
     gstart.push_back(num_maps);
     const int G = (int)gstart.size() - 1;
+    long long max_group = 0;
+    for (int g = 0; g < G; ++g) {
+        long long ng = 0;
+        for (int k = gstart[g]; k < gstart[g + 1]; ++k) ng += counts[order[k]];
+        max_group = std::max(max_group, ng);
+    }
+
+    // Two device edge buffers: a group's edges go up on the upload stream while the
+    // group before computes (a host-to-device copy beside the path's kernels slows them
+    // by 2% at most).
+    DBuf *ebuf[2] = {&e->edges, &e->edges_alt};
+    CVL_TRY(e->alloc(e->edges, sizeof(double) * (size_t)max_group * edge_data_sz));
+    CVL_TRY(e->alloc(e->edges_alt, sizeof(double) * (size_t)max_group * edge_data_sz));
+    for (int b = 0; b < 2; ++b) CVL_CUDA(cudaEventRecord(e->consumed[b], e->stream));
+    auto upload_group = [&](int g) -> int {
+        const int b = g & 1;
+        CVL_CUDA(cudaStreamWaitEvent(e->upload_stream, e->consumed[b], 0));
+        size_t at = 0;
+        for (int k = gstart[g]; k < gstart[g + 1];) {
+            // runs of maps that lie back to back in the host array go in one copy
+            int k1 = k + 1;
+            while (k1 < gstart[g + 1] && order[k1] == order[k1 - 1] + 1) ++k1;
+            const size_t rows = (size_t)(off[order[k1 - 1] + 1] - off[order[k]]);
+            CVL_CUDA(cudaMemcpyAsync((double *)ebuf[b]->p + at * edge_data_sz,
+                                     edges + (size_t)off[order[k]] * edge_data_sz, sizeof(double) * rows * edge_data_sz,
+                                     cudaMemcpyHostToDevice, e->upload_stream));
+            at += rows;
+            k = k1;
+        }
+        CVL_CUDA(cudaEventRecord(e->uploaded[b], e->upload_stream));
+        return CVL_OK;
+    };
 
     std::vector<cvl_result *> res(num_maps, nullptr);
     auto cleanup = [&](int rc) {
         cudaStreamSynchronize(e->copy_stream);
+        cudaStreamSynchronize(e->upload_stream);
         for (cvl_result *r : res) delete r;
         return rc;
     };
     double device_ms = 0.0;
     bool copy_pending[2] = {false, false};
+    if (int rc = upload_group(0)) return cleanup(rc);
     for (int g = 0; g < G; ++g) {
         const int m0 = gstart[g], m1 = gstart[g + 1], M = m1 - m0;
         const int buf = g & 1;
+        if (g + 1 < G) {
+            if (int rc = upload_group(g + 1)) return cleanup(rc);
+        }
         // this group's outputs go to the buffer pair the group before last used:
         // its copies must be done before run_pipeline may overwrite or regrow it
         if (g > 0) {
@@ -2867,14 +2945,20 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
         }
         if (copy_pending[buf]) CVL_CUDA(cudaStreamWaitEvent(e->stream, e->copied[buf], 0));
         std::vector<int32_t> mo(M + 1, 0);
-        for (int k = 0; k < M; ++k) mo[k + 1] = mo[k] + counts[m0 + k];
+        for (int k = 0; k < M; ++k) mo[k + 1] = mo[k] + counts[order[m0 + k]];
         const int n = mo[M];
-        int rc = upload(e, edges + (size_t)off[m0] * edge_data_sz, n, edge_data_sz, mo);
+        int rc = e->alloc(e->map_off, sizeof(int) * mo.size());
         if (rc != CVL_OK) return cleanup(rc);
+        if (cudaMemcpyAsync(e->map_off.p, mo.data(), sizeof(int) * mo.size(), cudaMemcpyHostToDevice, e->stream) !=
+                cudaSuccess ||
+            cudaStreamWaitEvent(e->stream, e->uploaded[buf], 0) != cudaSuccess)
+            return cleanup(fail(CVL_ECUDA, "map offsets upload failed"));
         RunOut ro;
-        rc = run_pipeline(e, (const double *)e->edges.p, n, edge_data_sz, (const int *)e->map_off.p, mo, md, cpl, 0,
+        rc = run_pipeline(e, (const double *)ebuf[buf]->p, n, edge_data_sz, (const int *)e->map_off.p, mo, md, cpl, 0,
                           false, ro);
         if (rc != CVL_OK) return cleanup(rc);
+        if (cudaEventRecord(e->consumed[buf], e->stream) != cudaSuccess)
+            return cleanup(fail(CVL_ECUDA, "event record failed"));
         e->collect_marks();
         device_ms += e->last_device_ms;
         if (cudaEventRecord(e->computed[buf], e->stream) != cudaSuccess ||
@@ -2883,7 +2967,7 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
         for (int k = 0; k < M; ++k) {
             const unsigned long long c0 = ro.cv_off[k], C = ro.cv_off[k + 1] - c0;
             cvl_result *r = new cvl_result();
-            res[m0 + k] = r;
+            res[order[m0 + k]] = r;
             r->pool = e->pinned;
             r->chains_p = e->pinned->get(sizeof(unsigned) * (C ? C : 1) * W);
             r->info_p = e->pinned->get(sizeof(double) * (C ? C : 1) * 10);
@@ -2908,7 +2992,7 @@ extern "C" int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *c
             v.total_neighbor_pairs = (int64_t)st.pairs;
             v.max_num_of_neighbors = st.max_deg;
             v.truncated_anchors = st.truncated;
-            v.num_edges = (uint32_t)counts[m0 + k];
+            v.num_edges = (uint32_t)counts[order[m0 + k]];
             v.flags = v.truncated_anchors ? CVL_FLAG_TRUNCATED : 0u;
         }
         if (cudaEventRecord(e->copied[buf], e->copy_stream) != cudaSuccess)

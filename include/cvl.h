@@ -307,10 +307,13 @@ void cvl_batch_result_free(cvl_batch_result *r);
  * would return it (out[m], freed with cvl_result_free). edges holds the maps'
  * rows back to back (counts[m] rows each). The maps go through the path in groups
  * of whole maps of about group_edges edges (<= 0: a sixth of the total, clamped
- * to [1 Mi, 8 Mi]); while one group computes on the engine's stream, the previous
- * group's results are copied to page-locked host memory on a second stream, so
- * the result copies overlap the compute. Each view's device_ms is the whole
- * call's device time. On error nothing is returned. */
+ * to [1 Mi, 8 Mi], with the smallest maps, about a sixteenth of the edges, held
+ * back for a last group of their own). While one group computes on the engine's
+ * stream, the next group's edges go up on a second stream and the previous
+ * group's results come down to page-locked host memory on a third, so both
+ * overlap the compute (page-locked input edges make the uploads asynchronous).
+ * Each view's device_ms is the whole call's device time. On error nothing is
+ * returned. */
 int cvl_run_maps(cvl_engine *e, const double *edges, const int32_t *counts, int32_t num_maps, int32_t edge_data_sz,
                  const cvl_params *p, int64_t group_edges, cvl_result **out);
 
