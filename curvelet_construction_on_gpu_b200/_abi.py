@@ -155,7 +155,8 @@ SIGNATURES = [
     ("cvl_debug_fail_allocations", C.c_int, [C.c_int64]),
     ("cvl_check_pair_bundles_literal", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), _dp, _dp,
                                                  C.POINTER(C.c_uint8), C.POINTER(C.c_int32)]),
-    ("cvl_check_transport_cells", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), _dp, C.POINTER(C.c_int32)]),
+    ("cvl_check_transport_cells", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(CvlParams), C.c_int32, _dp,
+                                            C.POINTER(C.c_int32)]),
     ("cvl_pair_bundles_noalloc", C.c_int, [_dp, C.c_int32, C.POINTER(CvlParams), _dp, _dp, C.POINTER(C.c_uint8),
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
     ("cvl_batch_upload", C.c_int, [_vp, _dp, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_vp)]),

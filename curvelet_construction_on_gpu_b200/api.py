@@ -453,9 +453,12 @@ class Engine:
         check(self._lib.cvl_engine_memory_get(self._h, C.byref(m)), "cvl_engine_memory_get")
         return {name: getattr(m, name) for name, _ in m._fields_}
 
-    def transport_cells(self, ops, params: CurveletParams | None = None, dt_rad: float = 0.0):
+    def transport_cells(self, ops, params: CurveletParams | None = None, dt_rad: float = 0.0,
+                        shared_quotients: bool = False):
         """cvl_check_transport_cells: one orientation column of the transport per row of
         ops [n, 10] = (DX, DY, tt, s_m, s_p, cos_m, sin_m, cos_p, sin_p, branch1).
+        shared_quotients: the rewrite's two k_dx quotients from one reciprocal
+        (Markstein's corrections, operands checked per cell) instead of two divisions.
         Returns (rewrite_min, rewrite_max, literal_min, literal_max), each [n, P]."""
         params = params or CurveletParams()
         q = np.ascontiguousarray(ops, dtype=np.float64).reshape(-1, 10)
@@ -463,12 +466,13 @@ class Engine:
         p = params.to_c(dt_rad)
         rows = C.c_int32(0)
         one = np.zeros(1)
-        check(self._lib.cvl_check_transport_cells(self._h, q.ctypes.data_as(_abi._dp), 0, C.byref(p),
+        quot = 1 if shared_quotients else 0
+        check(self._lib.cvl_check_transport_cells(self._h, q.ctypes.data_as(_abi._dp), 0, C.byref(p), quot,
                                                   one.ctypes.data_as(_abi._dp), C.byref(rows)),
               "cvl_check_transport_cells")
         P = rows.value
         out = np.zeros((max(n, 1), 4, P))
-        check(self._lib.cvl_check_transport_cells(self._h, q.ctypes.data_as(_abi._dp), n, C.byref(p),
+        check(self._lib.cvl_check_transport_cells(self._h, q.ctypes.data_as(_abi._dp), n, C.byref(p), quot,
                                                   out.ctypes.data_as(_abi._dp), C.byref(rows)),
               "cvl_check_transport_cells")
         out = out[:n]

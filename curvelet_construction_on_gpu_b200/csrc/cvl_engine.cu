@@ -170,6 +170,8 @@ struct cvl_engine {
     bool graphs_on = std::getenv("CVL_NO_GRAPHS") == nullptr;
     // direct runs on queue-pulling persistent grids (CVL_NO_PERSIST: short blocks)
     bool persist_on = std::getenv("CVL_NO_PERSIST") == nullptr;
+    // the transport's k_dx quotient pairs on one reciprocal (CVL_NO_SHARED_QUOTIENTS: divisions)
+    bool shared_quot_on = std::getenv("CVL_NO_SHARED_QUOTIENTS") == nullptr;
     uint64_t ws_epoch = 0;                         // workspace (re)allocations so far
     uint64_t graph_replays = 0, graph_fallbacks = 0, graph_captures = 0, graph_clock = 0;
     DBuf gdims, gchunks, gread;
@@ -412,6 +414,12 @@ int make_model(const cvl_engine *e, const cvl_params *p, double rad, unsigned nb
         md.sbits = sb;
     }
     md.hash_mask = 0;
+    // the FP64 transport's shared-reciprocal quotients need dx and sx in [2^-40, 2^40]
+    // (certify_* in cvl_kernels.cuh covers the run's own operands)
+    md.shared_quot = (std::is_same<T, double>::value && (!e || e->shared_quot_on) && p->dx >= 0x1p-40 &&
+                      p->dx <= 0x1p40 && p->sx >= 0x1p-40 && p->sx <= 0x1p40)
+                         ? 1
+                         : 0;
     return CVL_OK;
 }
 
@@ -541,8 +549,16 @@ int launch_bundles(cvl_engine *e, BundleArgsT<T> &a, int blocks) {
         blocks = (int)std::max(1LL, std::min<long long>(need, 0x7fffffffLL));
     }
     if constexpr (std::is_same<T, double>::value) {
-        if (a.queue) {  // a graph run: the queue-pulling variant
-            k_bundles<T, CPL, MINB, true><<<blocks, BUNDLE_THREADS, (size_t)ppb * pair_bytes, e->stream>>>(a);
+        const size_t smem = (size_t)ppb * pair_bytes;
+        if (a.shared_quot) {  // the k_dx quotient pairs on one reciprocal
+            if (a.queue)
+                k_bundles<T, CPL, MINB, true, QUOT_SHARED><<<blocks, BUNDLE_THREADS, smem, e->stream>>>(a);
+            else
+                k_bundles<T, CPL, MINB, false, QUOT_SHARED><<<blocks, BUNDLE_THREADS, smem, e->stream>>>(a);
+            return check_launch("k_bundles");
+        }
+        if (a.queue) {  // the queue-pulling variant
+            k_bundles<T, CPL, MINB, true><<<blocks, BUNDLE_THREADS, smem, e->stream>>>(a);
             return check_launch("k_bundles");
         }
     }
@@ -696,8 +712,9 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
 
     // ---- (a) binning
     const int gb = short_grid(n, 256);
+    unsigned *uncertified = (unsigned *)((unsigned long long *)e->work.p + 2);  // zeroed with the counters
     k_bin_keys<<<gb, 256, 0, s>>>(d_edges, sz, n, d_map_off, M, md, (unsigned *)e->ehash.p, (unsigned *)e->bcount.p,
-                                  err, nullptr);
+                                  err, uncertified, nullptr);
     CVL_TRY(check_launch("k_bin_keys"));
     CVL_TRY((scan<unsigned, unsigned>(e, (const unsigned *)e->bcount.p, T, (unsigned *)e->bstart.p)));
     k_bin_scatter<<<gb, 256, 0, s>>>(d_edges, sz, n, d_map_off, M, md, (const unsigned *)e->ehash.p,
@@ -774,6 +791,7 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
     na.pcls = path ? (unsigned char *)e->pcls.p : nullptr;
     na.pair_anchor = path ? (int *)e->pair_anchor.p : nullptr;
     na.atrig = path ? (R *)e->atrig.p : nullptr;
+    na.uncertified = uncertified;
     k_nb<R, NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
     CVL_TRY(check_launch("k_nb<FILL>"));
     e->mark("neighbors_fill");
@@ -827,7 +845,10 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
         for (int c = 0; c <= nchunks; ++c)
             CVL_CUDA(cudaMemcpyAsync(&h_poff[c], (unsigned long long *)e->pair_off.p + cstart[c],
                                      sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        unsigned h_uncertified = 0;
+        CVL_CUDA(cudaMemcpyAsync(&h_uncertified, uncertified, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         CVL_CUDA(cudaStreamSynchronize(s));
+        const int shared_quot = (md.shared_quot && !h_uncertified) ? 1 : 0;
         unsigned *queues = (unsigned *)((unsigned long long *)e->work.p + 3);
         for (int c = 0; c < nchunks; ++c) {
             const int a0 = cstart[c], a1 = cstart[c + 1];
@@ -851,6 +872,7 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
             ba.atrig = (const R *)e->atrig.p;
             ba.bund = (R *)e->bund.p;
             ba.pflag = (unsigned char *)e->pflag.p;
+            ba.shared_quot = shared_quot;  // the host read the run's certification above
             if (persist) {
                 CVL_CUDA(cudaMemsetAsync(queues, 0, 2 * sizeof(unsigned), s));
                 ba.queue = queues;
@@ -1141,8 +1163,9 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
             CVL_CUDA(cudaMemsetAsync(e->count.p, 0, sizeof(unsigned) * N, s));
             CVL_CUDA(cudaMemsetAsync(e->chunk_start.p, 0, sizeof(int) * (cap.K + 1), s));
             const int gb = short_grid(N, 256);
+            unsigned *uncertified = (unsigned *)((unsigned long long *)e->work.p + 2);  // zeroed above
             k_bin_keys<<<gb, 256, 0, s>>>(d_edges, sz, N, d_map_off, cap.M, md, (unsigned *)e->ehash.p,
-                                          (unsigned *)e->bcount.p, err, dd);
+                                          (unsigned *)e->bcount.p, err, uncertified, dd);
             CVL_TRY(check_launch("k_bin_keys"));
             CVL_TRY((scan<unsigned, unsigned>(e, (const unsigned *)e->bcount.p, T, (unsigned *)e->bstart.p)));
             k_bin_scatter<<<gb, 256, 0, s>>>(d_edges, sz, N, d_map_off, cap.M, md, (const unsigned *)e->ehash.p,
@@ -1179,6 +1202,7 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
             na.pcls = (unsigned char *)e->pcls.p;
             na.pair_anchor = (int *)e->pair_anchor.p;
             na.atrig = (double *)e->atrig.p;
+            na.uncertified = uncertified;
             k_nb<double, NB_FILL><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
             CVL_TRY(check_launch("k_nb<FILL>"));
             k_cell_ranks<double><<<1, 128, 0, s>>>(md, (unsigned short *)e->crank.p);
@@ -1204,6 +1228,14 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
                 // bucket 1 pulls work from the queues (measured: the 242k-edge map 2.79 ->
                 // 2.52 ms); bucket 0's runs are too small for the atomics to pay
                 ba.queue = b == 1 ? queues : nullptr;
+                if (md.shared_quot) {
+                    // the run's certification is known only on the device: both forms go
+                    // into the graph, and the one that does not match returns at once
+                    ba.uncertified = uncertified;
+                    ba.shared_quot = 1;
+                    CVL_TRY(bf(e, ba, sms * 16));
+                    ba.shared_quot = 0;
+                }
                 CVL_TRY(bf(e, ba, sms * 16));
                 GrowthArgsT<double> ga{};
                 ga.md = md;
@@ -1742,8 +1774,8 @@ int cvl_check_pair_bundles_literal(cvl_engine *e, const double *pairs, int32_t n
     return pair_bundles_form(e, pairs, n, p, 1, bmin, bmax, valid, cells);
 }
 
-int cvl_check_transport_cells(cvl_engine *e, const double *ops, int32_t n, const cvl_params *p, double *out,
-                              int32_t *rows) {
+int cvl_check_transport_cells(cvl_engine *e, const double *ops, int32_t n, const cvl_params *p, int32_t quotients,
+                              double *out, int32_t *rows) {
     if (!e || !ops || !out || !rows || n < 0) return fail(CVL_EINVAL, "invalid argument");
     CVL_CUDA(cudaSetDevice(e->device));
     Model md;
@@ -1757,6 +1789,7 @@ int cvl_check_transport_cells(cvl_engine *e, const double *ops, int32_t n, const
     cudaStream_t s = e->stream;
     CVL_CUDA(cudaMemcpyAsync(e->pairs_in.p, ops, sizeof(double) * 10 * (size_t)n, cudaMemcpyHostToDevice, s));
     k_transport_cells<<<grid_for(e, n, 128, 8), 128, 0, s>>>(md, (const double *)e->pairs_in.p, n,
+                                                             quotients ? QUOT_CHECKED : QUOT_DIVIDE,
                                                              (double *)e->pb_min.p);
     CVL_TRY(check_launch("k_transport_cells"));
     CVL_CUDA(cudaMemcpyAsync(out, e->pb_min.p, sizeof(double) * out_n, cudaMemcpyDeviceToHost, s));

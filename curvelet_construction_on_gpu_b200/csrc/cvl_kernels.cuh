@@ -57,7 +57,31 @@ struct ModelT {
     int w;                       // pixel-window half width (3, main.cpp:48)
     int sbits;                   // hash block edge S = 1 << sbits pixel cells
     unsigned hash_mask;          // table size - 1
+    int shared_quot;             // FP64 transport: the k_dx quotients on one reciprocal
+                                 // (QUOT_SHARED) unless a run's operands fail certify_*
 };
+
+// Operands whose ranges give every nonzero e1 and k_dx numerator of the FP64
+// transport a magnitude in [2^-500, 2^501), the range in which the transport's
+// shared-reciprocal quotients round correctly (cvl_path.cuh). With x, y and the
+// parameters dx, sx in {0} or [2^-40, 2^40] in magnitude (coordinates are below
+// 1e9 < 2^30 in any case), and the anchor trig values sin/cos(T2t_j) in {0} or
+// [2^-100, 1]: every value is a multiple of its lowest bit 2^(exponent - 52), sums
+// keep the smallest of their operands' lowest bits, and products multiply them,
+// so e1 = (((DX^2 - (2 d) tt) + DY^2) - dx^2) + d^2 is 0 or at least 2^-336 (DX
+// from 2^-92, tt = sin DX - cos DY from 2^-244, 2 d from 2^-92) and at most 2^94,
+// and the numerators (2 tt - 2 d) -+ 2 dx are 0 or in [2^-243, 2^48]. A run with
+// an operand outside these ranges sets its flag, and its transport divides.
+template <typename T>
+__device__ __forceinline__ bool certify_coord(T v) {
+    const T a = fabs(v);
+    return a == T(0) || (a >= T(0x1p-40) && a <= T(0x1p40));
+}
+template <typename T>
+__device__ __forceinline__ bool certify_trig(T v) {
+    const T a = fabs(v);
+    return a == T(0) || a >= T(0x1p-100);
+}
 using Model = ModelT<double>;
 
 // SoA copy of the edges in hash-bucket order ("internal" index space).
@@ -226,7 +250,8 @@ __device__ __forceinline__ int map_of(const int *map_off, int M, int e) {
 template <typename T>
 __global__ void k_bin_keys(const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off, int M,
                            ModelT<T> md, unsigned *__restrict__ ehash, unsigned *__restrict__ bcount,
-                           unsigned *__restrict__ err, const RunDims *__restrict__ dims) {
+                           unsigned *__restrict__ err, unsigned *__restrict__ uncertified,
+                           const RunDims *__restrict__ dims) {
     if (dims) {
         N = dims->N;
         M = dims->M;
@@ -241,6 +266,7 @@ __global__ void k_bin_keys(const T *__restrict__ edges, int sz, int N, const int
             atomicAdd(&bcount[0], 1u);
             continue;
         }
+        if (uncertified && !(certify_coord(x) && certify_coord(y))) atomicOr(uncertified, 1u);
         const int m = map_of(map_off, M, e);
         const int cx = lrint_dev(x);  // lrint, round half to even (preprocess.hpp:85-86)
         const int cy = lrint_dev(y);
@@ -454,6 +480,7 @@ struct NbArgsT {
     int *pair_anchor;                    // FILL (optional): internal anchor of each pair
     T *atrig;                            // FILL (optional): [N][2Q + 2] sin/cos(T2 + delta_t2_j), cos/sin(T2)
     unsigned *err;
+    unsigned *uncertified;               // FILL (optional): set when a trig value fails certify_trig
     const RunDims *dims;                 // graph runs: N and M from device memory
     unsigned long long pair_cap;         // graph runs: pairs the CSR buffers hold (0: sized to the run)
 };
@@ -568,8 +595,10 @@ __global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a
             T *row = a.atrig + (size_t)i * (2 * md.Q + 2);
             for (int j = lane; j < md.Q; j += 32) {
                 const T t = T2 + grid_offset(md.st, j, md.Q);  // T2t = T2 + delta_t2 (:698-702)
-                row[j] = cvl_sin(t);
-                row[md.Q + j] = cvl_cos(t);
+                const T sv = cvl_sin(t), cv = cvl_cos(t);
+                row[j] = sv;
+                row[md.Q + j] = cv;
+                if (a.uncertified && !(certify_trig(sv) && certify_trig(cv))) atomicOr(a.uncertified, 1u);
             }
             if (lane == 0) {
                 row[2 * md.Q] = cosT2;

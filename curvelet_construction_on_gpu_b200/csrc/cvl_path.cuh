@@ -87,6 +87,47 @@ __device__ __forceinline__ void bundle_cell_tt(const Model &md, double DX2, doub
     if (bmax > k2max) bmax = k2max;
 }
 
+// ---- two quotients on one reciprocal ----------------------------------------
+// Markstein's method (P. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990; J.-M. Muller et al.,
+// Handbook of Floating-Point Arithmetic, FMA-based division): with y = RN(1/b)
+// (__drcp_rn), the quotient q0 = RN(a y) followed by two residual corrections
+// r = RN(a - b q), q = RN(q + r y), each a single FMA, is RN(a / b) when
+//  (i)  a and b have magnitudes in [2^-500, 2^501) (markstein_range), and
+//  (ii) b's significand is below 2 - 4 ulp.
+// Proof (scaled to 1 <= a, b < 2, which powers of two do exactly within (i)): y is
+// within 2^-54 of 1/b, so e = b y - 1 has |e| <= b 2^-54 and q0 is within 2^-52 of
+// a/b; the first correction makes q faithful, so the second residual is exact and
+// q + r y = a/b + (a/b - q) e, off a/b by at most (ulp/2 + 2^-104) b 2^-54. a/b is
+// never a midpoint of two doubles, and no closer to one than 2^-106 / b (a - b m is
+// a nonzero multiple of 2^-106 for a midpoint m below 1; 2^-105 / b above 1), which
+// exceeds that offset whenever b^2 (1 + 2^-50) < 4: (ii).
+// a = +0 gives a/b's signed zero too: q0 = +0 y has it, each residual is +0, and
+// each correction adds a zero of q0's sign.
+// tests/probes/shared_quotients.cu compares the sequence with '/' on the device
+// (6.2e9 operand pairs, special operands included).
+constexpr int QUOT_DIVIDE = 0, QUOT_SHARED = 1, QUOT_CHECKED = 2;
+
+__device__ __forceinline__ double markstein_quotient(double a, double b, double y) {
+    const double q0 = a * y;
+    const double r0 = fma(-b, q0, a);
+    const double q1 = fma(r0, y, q0);
+    const double r1 = fma(-b, q1, a);
+    return fma(r1, y, q1);
+}
+// (ii)'s complement and more: significands of at least 2 - 2^-20 (the high 20 bits
+// of the fraction all ones)
+__device__ __forceinline__ bool high_significand(double b) {
+    return ((unsigned)__double2hiint(b) & 0xFFFFFu) == 0xFFFFFu;
+}
+// (i): the exponent field in [523, 1523]
+__device__ __forceinline__ bool markstein_range(double x) {
+    return ((((unsigned)__double2hiint(x) >> 20) & 0x7FFu) - 523u) <= 1000u;
+}
+__device__ __forceinline__ bool markstein_numerator(double a) {
+    return __double_as_longlong(a) == 0 || markstein_range(a);
+}
+
 // One (pair, j) column of the FP64 transport, cells (i, j) for i = 0 .. P-1, in
 // the rewritten form k_bundles runs (see the comment above k_bundles):
 //   e1   = (((DX2 - (2 dx2) tt) + DY2) - dx^2) + dx2^2     (branch 1's eq, :706)
@@ -96,13 +137,15 @@ __device__ __forceinline__ void bundle_cell_tt(const Model &md, double DX2, doub
 // dx2sq[i] = dx2[i]^2 are the per-i constants; store(i, bmin, bmax) takes each
 // cell. Returns whether any cell of the column is open (bmax > bmin).
 // k_bundles and k_pair_bundles (form 0) both run this function.
-#ifndef CVL_BUNDLE_UNROLL
-#define CVL_BUNDLE_UNROLL 1
-#endif
-#define CVL_PRAGMA_(x) _Pragma(#x)
-#define CVL_UNROLL_(n) CVL_PRAGMA_(unroll n)
-#define CVL_BUNDLE_UNROLL_PRAGMA CVL_UNROLL_(CVL_BUNDLE_UNROLL)
-template <class Store>
+//
+// QUOT selects how the two k_dx quotients, which share the divisor e1, are formed:
+//   QUOT_DIVIDE  two IEEE divisions;
+//   QUOT_SHARED  one correctly rounded reciprocal and Markstein's corrections
+//                (markstein_quotient), for operands a run has certified (below);
+//   QUOT_CHECKED the same, with every operand's range tested in each cell.
+// All three give the same bits. A cell whose e1 is zero, or whose significand is
+// among the largest (high_significand), divides.
+template <int QUOT, class Store>
 __device__ __forceinline__ bool bundle_column_fp64(const Model &md, const double *dx2, const double *dx2_2,
                                                    const double *dx2sq, const PairGeom &g2, double tt, double s_m,
                                                    double s_p, Store &&store) {
@@ -117,20 +160,35 @@ __device__ __forceinline__ bool bundle_column_fp64(const Model &md, const double
     const double n_lo = g2.branch1 ? g2.sin_m_DY : g2.sin_p_DY;
     const double n_hi = g2.branch1 ? g2.sin_p_DY : g2.sin_m_DY;
     bool open = false;
-CVL_BUNDLE_UNROLL_PRAGMA  // (measured: unrolling by 2 spills under the 64-register cap and is 2.6% slower)
+#pragma unroll 1  // (measured: unrolling by 2 or 3 is 1-2% slower, with or without a larger register budget)
     for (int i = 0; i < md.P; ++i) {
         const double delta_x2 = dx2[i], d2_2 = dx2_2[i];
         const double ttmdx2_2 = tt2 - d2_2;                          // 2 ttmdx2
         const double lo2 = ttmdx2_2 - dx_2, hi2 = ttmdx2_2 + dx_2;  // 2 (ttmdx2 -+ dx)
         const double e1 = (((g2.DX2 - d2_2 * tt) + g2.DY2) - md.dx2) + dx2sq[i];
-        double k_dx_min = lo2 / e1;
-        double k_dx_max = hi2 / e1;
+        double k_dx_min, k_dx_max;
         // The one value where branch 2's eq is not e1 * 0.5: when e1 cancels to
         // +0, branch 2's sum cancels to +0 as well and its eq is -(+0) / 2 = -0,
         // so its k_dx are the infinities of the other sign (0 / 0 stays NaN).
-        if (e1 == 0.0 && !g2.branch1) {
-            k_dx_min = -k_dx_min;
-            k_dx_max = -k_dx_max;
+        auto divide = [&] {
+            k_dx_min = lo2 / e1;
+            k_dx_max = hi2 / e1;
+            if (e1 == 0.0 && !g2.branch1) {
+                k_dx_min = -k_dx_min;
+                k_dx_max = -k_dx_max;
+            }
+        };
+        if constexpr (QUOT != QUOT_DIVIDE) {
+            const double y = __drcp_rn(e1);
+            k_dx_min = markstein_quotient(lo2, e1, y);
+            k_dx_max = markstein_quotient(hi2, e1, y);
+            bool by_division = e1 == 0.0 || high_significand(e1);
+            if constexpr (QUOT == QUOT_CHECKED)
+                by_division = by_division || !markstein_range(e1) || !markstein_numerator(lo2) ||
+                              !markstein_numerator(hi2);
+            if (by_division) divide();
+        } else {
+            divide();
         }
         double bmin = -md.max_k, bmax = md.max_k;
         if (bmin < k_dx_min) bmin = k_dx_min;
@@ -223,6 +281,8 @@ struct BundleArgsT {
     unsigned char *pflag;               // [P]: bit 0 valid, bit 1 close
     const ChunkDims *cd;                // graph runs: the pair range from device memory
     unsigned *queue;                    // graph runs: the work queue blocks take pair tiles from (0 at start)
+    int shared_quot;                    // the launcher's choice of form: QUOT_SHARED variant if nonzero
+    const unsigned *uncertified;        // graph runs: the run's certification flag (certify_*, cvl_kernels.cuh)
 };
 
 constexpr int BUNDLE_THREADS = 128;
@@ -240,10 +300,19 @@ __host__ __device__ inline int bundles_pairs_per_block(int Q, int pair_bytes) {
 // MINB: the resident 256-thread blocks per SM the register allocation is capped for
 // (3 or 4; with 128-thread blocks, twice as many of those). 128 threads measured 1%
 // faster than 256 at the same registers, and shorter blocks free SMs sooner.
-// QUEUE: a graph run's variant, whose persistent grid pulls tiles from a.queue.
-template <typename T, int CPL, int MINB, bool QUEUE = false>
+// QUEUE: the variant whose persistent grid pulls tiles from a.queue. QUOT: how the
+// FP64 transport forms its k_dx quotient pairs (bundle_column_fp64), the same bits
+// either way: one reciprocal (QUOT_SHARED) where the model allows it and the run's
+// operands are certified (certify_*), else two divisions.
+template <typename T, int CPL, int MINB, bool QUEUE = false, int QUOT = QUOT_DIVIDE>
 __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS)) k_bundles(BundleArgsT<T> a) {
     const ModelT<T> &md = a.md;
+    if (a.uncertified) {
+        // a graph run launches both forms; the one that does not match the run's
+        // certification returns at once
+        const bool shared = md.shared_quot && !*a.uncertified;
+        if (shared != (QUOT == QUOT_SHARED)) return;
+    }
     constexpr int BW = 2 * 32 * CPL;
     extern __shared__ __align__(16) unsigned char bn_smem[];
     T *s_b = (T *)bn_smem;  // [PPB][BW]: the block's bundles until their validity is known
@@ -330,8 +399,8 @@ __global__ void __launch_bounds__(BUNDLE_THREADS, MINB * (256 / BUNDLE_THREADS))
                         dst[32 * CPL + i * md.Q + jl] = bmax;
                     }
                 } else {
-                    open = bundle_column_fp64(md, s_dx2, s_dx2_2, s_dx2sq, g2, tt, s_m, s_p,
-                                              [&](int i, double lo, double hi) {
+                    open = bundle_column_fp64<QUOT>(md, s_dx2, s_dx2_2, s_dx2sq, g2, tt, s_m, s_p,
+                                                    [&](int i, double lo, double hi) {
                                                   dst[i * md.Q + jl] = lo;
                                                   dst[32 * CPL + i * md.Q + jl] = hi;
                                               });
@@ -844,7 +913,8 @@ __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, in
 // Standalone transport for independent pairs (cvl_pair_bundles,
 // cvl_pair_bundles_noalloc): warp per pair, lane j < Q computes the column of
 // orientation sample j, as a k_bundles lane does.
-//   form 0: bundle_column_fp64, the arithmetic k_bundles runs;
+//   form 0: bundle_column_fp64, the arithmetic k_bundles runs (its k_dx quotients
+//           on one reciprocal, each operand checked: QUOT_CHECKED);
 //   form 1: bundle_cell_tt, the reference's two branches as written, a check
 //           of form 0 on the same trig values.
 // pairs[p] = (te_x, te_y, te_theta, le_x, le_y, le_theta). valid_count, when
@@ -887,7 +957,7 @@ __global__ void __launch_bounds__(128) k_pair_bundles(Model md, const double *__
                 const double s_p = sin(T2t - (T0 + md.dt));           // :729
                 const double tt = sin(T2t) * g.DX - cos(T2t) * g.DY;  // :705
                 if (form == 0) {
-                    lv = bundle_column_fp64(md, s_dx2, s_dx2_2, s_dx2sq, g, tt, s_m, s_p, store);
+                    lv = bundle_column_fp64<QUOT_CHECKED>(md, s_dx2, s_dx2_2, s_dx2sq, g, tt, s_m, s_p, store);
                 } else {
                     for (int i = 0; i < md.P; ++i) {
                         double lo = -md.max_k, hi = md.max_k;
@@ -913,9 +983,9 @@ __global__ void __launch_bounds__(128) k_pair_bundles(Model md, const double *__
 // on operand sets given directly, so that cells built to cancel reach the device
 // code. ops[r] = (DX, DY, tt, s_m, s_p, cos_m, sin_m, cos_p, sin_p, branch1), with
 // cos/sin of T0 -+ dt as pair_geom takes them. out[r] = [form][bmin, bmax][P]:
-// bundle_column_fp64 (form 0, the production arithmetic) and bundle_cell_tt
-// (form 1, the reference's expressions as written). A thread per row.
-__global__ void k_transport_cells(Model md, const double *__restrict__ ops, int n, double *__restrict__ out) {
+// bundle_column_fp64 with the given quot (form 0, the production arithmetic) and
+// bundle_cell_tt (form 1, the reference's expressions as written). A thread per row.
+__global__ void k_transport_cells(Model md, const double *__restrict__ ops, int n, int quot, double *__restrict__ out) {
     __shared__ double s_dx2[CELLS_MAX], s_dx2_2[CELLS_MAX], s_dx2sq[CELLS_MAX];
     for (int i = threadIdx.x; i < md.P; i += blockDim.x) {
         const double d = grid_offset(md.sx, i, md.P);
@@ -939,10 +1009,15 @@ __global__ void k_transport_cells(Model md, const double *__restrict__ ops, int 
         g.branch1 = o[9] != 0.0;
         const double tt = o[2], s_m = o[3], s_p = o[4];
         double *dst = out + (size_t)r * 4 * md.P;
-        bundle_column_fp64(md, s_dx2, s_dx2_2, s_dx2sq, g, tt, s_m, s_p, [&](int i, double lo, double hi) {
+        auto put = [&](int i, double lo, double hi) {
             dst[i] = lo;
             dst[md.P + i] = hi;
-        });
+        };
+        if (quot == QUOT_CHECKED) {
+            bundle_column_fp64<QUOT_CHECKED>(md, s_dx2, s_dx2_2, s_dx2sq, g, tt, s_m, s_p, put);
+        } else {
+            bundle_column_fp64<QUOT_DIVIDE>(md, s_dx2, s_dx2_2, s_dx2sq, g, tt, s_m, s_p, put);
+        }
         for (int i = 0; i < md.P; ++i) {
             double lo = -md.max_k, hi = md.max_k;
             bundle_cell_tt(md, g.DX2, g.DY2, g.sin_p_DY, g.cos_p_DX, g.sin_m_DY, g.cos_m_DX, g.branch1, s_dx2[i], tt,

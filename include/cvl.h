@@ -215,9 +215,12 @@ int cvl_check_pair_bundles_literal(cvl_engine *e, const double *pairs, int32_t n
  * sin(T0 - dt), cos(T0 + dt), sin(T0 + dt), branch1 != 0), the operands of
  * cpu_curvelet.hpp:693-809 given directly, so that cells built to cancel reach the
  * device. out[n][4][P]: the path's rewritten arithmetic (bmin, then bmax), then
- * the reference's two branches as written (bmin, bmax). *rows = P. */
-int cvl_check_transport_cells(cvl_engine *e, const double *ops, int32_t n, const cvl_params *p, double *out,
-                              int32_t *rows);
+ * the reference's two branches as written (bmin, bmax). quotients selects how the
+ * rewritten arithmetic forms its two k_dx quotients: 0 two IEEE divisions, 1 one
+ * correctly rounded reciprocal and Markstein's corrections, each operand's range
+ * checked per cell (the bundle kernel's form on certified runs). *rows = P. */
+int cvl_check_transport_cells(cvl_engine *e, const double *ops, int32_t n, const cvl_params *p, int32_t quotients,
+                              double *out, int32_t *rows);
 
 /* ---- pair bundles without any allocation ------------------------------ */
 /* No reference counterpart. The same computation and outputs as

@@ -14,8 +14,9 @@ reach that code at chosen operands:
   reference's expressions as written, evaluated here with one rounding per
   operation, bit for bit, on the path's operand ranges, on other grids, on cells
   built to cancel (exact +0 denominators in both branches) and on zero
-  distances; the number of branch-2 cells that take the negation is counted and
-  must be positive;
+  distances, with the k_dx quotient pair formed both ways the kernel forms it
+  (two divisions; one reciprocal and Markstein's corrections); the number of
+  branch-2 cells that take the negation is counted and must be positive;
 - pairs: the reference's compute_curve_bundle on 64 pairs and on 256 pairs whose
   centre cell cancels to +0 in branch 2 (tests/golden/pair_bundles_cancel.npz):
   the path's arithmetic equals the literal two-branch form on the same device
@@ -109,13 +110,16 @@ def cancelling_ops(rng, n, d, dx):
 
 
 def check_ops(engine, ops, params):
+    """Both forms of the rewrite's k_dx quotients (two divisions; one reciprocal with
+    Markstein's corrections) and the literal form, against the reference, bit for bit."""
     d2 = grid(params.sx, params.dx)
-    rmin, rmax, lmin, lmax = engine.transport_cells(ops, params)
     emin, emax = reference_columns(ops, d2, params.dx, params.max_k)
-    for got, want in ((rmin, emin), (rmax, emax), (lmin, emin), (lmax, emax)):
-        assert got.shape == want.shape
-        bad = got.view(np.uint64) != want.view(np.uint64)
-        assert not bad.any(), f"{int(bad.sum())} cells differ; first {np.argwhere(bad)[:3].tolist()}"
+    for shared in (False, True):
+        rmin, rmax, lmin, lmax = engine.transport_cells(ops, params, shared_quotients=shared)
+        for got, want in ((rmin, emin), (rmax, emax), (lmin, emin), (lmax, emax)):
+            assert got.shape == want.shape
+            bad = got.view(np.uint64) != want.view(np.uint64)
+            assert not bad.any(), f"shared={shared}: {int(bad.sum())} cells differ; first {np.argwhere(bad)[:3].tolist()}"
     return negated_cells(ops, d2, params.dx)
 
 
