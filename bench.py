@@ -53,16 +53,16 @@ METRIC = "edges/s"
 FLOPS_PER_PAIR_CELL = 20
 # DRAM bytes of k_bundles per computed pair, from one ncu capture of the kernel
 # (--set full, profiles/k_bundles_k_growth_persistent_hd.md) on the 242k-edge
-# 1920x1080 map: dram__bytes_read.sum 0.153845 GB + dram__bytes_write.sum 1.428184 GB
+# 1920x1080 map: dram__bytes_read.sum 0.153864 GB + dram__bytes_write.sum 1.430769 GB
 # over 2,176,780 non-close pairs. The traffic is the valid pairs' bundle writes
 # (1,008 B each, about half of the computed pairs) plus the pair/anchor reads, so it
 # scales with the pairs a launch processes.
-BUNDLE_DRAM_BYTES_PER_PAIR = (0.153845e9 + 1.428184e9) / 2_176_780
+BUNDLE_DRAM_BYTES_PER_PAIR = (0.153864e9 + 1.430769e9) / 2_176_780
 # FP64-pipe instructions of k_bundles per cell, from the same capture: the pipe was
-# active 51.154% of 1,852,462 active cycles per SM on 148 SMs (each issues 2 FP64
-# warp-instructions a cycle), 30.72 active lanes per warp-instruction, 2,176,780 x 63
+# active 51.553% of 1,750,328 active cycles per SM on 148 SMs (each issues 2 FP64
+# warp-instructions a cycle), 30.73 active lanes per warp-instruction, 2,176,780 x 63
 # cells. A division costs about 10 of them, which the algorithmic count takes as 1 flop.
-BUNDLE_FP64_INSTR_PER_CELL = 0.51154 * 1_852_462 * 148 * 2 * 30.72 / (2_176_780 * 63)
+BUNDLE_FP64_INSTR_PER_CELL = 0.51553 * 1_750_328 * 148 * 2 * 30.73 / (2_176_780 * 63)
 
 
 def _args():
