@@ -301,13 +301,10 @@ __global__ void k_bin_scatter(const T *__restrict__ edges, int sz, int N, const 
         // T0 +- dt and their sin/cos (cpu_curvelet.hpp:655-656, 730-733), once per edge
         const T t_p = th + md.dt;
         const T t_m = th - md.dt;
-        T s_p, c_p, s_m, c_m;
-        cvl_sincos(t_p, &s_p, &c_p);
-        cvl_sincos(t_m, &s_m, &c_m);
-        B.sp[pos] = s_p;
-        B.cp[pos] = c_p;
-        B.sm[pos] = s_m;
-        B.cm[pos] = c_m;
+        B.sp[pos] = sin(t_p);
+        B.cp[pos] = cos(t_p);
+        B.sm[pos] = sin(t_m);
+        B.cm[pos] = cos(t_m);
         B.cell[pos] = make_int2(lrint_dev(x), lrint_dev(y));
         B.orig[pos] = e;
         B.map[pos] = map_of(map_off, M, e);
