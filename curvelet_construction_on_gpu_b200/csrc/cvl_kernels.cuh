@@ -190,8 +190,8 @@ __device__ __forceinline__ T sq_dist(T x1, T y1, T x2, T y2) {
 // one per call site keeps the kernels' code within the instruction cache.
 __device__ __noinline__ double cvl_sin(double x) { return sin(x); }
 __device__ __noinline__ double cvl_cos(double x) { return cos(x); }
-// sin and cos of one argument in one call (the same values as sin and cos: checked on
-// the device over 1.8e9 arguments, path angles, large ones and any finite double)
+// sin and cos of one argument in one call, the same values as sin and cos
+// (tests/probes/sincos_identity.cu compares them on the device, double and float)
 __device__ __noinline__ void cvl_sincos(double x, double *s, double *c) { sincos(x, s, c); }
 __device__ __noinline__ void cvl_sincos(float x, float *s, float *c) { sincosf(x, s, c); }
 __device__ __noinline__ double cvl_atan2(double y, double x) { return atan2(y, x); }

@@ -74,3 +74,19 @@ def test_engine_shared_quotients_equal_divisions(engine, monkeypatch):
         assert all(_same(a, b) for a, b in zip(got, want))
     finally:
         divide.close()
+
+
+def test_sincos_equals_sin_and_cos(tmp_path):
+    """The neighbour kernel's anchor trig row comes from sincos (tests/probes/
+    sincos_identity.cu): bit for bit the values of sin and cos, in double and float."""
+    exe = str(tmp_path / "sincos_identity")
+    subprocess.run([_nvcc(), "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-fmad=false",
+                    "-o", exe, os.path.join(HERE, "probes", "sincos_identity.cu")], check=True,
+                   capture_output=True, text=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    print(out.stdout)
+    assert out.returncode == 0, out.stdout + out.stderr
+    checks = re.findall(r"check mode (\d) arguments (\d+) mismatches (\d+)", out.stdout)
+    assert len(checks) == 3
+    for mode, n, bad in checks:
+        assert int(n) > 10**8 and int(bad) == 0, (mode, n, bad)
