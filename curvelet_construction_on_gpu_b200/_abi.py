@@ -150,6 +150,7 @@ SIGNATURES = [
                                             C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("cvl_engine_reserve_workspace", C.c_int, [_vp, C.POINTER(CvlWorkspaceShape), C.POINTER(CvlParams)]),
     ("cvl_engine_memory_get", C.c_int, [_vp, C.POINTER(CvlEngineMemory)]),
+    ("cvl_engine_warmup", C.c_int, [_vp]),
     ("cvl_engine_set_graphs", C.c_int, [_vp, C.c_int]),
     ("cvl_engine_graph_stats", C.c_int, [_vp, C.POINTER(CvlEngineGraphs)]),
     ("cvl_debug_fail_allocations", C.c_int, [C.c_int64]),

@@ -437,6 +437,11 @@ class Engine:
         check(self._lib.cvl_engine_reserve_workspace(self._h, C.byref(shp), C.byref(p)),
               "cvl_engine_reserve_workspace")
 
+    def warmup(self) -> None:
+        """cvl_engine_warmup: run two built-in maps through the engine's forms of the path,
+        so that the first real run pays no module loading or pool growth."""
+        check(self._lib.cvl_engine_warmup(self._h), "cvl_engine_warmup")
+
     def set_graphs(self, enable: bool) -> None:
         """cvl_engine_set_graphs: replay a CUDA graph per size bucket (default) or launch kernel by kernel."""
         check(self._lib.cvl_engine_set_graphs(self._h, 1 if enable else 0), "cvl_engine_set_graphs")

@@ -2103,6 +2103,47 @@ int cvl_engine_set_graphs(cvl_engine *e, int enable) {
     return CVL_OK;
 }
 
+// Rings of edgels (position, tangent orientation, strength 1) centred on a grid of
+// tiles: a built-in map of about tiles^2 x 520 edges for the warm-up.
+static std::vector<double> warmup_map(int tiles) {
+    std::vector<double> v;
+    const double two_pi = 2.0 * CVL_PI;
+    for (int ty = 0; ty < tiles; ++ty)
+        for (int tx = 0; tx < tiles; ++tx) {
+            const double cx = 60.0 + 120.0 * tx, cy = 60.0 + 120.0 * ty;
+            for (double r : {11.0, 23.0, 48.0}) {
+                const int k = (int)(two_pi * r);
+                for (int i = 0; i < k; ++i) {
+                    const double phi = two_pi * i / k;
+                    const double th = std::fmod(phi + 0.5 * CVL_PI, two_pi);
+                    v.insert(v.end(), {cx + r * std::cos(phi), cy + r * std::sin(phi), th, 1.0});
+                }
+            }
+        }
+    return v;
+}
+
+int cvl_engine_warmup(cvl_engine *e) {
+    if (!e) return fail(CVL_EINVAL, "engine is NULL");
+    cvl_params p;
+    cvl_params_default(&p);
+    const bool graphs = e->graphs_on;
+    // a small map (the bucket-0 graph, or its kernels one by one), and a map above
+    // 64 Ki edges (the persistent grids, and the bucket-1 graph)
+    const std::vector<double> small = warmup_map(1), large = warmup_map(12);
+    int rc = CVL_OK;
+    for (const std::vector<double> *m : {&small, &large})
+        for (int g = 0; g < 2 && rc == CVL_OK; ++g) {
+            e->graphs_on = graphs && g == 0;
+            cvl_result *r = nullptr;
+            rc = cvl_run(e, m->data(), (int32_t)(m->size() / 4), 4, &p, &r);
+            cvl_result_free(r);
+            if (!graphs) break;
+        }
+    e->graphs_on = graphs;
+    return rc;
+}
+
 int cvl_engine_graph_stats(cvl_engine *e, cvl_engine_graphs *out) {
     if (!e || !out) return fail(CVL_EINVAL, "engine/out is NULL");
     out->enabled = e->graphs_on ? 1 : 0;

@@ -78,6 +78,12 @@ typedef struct cvl_engine_cfg {
 
 void cvl_engine_cfg_default(cvl_engine_cfg *cfg);
 int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out);
+/* No reference counterpart. Runs two built-in maps (about 520 and 75,000 edges)
+ * through the engine's forms of the path (kernel by kernel, and the graphs of the
+ * two small size buckets), so that the kernels are loaded and the workspace pools
+ * hold memory before the first real input: a process's first run otherwise pays
+ * module loading and allocation. The engine's settings are unchanged afterwards. */
+int cvl_engine_warmup(cvl_engine *e);
 /* Also frees the engine's batches that are still alive (their handles become
  * invalid), and any batch result of the engine can then no longer be read. */
 void cvl_engine_destroy(cvl_engine *e);

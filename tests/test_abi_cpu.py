@@ -63,6 +63,7 @@ def test_null_arguments_are_rejected():
     assert lib.cvl_run(None, None, 0, 4, None, C.byref(r)) == _abi.CVL_EINVAL
     assert lib.cvl_result_get(None, None) == _abi.CVL_EINVAL
     assert lib.cvl_engine_create(None, None) == _abi.CVL_EINVAL
+    assert lib.cvl_engine_warmup(None) == _abi.CVL_EINVAL
     assert "NULL" in lib.cvl_last_error().decode()
     assert lib.cvl_version().decode().startswith("cvl ")
 

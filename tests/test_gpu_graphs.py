@@ -72,3 +72,16 @@ def test_graph_capacity_overflow_falls_back(direct):
         small = synth.plain_small(2)
         _same(eng.run(small), direct.run(small))
         assert eng.graph_stats()["fallbacks"] == 1
+
+
+def test_warmup_then_runs_equal_a_fresh_engine(engine):
+    """cvl_engine_warmup runs its built-in maps through every form; the engine's later
+    results equal a fresh engine's, and its graph switch is as it was."""
+    maps = [synth.plain_small(11), synth.plain_hd(1000)]
+    with cvl.Engine() as warm:
+        warm.warmup()
+        assert warm.graph_stats()["enabled"] == 1
+        got = [warm.run(m) for m in maps]
+    for a, m in zip(got, maps):
+        b = engine.run(m)
+        assert np.array_equal(a.chains, b.chains) and np.array_equal(a.info.view(np.uint64), b.info.view(np.uint64))
