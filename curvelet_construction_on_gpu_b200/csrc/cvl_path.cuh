@@ -847,7 +847,11 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
     }
 }
 
-// (e) finalize: records -> chain rows + info rows at anchor-major positions
+// (e) finalize: records -> chain rows + info rows at anchor-major positions.
+// A warp per tile of 32 consecutive anchors (input order): the tile's curvelets fill
+// consecutive output rows, so the warp's lanes take them in row order (coalesced
+// stores, no lane serialised behind a dense anchor), each finding its anchor among
+// the tile's by a shuffle search over the tile's prefix of counts.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
@@ -860,19 +864,58 @@ __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, in
         M = dims->M;
     }
     const int W = md.gms + 1;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < N; a += gridDim.x * blockDim.x) {
-        const unsigned c0 = run_cnt[2 * a], c1 = run_cnt[2 * a + 1];
-        if (c0 + c1 == 0 || out_off[a] + c0 + c1 > out_cap) continue;
-        const int m = map_of(map_off, M, a);
-        const int moff = map_off[m];
-        const unsigned long long dst = out_off[a];
-        const T ref_x = edges[(size_t)a * sz + 0];
-        const T ref_y = edges[(size_t)a * sz + 1];
-        const T ref_theta = edges[(size_t)a * sz + 2];
-        for (unsigned r = 0; r < c0 + c1; ++r) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int warps = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    for (long long a0 = (long long)warp * 32; a0 < N; a0 += (long long)warps * 32) {
+        // this lane's anchor: its curvelets (none when past the outputs' capacity)
+        const int a = (int)a0 + lane;
+        unsigned c0 = 0, cnt = 0, rb0 = 0, rb1 = 0;
+        unsigned long long dst = 0;
+        int moff = 0;
+        T ref_x = T(0), ref_y = T(0), ref_theta = T(0);
+        if (a < N) {
+            c0 = run_cnt[2 * a];
+            const unsigned c1 = run_cnt[2 * a + 1];
+            dst = out_off[a];
+            if (c0 + c1 > 0 && dst + c0 + c1 <= out_cap) {
+                cnt = c0 + c1;
+                rb0 = rec_base[2 * a];
+                rb1 = rec_base[2 * a + 1];
+                moff = map_off[map_of(map_off, M, a)];
+                ref_x = edges[(size_t)a * sz + 0];
+                ref_y = edges[(size_t)a * sz + 1];
+                ref_theta = edges[(size_t)a * sz + 2];
+            }
+        }
+        unsigned incl = cnt;  // inclusive prefix of the tile's counts
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned o = __shfl_up_sync(FULL, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const unsigned total = __shfl_sync(FULL, incl, 31);
+        for (unsigned e0 = 0; e0 < total; e0 += 32) {
+            const unsigned e = e0 + lane;
+            // the anchor of curvelet e: the first lane whose inclusive prefix exceeds e
+            int L = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const unsigned v = __shfl_sync(FULL, incl, L + step - 1);
+                if (v <= e) L += step;
+            }
+            const unsigned r = e - (__shfl_sync(FULL, incl, L) - __shfl_sync(FULL, cnt, L));
+            const unsigned lc0 = __shfl_sync(FULL, c0, L);
+            const unsigned lrb0 = __shfl_sync(FULL, rb0, L), lrb1 = __shfl_sync(FULL, rb1, L);
+            const unsigned long long ldst = __shfl_sync(FULL, dst, L);
+            const int lmoff = __shfl_sync(FULL, moff, L);
+            const T lx = __shfl_sync(FULL, ref_x, L), ly = __shfl_sync(FULL, ref_y, L);
+            const T ltheta = __shfl_sync(FULL, ref_theta, L);
+            if (e >= total) continue;
+            const int la = (int)a0 + L;
             const unsigned long long s =
-                (r < c0) ? (unsigned long long)rec_base[2 * a] + r : (unsigned long long)rec_base[2 * a + 1] + (r - c0);
-            const unsigned long long d = dst + r;
+                (r < lc0) ? (unsigned long long)lrb0 + r : (unsigned long long)lrb1 + (r - lc0);
+            const unsigned long long d = ldst + r;
             const unsigned meta = rec.meta[s];
             const unsigned len = meta & 0xffu;
             const unsigned bcell = (meta >> 8) & 0xffffu;
@@ -880,8 +923,8 @@ __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, in
             const unsigned *ids = rec.ids + s * (unsigned long long)md.gms;
             // chain row (record_curvelet_chain, :269-276): [anchor+1, chain[0]+1, ...], zero padded
             unsigned *row = chains + d * (unsigned long long)W;
-            row[0] = (unsigned)(a - moff) + 1u;
-            for (int z = 0; z + 1 < W; ++z) row[z + 1] = (z < (int)len) ? (ids[z] - (unsigned)moff) + 1u : 0u;
+            row[0] = (unsigned)(la - lmoff) + 1u;
+            for (int z = 0; z + 1 < W; ++z) row[z + 1] = (z < (int)len) ? (ids[z] - (unsigned)lmoff) + 1u : 0u;
             // fill_curvelet_info (:221-255)
             const int mini = (int)bcell / md.Q, minj = (int)bcell % md.Q;
             const T k_max = (T)rec.k[s * 2 + 0];
@@ -889,9 +932,9 @@ __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, in
             const T k = (k_max + k_min) / T(2);
             const T dx = info_offset(md.sx, mini, md.P);
             const T dt = info_offset(md.st, minj, md.Q);
-            const T theta = to_2pi(ref_theta + dt);
-            const T pt_x = ref_x - dx * sin(theta);
-            const T pt_y = ref_y + dx * cos(theta);
+            const T theta = to_2pi(ltheta + dt);
+            const T pt_x = lx - dx * sin(theta);
+            const T pt_y = ly + dx * cos(theta);
             T length = T(0);
             for (unsigned z = 0; z + 1 < len; ++z) {
                 const unsigned e1 = ids[z], e2 = ids[z + 1];
@@ -904,7 +947,7 @@ __global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, in
             inf[0] = forward ? 1.0 : 0.0;
             inf[1] = (double)k_max;
             inf[2] = (double)k_min;
-            inf[3] = (double)ref_theta;
+            inf[3] = (double)ltheta;
             inf[4] = (double)pt_x;
             inf[5] = (double)pt_y;
             inf[6] = (double)theta;
