@@ -338,7 +338,8 @@ __host__ __device__ inline size_t nbr_smem_per_warp(int max_cand) {
 // and calls f(ok, j, d2, key) warp-uniformly, 32 entries at a time; ok is the
 // reference predicate. The window's bucket ranges (up to 32 per round) are
 // loaded by the lanes at once; entries are enumerated over their prefix sums.
-template <typename T, typename F>
+// WANT_KEY: compute the scan key (a counting pass needs none).
+template <bool WANT_KEY = true, typename T, typename F>
 __device__ __forceinline__ void for_window_candidates(const ModelT<T> &md, const BinnedT<T> &B, const unsigned *bstart,
                                                       int i, int m, int2 ac, T ax, T ay, int lane, F &&f) {
     const int bx0 = (ac.x - md.w) >> md.sbits, bx1 = (ac.x + md.w) >> md.sbits;
@@ -388,7 +389,7 @@ __device__ __forceinline__ void for_window_candidates(const ModelT<T> &md, const
                     abs(cc.x - ac.x) <= md.w && abs(cc.y - ac.y) <= md.w) {
                     d2 = sq_dist(ax, ay, B.x[j], B.y[j]);  // sq_dist(te, ne), preprocess.hpp:160
                     ok = !(d2 > md.rad_sqr);               // preprocess.hpp:161-163
-                    key = scan_key(cc, ac.x, ac.y, md.w, B.orig[j]);
+                    if (WANT_KEY) key = scan_key(cc, ac.x, ac.y, md.w, B.orig[j]);
                 }
             }
             f(ok, j, d2, key);
@@ -542,8 +543,8 @@ __global__ void __launch_bounds__(256) k_nb(const __grid_constant__ NbArgsT<T> a
         const T ax = a.B.x[i], ay = a.B.y[i];
         if (MODE == NB_COUNT) {
             unsigned cnt = 0;
-            for_window_candidates(md, a.B, a.bstart, i, m, ac, ax, ay, lane,
-                                  [&](bool ok, int, T, unsigned long long) {
+            for_window_candidates<false>(md, a.B, a.bstart, i, m, ac, ax, ay, lane,
+                                         [&](bool ok, int, T, unsigned long long) {
                                       cnt += __popc(__ballot_sync(FULL, ok));
                                   });
             if (lane == 0) {
