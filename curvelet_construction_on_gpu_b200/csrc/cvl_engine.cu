@@ -1491,11 +1491,12 @@ int cvl_engine_create(const cvl_engine_cfg *cfg, cvl_engine **out) {
             const int cs = (c.cell_size == 2 || c.cell_size == 4 || c.cell_size == 8) ? c.cell_size : dflt;
             e->tune[b] = default_tuning(cs, e->seeds_per_group);
         }
-        // batches above 4 Mi edges: bundle chunks of 16 Mi pairs (a 17 GB bundle
-        // buffer), a quarter of the bundle/growth launches of 4 Mi; measured on the
-        // 64-map batch (33.7M edges): 8 Mi 1.6% faster than 4 Mi, 16 Mi another 0.6%
-        // (32 Mi another 0.3%, for a 34 GB buffer); smaller chunks were slower everywhere
-        e->tune[CVL_TUNING_BUCKETS - 1].chunk_pairs = (int64_t)(16ull << 20);
+        // batches above 4 Mi edges: bundle chunks of 8 Mi pairs (an 8 GB bundle
+        // buffer), half the bundle/growth launches of 4 Mi; measured on the 64-map
+        // batch (33.7M edges): 1.6% faster than 4 Mi. 16 Mi was 0.6% faster again on
+        // the resident batch but 4.5% slower through cvl_run_maps (its result copies
+        // run beside the compute); smaller chunks were slower everywhere
+        e->tune[CVL_TUNING_BUCKETS - 1].chunk_pairs = (int64_t)(8ull << 20);
     }
     e->slots = c.bundle_slots > 0 ? c.bundle_slots : 10;
     cudaError_t ce = cudaSetDevice(e->device);

@@ -481,7 +481,7 @@ typedef struct cvl_tuning {
                                          (8: 63 registers; grids other than the default 63-cell one take 6 for 8) */
     int seeds_per_group;              /* chain-growth seeds walked together per warp: 4 or 8 (4) */
     int anchors_per_warp;             /* chain-growth anchors per warp: 1..32 (8) */
-    int64_t chunk_pairs;              /* neighbour pairs whose bundles are held in HBM at once (4 Mi; 16 Mi above 4 Mi edges) */
+    int64_t chunk_pairs;              /* neighbour pairs whose bundles are held in HBM at once (4 Mi; 8 Mi above 4 Mi edges) */
 } cvl_tuning;
 /* The bucket a batch of num_edges edges uses. */
 int cvl_tuning_bucket(int64_t num_edges);
