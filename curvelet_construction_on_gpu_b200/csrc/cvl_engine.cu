@@ -739,7 +739,7 @@ int run_pipeline_direct(cvl_engine *e, const R *d_edges, int n, int sz, const in
     na.stats = stats;
     na.pair_off = (const unsigned long long *)e->pair_off.p;
     na.err = err;
-    k_nb<R, NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+    k_nb<R, NB_COUNT><<<gn, nb_wpb * 32, 0, s>>>(na);  // no candidate staging
     CVL_TRY(check_launch("k_nb<COUNT>"));
     k_deg_from_ncand<<<gb, 256, 0, s>>>(n, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p, nullptr);
     CVL_TRY(check_launch("k_deg_from_ncand"));
@@ -1185,7 +1185,7 @@ int run_pipeline_graph(cvl_engine *e, const double *d_edges, int n, int sz, cons
             na.dims = dd;
             na.pair_cap = (unsigned long long)sh.num_pairs;
             const int gn = std::min(short_grid(N, (long long)nb_wpb * 4), sms * 8);
-            k_nb<double, NB_COUNT><<<gn, nb_wpb * 32, nb_smem, s>>>(na);
+            k_nb<double, NB_COUNT><<<gn, nb_wpb * 32, 0, s>>>(na);  // no candidate staging
             CVL_TRY(check_launch("k_nb<COUNT>"));
             k_deg_from_ncand<<<gb, 256, 0, s>>>(N, md.max_cand, (const unsigned *)e->ncand.p, (unsigned *)e->deg.p, dd);
             CVL_TRY(check_launch("k_deg_from_ncand"));
