@@ -516,10 +516,11 @@ __device__ __forceinline__ unsigned direction_class(T ax, T ay, T lx, T ly, T co
 // be copied to every thread's local stack for that (~300 bytes per thread, stored
 // in the prologue of every launch whether or not any anchor is truncated).
 template <typename T, int MODE>
-// Register budgets: COUNT 8 blocks per SM (32 registers; its latency-bound gathers
-// gain more from 64 resident warps than its few spills cost: 21.8 -> 18.2 ms on the
-// 64-map batch), FILL 4 (64 registers; without a bound it took more and ran 78% slower).
-__global__ void __launch_bounds__(256, MODE == NB_COUNT ? 8 : 4) k_nb(const __grid_constant__ NbArgsT<T> a) {
+// Register budgets: both passes are latency-bound gathers, which gain more from
+// resident warps than their few spills cost. COUNT 8 blocks per SM (32 registers:
+// 21.8 -> 18.2 ms on the 64-map batch); FILL 6 (40 registers: 48.1 -> 42.1 ms against
+// 64 registers, 42.8 ms at 48; without a bound it took more and ran 78% slower).
+__global__ void __launch_bounds__(256, MODE == NB_COUNT ? 8 : 6) k_nb(const __grid_constant__ NbArgsT<T> a) {
     extern __shared__ __align__(16) unsigned char nb_smem[];
     __shared__ BlockStats bstats;
     const ModelT<T> &md = a.md;

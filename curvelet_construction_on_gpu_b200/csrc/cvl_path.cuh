@@ -853,8 +853,10 @@ __global__ void __launch_bounds__(GROWTH_THREADS, 4 * MINB) k_growth(GrowthArgsT
 // stores, no lane serialised behind a dense anchor), each finding its anchor among
 // the tile's by a shuffle search over the tile's prefix of counts.
 // ---------------------------------------------------------------------------
+// 4 blocks of 256 per SM (64 registers, a few spills): 8.45 -> 7.9 ms on the 64-map
+// batch against the 78 registers it takes unbounded (3 blocks).
 template <typename T>
-__global__ void k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
+__global__ void __launch_bounds__(256, 4) k_finalize(ModelT<T> md, const T *__restrict__ edges, int sz, int N, const int *__restrict__ map_off,
                            int M, Records rec, const unsigned *__restrict__ rec_base,
                            const unsigned *__restrict__ run_cnt, const unsigned long long *__restrict__ out_off,
                            unsigned long long out_cap, unsigned *__restrict__ chains, double *__restrict__ info,
